@@ -1,0 +1,194 @@
+/*
+ * mrlbm.h -- C ABI of the B200 moment-representation LBM (MR-LBM) library.
+ *
+ * The reference solver (CERNN/MR-LBM) has no runtime plugin interface: its
+ * boundary is a compile-time case API, one fused kernel launched from main(),
+ * and its on-disk formats.  Each entry point below names the reference
+ * interface it replaces (paths relative to the reference's source tree).
+ *
+ * Conventions
+ *   - Every function returns an mrlbm_status; 0 is success.  Nothing calls
+ *     exit(); the message of the last failure on the calling thread is
+ *     available from mrlbm_last_error().
+ *   - Host buffers are owned by the caller.  Device memory is owned by the
+ *     handle that allocated it.
+ *   - A handle is thread-compatible, not thread-safe: one host thread at a time.
+ *   - "x-fastest" arrays are indexed x + nx*(y + ny*z) (the reference's
+ *     idxScalarGlobal, src/globalFunctions.h:271-275).
+ *   - "reference layout" is the reference's block-interleaved moment array
+ *     idxMom (src/globalFunctions.h:31-42) with 8x8x8 blocks; it needs nx, ny
+ *     and nz to be multiples of 8, like the reference.
+ *   - Stored moments use the reference's scaled form (src/arrayIndex.h:8-17,
+ *     186-187): rho-rho0, 3u, 4.5*Pi_xx, 9*Pi_xy, 9*Pi_xz, 4.5*Pi_yy, 9*Pi_yz,
+ *     4.5*Pi_zz (+ omega as moment 10 when the viscosity is non-Newtonian).
+ */
+#ifndef MRLBM_H
+#define MRLBM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    MRLBM_OK = 0,
+    MRLBM_EINVAL = 1,     /* bad argument or unsupported configuration */
+    MRLBM_ENOMEM = 2,     /* device or host allocation failed / over budget */
+    MRLBM_ECUDA = 3,      /* a CUDA call failed */
+    MRLBM_EIO = 4,        /* file could not be read or written */
+    MRLBM_EDIVERGED = 5,  /* NaN/Inf or |u| above the stability limit */
+    MRLBM_ETIMEDOUT = 6,  /* a bounded device wait gave up */
+    MRLBM_ENOTFOUND = 7,  /* unknown request / handle */
+    MRLBM_EBUSY = 8       /* no free slot */
+} mrlbm_status;
+
+typedef enum { MRLBM_D3Q19 = 19, MRLBM_D3Q27 = 27 } mrlbm_lattice;
+typedef enum { MRLBM_F32 = 0, MRLBM_F16 = 1, MRLBM_BF16 = 2 } mrlbm_storage;
+typedef enum { MRLBM_NEWTONIAN = 0, MRLBM_POWERLAW = 1, MRLBM_BINGHAM = 2 } mrlbm_rheology;
+
+/* Node-type words follow the reference's nodeTypeMap (src/nodeTypeMap.h:10-80):
+ * bits 0-7 octant solid mask (0 = bulk, 0xFF = solid), bits 8-10 BC kind
+ * (0 no-slip wall, 1 prescribed-velocity wall), bits 11-12 velocity index. */
+#define MRLBM_NODE_BULK 0x00u
+#define MRLBM_NODE_SOLID 0xFFu
+#define MRLBM_BC_VELOCITY_WALL (1u << 8)
+#define MRLBM_BC_VELOCITY_INDEX(k) (((uint32_t)(k) & 3u) << 11)
+
+/* Run-time description of one domain: the physics that a reference case fixes
+ * at compile time in constants.inc / model.inc (src/cases/<case>/). */
+typedef struct {
+    int nx, ny, nz;
+    int lattice;            /* MRLBM_D3Q19 or MRLBM_D3Q27 (model.inc D3Qxx) */
+    int storage;            /* mrlbm_storage: precision of the stored moments */
+    int periodic[3];        /* 1 = BC_<axis>_PERIODIC, 0 = BC_<axis>_WALL */
+    double tau;             /* relaxation time (constants.inc TAU) */
+    double rho0;            /* RHO_0 */
+    double force[3];        /* body force FX, FY, FZ (lattice units) */
+    double bc_velocity[4][3]; /* wall velocity per velocity index (UX_BC..UZ_BC) */
+    int rheology;           /* mrlbm_rheology (model.inc POWERLAW / BINGHAM) */
+    double nnf_n;           /* power-law index N_INDEX */
+    double nnf_k;           /* power-law consistency K_CONSISTENCY (0: rho0*(tau-1/2)/3) */
+    double nnf_yield;       /* Bingham yield stress S_Y */
+    double nnf_omega_p;     /* Bingham plastic omega OMEGA_P (0: 1/tau) */
+    int bc_matrix_q;        /* 0: reference behaviour (19 on D3Q27, i.e. the
+                               D3Q19 wall closed forms), or 19 / 27 explicitly */
+    int reserved[7];
+} mrlbm_desc;
+
+typedef struct mrlbm_domain mrlbm_domain;
+
+/* FP64 global sums over non-solid nodes (the reference's FP32 reductions,
+ * src/reduction.cu:100-155, done in double). */
+typedef struct {
+    double mass;            /* sum rho */
+    double momentum[3];     /* sum rho u */
+    double kinetic_energy;  /* sum rho |u|^2 / 2 */
+    double fluid_nodes;
+    double max_speed;       /* max |u| */
+    double nonfinite;       /* count of non-finite moments */
+} mrlbm_sums;
+
+const char* mrlbm_last_error(void);
+const char* mrlbm_version(void);
+
+/* Device selection for the calling host thread (the reference hard-codes
+ * GPU_INDEX, src/var.h:31) and pinned host buffers for fast transfers. */
+mrlbm_status mrlbm_set_device(int device);
+mrlbm_status mrlbm_device_count(int* count);
+mrlbm_status mrlbm_host_alloc(size_t bytes, void** ptr);
+mrlbm_status mrlbm_host_free(void* ptr);
+
+/* Allocation + setup.  Replaces allocateDeviceMemory/interfaceMalloc
+ * (src/main.cuh:455-900) for one case. */
+mrlbm_status mrlbm_domain_create(const mrlbm_desc* desc, mrlbm_domain** out);
+mrlbm_status mrlbm_domain_destroy(mrlbm_domain* dom);
+/* Device bytes held by a domain of this description (moments, node classes). */
+mrlbm_status mrlbm_domain_bytes(const mrlbm_desc* desc, size_t* bytes);
+
+/* Node types, x-fastest, reference nodeTypeMap words.  Replaces
+ * hostInitialization_nodeType / bc_initialization.inc
+ * (src/lbmInitialization.cu:958-975). */
+mrlbm_status mrlbm_set_node_types(mrlbm_domain* dom, const uint32_t* node_type);
+
+/* Initial state from physical rho, u fields (x-fastest, host).  Replaces
+ * gpuInitialization_mom + flow_initialization.inc
+ * (src/lbmInitialization.cu:28-131), including its D3Q19-sum second moments. */
+mrlbm_status mrlbm_init_flow(mrlbm_domain* dom, const float* rho, const float* ux, const float* uy,
+                             const float* uz);
+/* Built-in initial states computed on the device:
+ * uniform rho0 and velocity (u0[3]), and the Taylor-Green vortex of
+ * src/cases/taylorGreen/flow_initialization.inc:1-4 with amplitude u0 and
+ * length scale L (L = N / 2pi in the reference). */
+mrlbm_status mrlbm_init_uniform(mrlbm_domain* dom, const double u0[3]);
+mrlbm_status mrlbm_init_taylor_green(mrlbm_domain* dom, double u0, double L);
+
+/* Advance nsteps fused collide-stream steps on the domain's stream.  Replaces
+ * the gpuMomCollisionStream launch + swapGhostInterfaces loop
+ * (src/main.cu:200-230, src/mlbm.cu:3-714); no host sync per step. */
+mrlbm_status mrlbm_step(mrlbm_domain* dom, int nsteps);
+/* Same, recorded once into a CUDA graph and replayed (for small domains where
+ * launch cost matters). */
+mrlbm_status mrlbm_step_graph(mrlbm_domain* dom, int nsteps);
+/* Device-timed nsteps: CUDA events on the domain's stream around the launches. */
+mrlbm_status mrlbm_time_steps(mrlbm_domain* dom, int nsteps, float* ms);
+mrlbm_status mrlbm_synchronize(mrlbm_domain* dom);
+mrlbm_status mrlbm_get_step(mrlbm_domain* dom, int* step);
+
+/* Moments in the reference's idxMom layout (fMom, host float buffer of
+ * nx*ny*nz*num_moments).  Used by checkpoints and drop-in callers. */
+mrlbm_status mrlbm_num_moments(mrlbm_domain* dom, int* nm);
+mrlbm_status mrlbm_get_moments_ref_layout(mrlbm_domain* dom, float* fmom);
+mrlbm_status mrlbm_set_moments_ref_layout(mrlbm_domain* dom, const float* fmom);
+/* Moments as float, [moment][z][y][x] (x fastest). */
+mrlbm_status mrlbm_get_moments(mrlbm_domain* dom, float* m);
+mrlbm_status mrlbm_set_moments(mrlbm_domain* dom, const float* m);
+/* Macroscopic fields as saveMacr writes them (src/saveData.cu:62-74):
+ * rho = rho0 + m0, u = stored 3u (NOT divided by 3), x-fastest.  Any pointer
+ * may be NULL. */
+mrlbm_status mrlbm_get_macr(mrlbm_domain* dom, float* rho, float* ux, float* uy, float* uz, float* omega);
+
+/* FP64 reductions (mass, momentum, kinetic energy, divergence watch).  Replaces
+ * sumReductionThread_* + sumReductionBlock + totalKineticEnergy
+ * (src/reduction.cu:37-243, src/treatData.cu:105-165). */
+mrlbm_status mrlbm_reduce_fp64(mrlbm_domain* dom, mrlbm_sums* out);
+/* Steady-state residual ||u^n - u^ref||_2 / (||u^n||_2 + 1e-30) over fluid
+ * nodes, FP64, against the snapshot taken by the previous call (the first
+ * call takes the snapshot and returns 1). */
+mrlbm_status mrlbm_residual(mrlbm_domain* dom, double* residual);
+
+/* Files in the reference formats. */
+/* <path>/<id>/checkpoint/_curr_step.bin, _fMom.bin, _fGhost.{X,Y,Z}_{0,1}.bin
+ * (src/checkpoint.cu:129-186, 372-382; POSIX separators). */
+mrlbm_status mrlbm_save_checkpoint(mrlbm_domain* dom, const char* path_files, const char* id_sim, int step);
+/* Loads the same file set; *step receives the saved step + 1 (checkpoint.cu:157-159). */
+mrlbm_status mrlbm_load_checkpoint(mrlbm_domain* dom, const char* path_files, const char* id_sim, int* step);
+/* <path>/<id>/<id>_{rho,ux,uy,uz[,omega]}NNNNNN.bin (src/saveData.cu:62-260, 439-467). */
+mrlbm_status mrlbm_save_macr_bin(mrlbm_domain* dom, const char* path_files, const char* id_sim, int step);
+/* <path>/<id>/<id>_info.txt (src/saveData.cu:469-613); case_name = BC type. */
+mrlbm_status mrlbm_save_info(mrlbm_domain* dom, const char* path_files, const char* id_sim,
+                             const char* case_name, int nsteps, double mlups);
+
+/* Host-side node-type builders (no device work).
+ * Voxel geometry: solid (x-fastest, nonzero = solid) -> nodeTypeMap words: solid
+ * nodes 0xFF, fluid nodes the octant mask of their solid neighbours; neighbours
+ * outside a non-periodic axis count as solid (domain walls).  Replaces bc_id +
+ * define_voxel_bc (src/lbmInitialization.cu:1058-1227). */
+mrlbm_status mrlbm_voxel_node_types(int nx, int ny, int nz, const uint8_t* solid, const int periodic[3],
+                                    uint32_t* node_type);
+/* The lid-driven cavity typing of src/cases/lidDrivenCavity_3D/bc_initialization.inc:
+ * the whole y = ny-1 face (edges and corners included) is the lid, a velocity
+ * wall with the given velocity index; other boundary nodes are no-slip walls. */
+mrlbm_status mrlbm_lid_cavity_node_types(int nx, int ny, int nz, int lid_velocity_index, uint32_t* node_type);
+/* The moment-BC data the device uses for one node type (host only; for
+ * inspection and tests).  out[0..48] A(omega0)^-1 row-major, out[49..55]
+ * A^-1 e0, out[56..62] q^T A^-1, out[63] q^T A^-1 e0, out[64..66] wall
+ * velocity; *known = bitmask of known populations. */
+mrlbm_status mrlbm_bc_class_info(int lattice, int bc_matrix_q, uint32_t node_type, const double bc_velocity[4][3],
+                                 double omega0, float* out, uint32_t* known);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MRLBM_H */

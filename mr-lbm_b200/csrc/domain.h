@@ -1,0 +1,66 @@
+// domain.h -- internal state of one MR-LBM domain (not part of the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "../../include/mrlbm.h"
+#include "kernels.cuh"
+
+namespace mrlbm {
+
+constexpr int TILE_Y = 14;       // interior rows per CTA (16 warps with the halo rows)
+constexpr int GRAPH_STEPS = 16;  // launches per captured graph (even: parities chain)
+
+}  // namespace mrlbm
+
+// HBM layout: each of the nm moments is a plane stack [z][y][pitch] (x
+// fastest, pitch = nx rounded up to 8), stored in the domain's storage type,
+// twice (ping-pong: step n reads m[cur] and writes m[cur^1]).  Node classes
+// are one byte per node in the same padded layout.
+struct mrlbm_domain {
+    mrlbm_desc d{};
+    int q = 19, nm = 10;
+    size_t esize = 4;
+    int pitch = 0;
+    long long plane = 0, field = 0;
+    double omega0 = 1.0;
+    void* m[2] = {nullptr, nullptr};
+    int cur = 0;
+    int step = 0;
+    uint8_t* cls = nullptr;
+    mrlbm::BcClass* bc = nullptr;
+    int nclasses = 0;
+    bool has_bc = false;
+    float ext[11] = {};
+    float scale[11] = {}, iscale[11] = {};
+    int lz = 16;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double* red_scratch = nullptr;  // block partials + 8 results
+    double* red_host = nullptr;     // pinned
+    int red_blocks = 0;
+    float* usnap = nullptr;         // residual snapshot (3 floats per node)
+    float* stage = nullptr;         // float staging buffer for layout conversions
+    bool have_snap = false;
+    cudaGraphExec_t graph_exec = nullptr;
+};
+
+namespace mrlbm {
+
+mrlbm_status fail(mrlbm_status st, const char* fmt, ...);
+uint32_t known_mask(int q, uint32_t octants);
+mrlbm_status build_bc_class(int q, int mq, uint32_t word, const double uvel[4][3], double omega0, BcClass* out);
+mrlbm_status classify_nodes(int q, int mq, const uint32_t* nt, long long n, const double uvel[4][3], double omega0,
+                            std::vector<uint8_t>& cls, std::vector<BcClass>& table, bool& any_bc);
+void storage_scales(int storage, float* scale, float* iscale);
+mrlbm_status domain_alloc(mrlbm_domain* dom);
+int choose_lz(const mrlbm_domain* dom);
+void fill_step_args(const mrlbm_domain* dom, StepArgs& a, int parity, int& flags);
+mrlbm_status enqueue_step(mrlbm_domain* dom, int parity, cudaStream_t s);
+template <int Q, typename T>
+mrlbm_status dispatch_step(const StepArgs& a, int flags, cudaStream_t s);
+mrlbm_status enqueue_reduce(mrlbm_domain* dom, double* partial, double* out, int residual_mode, cudaStream_t s);
+
+}  // namespace mrlbm

@@ -1,0 +1,742 @@
+// mrlbm.cu -- C ABI (include/mrlbm.h) over the sm_100a MR-LBM kernels.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/mrlbm.h"
+#include "aux_kernels.cuh"
+#include "domain.h"
+#include "kernels.cuh"
+
+using namespace mrlbm;
+
+// ------------------------------------------------------------------ errors
+
+static thread_local std::string g_err;
+
+mrlbm_status mrlbm::fail(mrlbm_status st, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return st;
+}
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return fail(MRLBM_ECUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                        __LINE__);                                                                 \
+    } while (0)
+
+extern "C" const char* mrlbm_last_error(void) { return g_err.c_str(); }
+extern "C" const char* mrlbm_version(void) { return "mrlbm-b200 0.1 (sm_100a)"; }
+
+extern "C" mrlbm_status mrlbm_set_device(int device)
+{
+    CK(cudaSetDevice(device));
+    return MRLBM_OK;
+}
+
+extern "C" mrlbm_status mrlbm_device_count(int* count)
+{
+    if (!count) return fail(MRLBM_EINVAL, "null argument");
+    CK(cudaGetDeviceCount(count));
+    return MRLBM_OK;
+}
+
+extern "C" mrlbm_status mrlbm_host_alloc(size_t bytes, void** ptr)
+{
+    if (!ptr) return fail(MRLBM_EINVAL, "null argument");
+    *ptr = nullptr;
+    cudaError_t e = cudaMallocHost(ptr, bytes);
+    if (e != cudaSuccess) return fail(MRLBM_ENOMEM, "cudaMallocHost(%zu): %s", bytes, cudaGetErrorString(e));
+    return MRLBM_OK;
+}
+
+extern "C" mrlbm_status mrlbm_host_free(void* ptr)
+{
+    if (ptr) CK(cudaFreeHost(ptr));
+    return MRLBM_OK;
+}
+
+// ------------------------------------------------------- BC class building
+
+// h_k(c) = c_a c_b - delta_ab/3 and g_k(c) = coefficient of Pi_k in 4.5 H(c):Pi
+static void hg(int i, double* h, double* g)
+{
+    const double cx = lat_cx(i), cy = lat_cy(i), cz = lat_cz(i);
+    h[0] = cx * cx - 1.0 / 3.0; h[1] = cx * cy; h[2] = cx * cz;
+    h[3] = cy * cy - 1.0 / 3.0; h[4] = cy * cz; h[5] = cz * cz - 1.0 / 3.0;
+    g[0] = 4.5 * h[0]; g[1] = 9.0 * h[1]; g[2] = 9.0 * h[2];
+    g[3] = 4.5 * h[3]; g[4] = 9.0 * h[4]; g[5] = 4.5 * h[5];
+}
+
+uint32_t mrlbm::known_mask(int q, uint32_t octants)
+{
+    uint32_t known = 0;
+    for (int i = 0; i < q; i++) {
+        const int d[3] = {-lat_cx(i), -lat_cy(i), -lat_cz(i)};
+        bool all = true;
+        for (int o = 0; o < 8 && all; o++) {
+            const int s[3] = {(o & 1) ? 1 : -1, (o & 2) ? 1 : -1, (o & 4) ? 1 : -1};
+            bool consistent = true;
+            for (int k = 0; k < 3; k++)
+                if (d[k] != 0 && d[k] != s[k]) consistent = false;
+            if (consistent && !((octants >> o) & 1u)) all = false;
+        }
+        if (!all) known |= 1u << i;
+    }
+    return known;
+}
+
+static bool invert7(const double A[7][7], double inv[7][7])
+{
+    double M[7][14];
+    for (int r = 0; r < 7; r++)
+        for (int c = 0; c < 14; c++) M[r][c] = c < 7 ? A[r][c] : (c - 7 == r ? 1.0 : 0.0);
+    for (int c = 0; c < 7; c++) {
+        int best = c;
+        for (int r = c + 1; r < 7; r++)
+            if (std::fabs(M[r][c]) > std::fabs(M[best][c])) best = r;
+        if (std::fabs(M[best][c]) < 1e-12) return false;
+        if (best != c)
+            for (int k = 0; k < 14; k++) std::swap(M[c][k], M[best][k]);
+        const double p = M[c][c];
+        for (int k = 0; k < 14; k++) M[c][k] /= p;
+        for (int r = 0; r < 7; r++) {
+            if (r == c || M[r][c] == 0.0) continue;
+            const double f = M[r][c];
+            for (int k = 0; k < 14; k++) M[r][k] -= f * M[c][k];
+        }
+    }
+    for (int r = 0; r < 7; r++)
+        for (int c = 0; c < 7; c++) inv[r][c] = M[r][c + 7];
+    return true;
+}
+
+mrlbm_status mrlbm::build_bc_class(int q, int mq, uint32_t word, const double uvel[4][3], double omega0,
+                                    BcClass* out)
+{
+    const uint32_t oct = word & 0xFFu;
+    const uint32_t kind = (word >> 8) & 7u;
+    const uint32_t vidx = (word >> 11) & 3u;
+    if (kind > 1)
+        return fail(MRLBM_EINVAL, "node type 0x%x: BC kind %u not supported (only no-slip and velocity walls)",
+                    word, kind);
+    double u[3] = {0, 0, 0};
+    if (kind == 1)
+        for (int a = 0; a < 3; a++) u[a] = uvel[vidx][a];
+    const uint32_t known = known_mask(q, oct);
+    const double uu[6] = {u[0] * u[0], u[0] * u[1], u[0] * u[2], u[1] * u[1], u[1] * u[2], u[2] * u[2]};
+    double A[7][7] = {};
+    double a1 = 0.0, r[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = 0; i < mq; i++) {
+        if (!((known >> i) & 1u)) continue;
+        const double w = lat_w(mq, i);
+        double h[6], g[6];
+        hg(i, h, g);
+        const double cu = 3.0 * (lat_cx(i) * u[0] + lat_cy(i) * u[1] + lat_cz(i) * u[2]);
+        double guu = 0.0;
+        for (int k = 0; k < 6; k++) guu += g[k] * uu[k];
+        A[0][0] += w * (1.0 + cu + omega0 * guu);
+        a1 += w * guu;
+        for (int k = 0; k < 6; k++) {
+            A[0][1 + k] += (1.0 - omega0) * w * g[k];
+            r[k] += w * g[k];
+        }
+        for (int rr = 0; rr < 6; rr++) {
+            A[1 + rr][0] += w * h[rr] * (1.0 + cu);
+            for (int k = 0; k < 6; k++) A[1 + rr][1 + k] += w * h[rr] * g[k];
+        }
+    }
+    double inv[7][7];
+    if (!invert7(A, inv))
+        return fail(MRLBM_EINVAL, "node type 0x%x: singular moment-BC system at omega=%g", word, omega0);
+    const double qv[7] = {a1, -r[0], -r[1], -r[2], -r[3], -r[4], -r[5]};
+    double qa[7];
+    for (int c = 0; c < 7; c++) {
+        qa[c] = 0.0;
+        for (int k = 0; k < 7; k++) qa[c] += qv[k] * inv[k][c];
+    }
+    memset(out, 0, sizeof(*out));
+    for (int rr = 0; rr < 7; rr++)
+        for (int c = 0; c < 7; c++) out->ainv[rr * 7 + c] = (float)inv[rr][c];
+    for (int rr = 0; rr < 7; rr++) {
+        out->v[rr] = (float)inv[rr][0];
+        out->qa[rr] = (float)qa[rr];
+    }
+    out->s = (float)qa[0];
+    for (int a = 0; a < 3; a++) out->u[a] = (float)u[a];
+    out->known = known;
+    out->valid = 1;
+    return MRLBM_OK;
+}
+
+// ------------------------------------------------------------ domain setup
+
+static int moments_of(const mrlbm_desc& d) { return d.rheology != MRLBM_NEWTONIAN ? 11 : 10; }
+
+static size_t elem_size(int storage) { return storage == MRLBM_F32 ? 4 : 2; }
+
+void mrlbm::storage_scales(int storage, float* scale, float* iscale)
+{
+    for (int k = 0; k < 11; k++) {
+        float s = 1.0f;
+        if (storage != MRLBM_F32) {
+            // powers of two keep values of the shifted moments in the normal
+            // range of fp16 (exact, no rounding from the scaling itself)
+            s = k == 0 ? 256.0f : (k <= 3 ? 8.0f : (k <= 9 ? 64.0f : 1.0f));
+        }
+        scale[k] = s;
+        iscale[k] = 1.0f / s;
+    }
+}
+
+static mrlbm_status validate(const mrlbm_desc* d)
+{
+    if (!d) return fail(MRLBM_EINVAL, "null descriptor");
+    if (d->nx < 1 || d->ny < 1 || d->nz < 1 || d->nx > 8192 || d->ny > 8192 || d->nz > 8192)
+        return fail(MRLBM_EINVAL, "bad grid %dx%dx%d", d->nx, d->ny, d->nz);
+    if (d->lattice != 19 && d->lattice != 27) return fail(MRLBM_EINVAL, "lattice must be 19 or 27");
+    if (d->storage < 0 || d->storage > 2) return fail(MRLBM_EINVAL, "bad storage %d", d->storage);
+    if (!(d->tau > 0.5)) return fail(MRLBM_EINVAL, "tau must be > 0.5 (got %g)", d->tau);
+    if (d->rheology < 0 || d->rheology > 2) return fail(MRLBM_EINVAL, "bad rheology");
+    if (d->bc_matrix_q != 0 && d->bc_matrix_q != 19 && d->bc_matrix_q != d->lattice)
+        return fail(MRLBM_EINVAL, "bc_matrix_q must be 0, 19 or the lattice size");
+    return MRLBM_OK;
+}
+
+extern "C" mrlbm_status mrlbm_domain_bytes(const mrlbm_desc* d, size_t* bytes)
+{
+    mrlbm_status st = validate(d);
+    if (st) return st;
+    const size_t pitch = (size_t)((d->nx + 7) / 8 * 8);
+    const size_t field = pitch * d->ny * d->nz;
+    *bytes = 2 * field * moments_of(*d) * elem_size(d->storage) + field;
+    return MRLBM_OK;
+}
+
+mrlbm_status mrlbm::domain_alloc(mrlbm_domain* dom)
+{
+    const mrlbm_desc& d = dom->d;
+    dom->q = d.lattice;
+    dom->nm = moments_of(d);
+    dom->esize = elem_size(d.storage);
+    dom->pitch = (d.nx + 7) / 8 * 8;
+    dom->plane = (long long)dom->pitch * d.ny;
+    dom->field = dom->plane * d.nz;
+    dom->omega0 = 1.0 / d.tau;
+    storage_scales(d.storage, dom->scale, dom->iscale);
+    const size_t mbytes = (size_t)dom->field * dom->nm * dom->esize;
+    CK(cudaMalloc(&dom->m[0], mbytes));
+    CK(cudaMalloc(&dom->m[1], mbytes));
+    CK(cudaMemset(dom->m[0], 0, mbytes));
+    CK(cudaMemset(dom->m[1], 0, mbytes));
+    // exterior state: the reference's initial rest state (stale wall ghosts)
+    float ext[11];
+    {
+        const int qs = (d.lattice == 27) ? 19 : 19;
+        double pxx = 0, pyy = 0, pzz = 0;
+        for (int i = 0; i < qs; i++) {
+            const double f = lat_w(d.lattice, i) * d.rho0;
+            pxx += f * lat_cx(i) * lat_cx(i);
+            pyy += f * lat_cy(i) * lat_cy(i);
+            pzz += f * lat_cz(i) * lat_cz(i);
+        }
+        for (int k = 0; k < 11; k++) ext[k] = 0.f;
+        ext[4] = (float)(4.5 * (pxx / d.rho0 - 1.0 / 3.0));
+        ext[7] = (float)(4.5 * (pyy / d.rho0 - 1.0 / 3.0));
+        ext[9] = (float)(4.5 * (pzz / d.rho0 - 1.0 / 3.0));
+        ext[10] = (float)dom->omega0;
+    }
+    memcpy(dom->ext, ext, sizeof(ext));
+    CK(cudaStreamCreateWithFlags(&dom->stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&dom->ev0));
+    CK(cudaEventCreate(&dom->ev1));
+    CK(cudaMalloc(&dom->cls, (size_t)dom->field));
+    CK(cudaMemset(dom->cls, 0, (size_t)dom->field));
+    CK(cudaMalloc(&dom->bc, sizeof(BcClass)));
+    CK(cudaMemset(dom->bc, 0, sizeof(BcClass)));
+    dom->red_blocks = 148 * 4;
+    CK(cudaMalloc(&dom->red_scratch, (size_t)(dom->red_blocks * 8 + 8) * sizeof(double)));
+    CK(cudaMallocHost(&dom->red_host, 8 * sizeof(double)));
+    dom->lz = choose_lz(dom);
+    return MRLBM_OK;
+}
+
+int mrlbm::choose_lz(const mrlbm_domain* dom)
+{
+    const mrlbm_desc& d = dom->d;
+    const int gx = (d.nx + TILE_X - 1) / TILE_X;
+    const int gy = (d.ny + TILE_Y - 1) / TILE_Y;
+    const long long cols = (long long)gx * gy;
+    // aim for >= 8 waves of one 512-thread CTA per SM, keep LZ >= 16
+    long long want = 148LL * 8;
+    int nzc = (int)((want + cols - 1) / cols);
+    if (nzc < 1) nzc = 1;
+    int lz = (d.nz + nzc - 1) / nzc;
+    if (lz < 16) lz = 16;
+    if (lz > d.nz) lz = d.nz;
+    return lz;
+}
+
+extern "C" mrlbm_status mrlbm_domain_create(const mrlbm_desc* desc, mrlbm_domain** out)
+{
+    if (!out) return fail(MRLBM_EINVAL, "null output handle");
+    *out = nullptr;
+    mrlbm_status st = validate(desc);
+    if (st) return st;
+    mrlbm_domain* dom = new mrlbm_domain();
+    dom->d = *desc;
+    if (dom->d.bc_matrix_q == 0) dom->d.bc_matrix_q = 19;
+    if (dom->d.rheology == MRLBM_POWERLAW && dom->d.nnf_k == 0.0)
+        dom->d.nnf_k = dom->d.rho0 * (dom->d.tau - 0.5) / 3.0;
+    if (dom->d.rheology == MRLBM_BINGHAM && dom->d.nnf_omega_p == 0.0) dom->d.nnf_omega_p = 1.0 / dom->d.tau;
+    st = domain_alloc(dom);
+    if (st) {
+        mrlbm_domain_destroy(dom);
+        return st;
+    }
+    *out = dom;
+    return MRLBM_OK;
+}
+
+extern "C" mrlbm_status mrlbm_domain_destroy(mrlbm_domain* dom)
+{
+    if (!dom) return MRLBM_OK;
+    if (dom->graph_exec) cudaGraphExecDestroy(dom->graph_exec);
+    if (dom->stream) cudaStreamSynchronize(dom->stream);
+    cudaFree(dom->m[0]);
+    cudaFree(dom->m[1]);
+    cudaFree(dom->cls);
+    cudaFree(dom->bc);
+    cudaFree(dom->red_scratch);
+    cudaFree(dom->usnap);
+    cudaFree(dom->stage);
+    if (dom->red_host) cudaFreeHost(dom->red_host);
+    if (dom->ev0) cudaEventDestroy(dom->ev0);
+    if (dom->ev1) cudaEventDestroy(dom->ev1);
+    if (dom->stream) cudaStreamDestroy(dom->stream);
+    delete dom;
+    return MRLBM_OK;
+}
+
+mrlbm_status mrlbm::classify_nodes(int q, int mq, const uint32_t* nt, long long n, const double uvel[4][3],
+                                   double omega0, std::vector<uint8_t>& cls, std::vector<BcClass>& table,
+                                   bool& any_bc)
+{
+    std::map<uint32_t, int> ids;
+    table.assign(1, BcClass{});  // class 0: bulk (unused entry)
+    cls.resize(n);
+    any_bc = false;
+    for (long long k = 0; k < n; k++) {
+        const uint32_t w = nt[k];
+        const uint32_t oct = w & 0xFFu;
+        if (oct == 0) { cls[k] = CLS_BULK; continue; }
+        any_bc = true;
+        if (oct == 0xFFu) { cls[k] = CLS_SOLID; continue; }
+        const uint32_t key = w & 0x1FFFu;
+        auto it = ids.find(key);
+        if (it == ids.end()) {
+            if ((int)table.size() >= 255) return fail(MRLBM_EINVAL, "more than 254 distinct boundary node types");
+            BcClass c;
+            mrlbm_status st = build_bc_class(q, mq, key, uvel, omega0, &c);
+            if (st) return st;
+            const int id = (int)table.size();
+            table.push_back(c);
+            it = ids.emplace(key, id).first;
+        }
+        cls[k] = (uint8_t)it->second;
+    }
+    return MRLBM_OK;
+}
+
+extern "C" mrlbm_status mrlbm_set_node_types(mrlbm_domain* dom, const uint32_t* nt)
+{
+    if (!dom || !nt) return fail(MRLBM_EINVAL, "null argument");
+    const mrlbm_desc& d = dom->d;
+    const long long n = (long long)d.nx * d.ny * d.nz;
+    std::vector<uint8_t> cls;
+    std::vector<BcClass> table;
+    bool any = false;
+    mrlbm_status st = classify_nodes(dom->q, d.bc_matrix_q, nt, n, d.bc_velocity, dom->omega0, cls, table, any);
+    if (st) return st;
+    // scatter into the padded plane layout
+    std::vector<uint8_t> padded((size_t)dom->field, 0);
+    for (int z = 0; z < d.nz; z++)
+        for (int y = 0; y < d.ny; y++)
+            memcpy(&padded[(size_t)z * dom->plane + (size_t)y * dom->pitch], &cls[((size_t)z * d.ny + y) * d.nx], d.nx);
+    CK(cudaMemcpyAsync(dom->cls, padded.data(), padded.size(), cudaMemcpyHostToDevice, dom->stream));
+    cudaFree(dom->bc);
+    dom->bc = nullptr;
+    CK(cudaMalloc(&dom->bc, table.size() * sizeof(BcClass)));
+    CK(cudaMemcpyAsync(dom->bc, table.data(), table.size() * sizeof(BcClass), cudaMemcpyHostToDevice, dom->stream));
+    CK(cudaStreamSynchronize(dom->stream));
+    dom->has_bc = any;
+    dom->nclasses = (int)table.size();
+    if (dom->graph_exec) { cudaGraphExecDestroy(dom->graph_exec); dom->graph_exec = nullptr; }
+    return MRLBM_OK;
+}
+
+// ------------------------------------------------------------------- init
+
+template <int Q>
+static void launch_init(mrlbm_domain* dom, InitArgs& a)
+{
+    const int threads = 256;
+    const long long n = (long long)dom->d.nx * dom->d.ny * dom->d.nz;
+    int blocks = (int)std::min<long long>((n + threads - 1) / threads, 148LL * 32);
+    if (dom->d.storage == MRLBM_F32)
+        init_kernel<Q, float><<<blocks, threads, 0, dom->stream>>>(a);
+    else if (dom->d.storage == MRLBM_F16)
+        init_kernel<Q, __half><<<blocks, threads, 0, dom->stream>>>(a);
+    else
+        init_kernel<Q, __nv_bfloat16><<<blocks, threads, 0, dom->stream>>>(a);
+}
+
+static mrlbm_status run_init(mrlbm_domain* dom, InitArgs& a)
+{
+    const mrlbm_desc& d = dom->d;
+    a.m0 = dom->m[0];
+    a.m1 = dom->m[1];
+    a.nx = d.nx; a.ny = d.ny; a.nz = d.nz; a.pitch = dom->pitch;
+    a.plane = dom->plane; a.field = dom->field;
+    a.nm = dom->nm;
+    a.qs = 19;  // the reference's D3Q19 second-moment sums (also on D3Q27)
+    a.rho0 = (float)d.rho0;
+    a.omega0 = (float)dom->omega0;
+    memcpy(a.scale, dom->scale, sizeof(a.scale));
+    if (d.lattice == 19) launch_init<19>(dom, a); else launch_init<27>(dom, a);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(dom->stream));
+    dom->cur = 0;
+    dom->step = 0;
+    dom->have_snap = false;
+    return MRLBM_OK;
+}
+
+extern "C" mrlbm_status mrlbm_init_flow(mrlbm_domain* dom, const float* rho, const float* ux, const float* uy,
+                                         const float* uz)
+{
+    if (!dom || !rho || !ux || !uy || !uz) return fail(MRLBM_EINVAL, "null argument");
+    const size_t n = (size_t)dom->d.nx * dom->d.ny * dom->d.nz;
+    float* dbuf = nullptr;
+    CK(cudaMalloc(&dbuf, 4 * n * sizeof(float)));
+    const float* src[4] = {rho, ux, uy, uz};
+    for (int k = 0; k < 4; k++) {
+        cudaError_t e = cudaMemcpyAsync(dbuf + k * n, src[k], n * sizeof(float), cudaMemcpyHostToDevice, dom->stream);
+        if (e != cudaSuccess) { cudaFree(dbuf); return fail(MRLBM_ECUDA, "copy: %s", cudaGetErrorString(e)); }
+    }
+    InitArgs a{};
+    a.kind = 0;
+    a.rho = dbuf; a.ux = dbuf + n; a.uy = dbuf + 2 * n; a.uz = dbuf + 3 * n;
+    mrlbm_status st = run_init(dom, a);
+    cudaFree(dbuf);
+    return st;
+}
+
+extern "C" mrlbm_status mrlbm_init_uniform(mrlbm_domain* dom, const double u0[3])
+{
+    if (!dom) return fail(MRLBM_EINVAL, "null domain");
+    InitArgs a{};
+    a.kind = 1;
+    for (int k = 0; k < 3; k++) a.u0[k] = u0 ? (float)u0[k] : 0.f;
+    return run_init(dom, a);
+}
+
+extern "C" mrlbm_status mrlbm_init_taylor_green(mrlbm_domain* dom, double u0, double L)
+{
+    if (!dom || !(L > 0)) return fail(MRLBM_EINVAL, "bad argument");
+    InitArgs a{};
+    a.kind = 2;
+    a.tg_u0 = (float)u0;
+    a.tg_L = (float)L;
+    return run_init(dom, a);
+}
+
+// ------------------------------------------------------------------- step
+
+void mrlbm::fill_step_args(const mrlbm_domain* dom, StepArgs& a, int parity, int& flags)
+{
+    const mrlbm_desc& d = dom->d;
+    a.m_in = dom->m[parity];
+    a.m_out = dom->m[parity ^ 1];
+    a.cls = dom->cls;
+    a.bc = dom->bc;
+    a.nx = d.nx; a.ny = d.ny; a.nz = d.nz; a.pitch = dom->pitch;
+    a.plane = dom->plane; a.field = dom->field;
+    a.periodic = (d.periodic[0] ? 1 : 0) | (d.periodic[1] ? 2 : 0) | (d.periodic[2] ? 4 : 0);
+    a.lz = dom->lz;
+    a.rho0 = (float)d.rho0;
+    a.omega0 = (float)dom->omega0;
+    a.fx = (float)d.force[0]; a.fy = (float)d.force[1]; a.fz = (float)d.force[2];
+    a.nnf_n = (float)d.nnf_n; a.nnf_k = (float)d.nnf_k;
+    a.nnf_yield = (float)d.nnf_yield; a.nnf_omega_p = (float)d.nnf_omega_p;
+    memcpy(a.ext, dom->ext, sizeof(a.ext));
+    memcpy(a.scale, dom->scale, sizeof(a.scale));
+    memcpy(a.iscale, dom->iscale, sizeof(a.iscale));
+    flags = 0;
+    if (dom->has_bc && dom->cls) flags |= F_BC;
+    if (d.force[0] != 0.0 || d.force[1] != 0.0 || d.force[2] != 0.0) flags |= F_FORCE;
+    if (d.rheology == MRLBM_POWERLAW) flags |= F_POWERLAW;
+    if (d.rheology == MRLBM_BINGHAM) flags |= F_BINGHAM;
+    if (flags & (F_POWERLAW | F_BINGHAM)) flags |= F_BC;  // nnf variants always read the class map
+}
+
+mrlbm_status mrlbm::enqueue_step(mrlbm_domain* dom, int parity, cudaStream_t s)
+{
+    StepArgs a;
+    int flags;
+    fill_step_args(dom, a, parity, flags);
+    const int q = dom->q;
+    const int stg = dom->d.storage;
+    mrlbm_status st;
+    if (q == 19) {
+        if (stg == MRLBM_F32) st = dispatch_step<19, float>(a, flags, s);
+        else if (stg == MRLBM_F16) st = dispatch_step<19, __half>(a, flags, s);
+        else st = dispatch_step<19, __nv_bfloat16>(a, flags, s);
+    } else {
+        if (stg == MRLBM_F32) st = dispatch_step<27, float>(a, flags, s);
+        else if (stg == MRLBM_F16) st = dispatch_step<27, __half>(a, flags, s);
+        else st = dispatch_step<27, __nv_bfloat16>(a, flags, s);
+    }
+    return st;
+}
+
+extern "C" mrlbm_status mrlbm_step(mrlbm_domain* dom, int nsteps)
+{
+    if (!dom || nsteps < 0) return fail(MRLBM_EINVAL, "bad argument");
+    for (int s = 0; s < nsteps; s++) {
+        mrlbm_status st = enqueue_step(dom, dom->cur, dom->stream);
+        if (st) return st;
+        dom->cur ^= 1;
+        dom->step++;
+    }
+    CK(cudaGetLastError());
+    return MRLBM_OK;
+}
+
+extern "C" mrlbm_status mrlbm_step_graph(mrlbm_domain* dom, int nsteps)
+{
+    if (!dom || nsteps < 0) return fail(MRLBM_EINVAL, "bad argument");
+    if (nsteps == 0) return MRLBM_OK;
+    // One graph of GRAPH_STEPS launches starting from parity 0 (an even count,
+    // so replays chain); an odd leading step or a short remainder runs eagerly.
+    if (!dom->graph_exec) {
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(dom->stream, cudaStreamCaptureModeThreadLocal));
+        for (int s = 0; s < GRAPH_STEPS; s++) {
+            mrlbm_status st = enqueue_step(dom, s & 1, dom->stream);
+            if (st) {
+                cudaStreamEndCapture(dom->stream, &g);
+                if (g) cudaGraphDestroy(g);
+                return st;
+            }
+        }
+        CK(cudaStreamEndCapture(dom->stream, &g));
+        CK(cudaGraphInstantiate(&dom->graph_exec, g, 0));
+        cudaGraphDestroy(g);
+    }
+    int left = nsteps;
+    if (dom->cur != 0) {
+        mrlbm_status st = mrlbm_step(dom, 1);
+        if (st) return st;
+        left--;
+    }
+    while (left >= GRAPH_STEPS) {
+        CK(cudaGraphLaunch(dom->graph_exec, dom->stream));
+        dom->step += GRAPH_STEPS;
+        left -= GRAPH_STEPS;
+    }
+    if (left > 0) return mrlbm_step(dom, left);
+    return MRLBM_OK;
+}
+
+extern "C" mrlbm_status mrlbm_time_steps(mrlbm_domain* dom, int nsteps, float* ms)
+{
+    if (!dom || !ms) return fail(MRLBM_EINVAL, "null argument");
+    CK(cudaEventRecord(dom->ev0, dom->stream));
+    mrlbm_status st = mrlbm_step(dom, nsteps);
+    if (st) return st;
+    CK(cudaEventRecord(dom->ev1, dom->stream));
+    CK(cudaEventSynchronize(dom->ev1));
+    CK(cudaEventElapsedTime(ms, dom->ev0, dom->ev1));
+    return MRLBM_OK;
+}
+
+extern "C" mrlbm_status mrlbm_synchronize(mrlbm_domain* dom)
+{
+    if (!dom) return fail(MRLBM_EINVAL, "null domain");
+    CK(cudaStreamSynchronize(dom->stream));
+    return MRLBM_OK;
+}
+
+extern "C" mrlbm_status mrlbm_get_step(mrlbm_domain* dom, int* step)
+{
+    if (!dom || !step) return fail(MRLBM_EINVAL, "null argument");
+    *step = dom->step;
+    return MRLBM_OK;
+}
+
+// ------------------------------------------------------------ conversions
+
+static mrlbm_status convert(mrlbm_domain* dom, float* hbuf_out, const float* hbuf_in, int mode)
+{
+    const mrlbm_desc& d = dom->d;
+    if ((mode == 2 || mode == 3) && (d.nx % 8 || d.ny % 8 || d.nz % 8))
+        return fail(MRLBM_EINVAL, "reference layout needs nx, ny, nz multiples of 8");
+    const size_t n = (size_t)d.nx * d.ny * d.nz * dom->nm;
+    if (!dom->stage) CK(cudaMalloc(&dom->stage, n * sizeof(float)));
+    float* dbuf = dom->stage;
+    if (mode == 1 || mode == 3)
+        CK(cudaMemcpyAsync(dbuf, hbuf_in, n * sizeof(float), cudaMemcpyHostToDevice, dom->stream));
+    ConvArgs a{};
+    a.m0 = dom->m[dom->cur];
+    a.m1 = dom->m[dom->cur ^ 1];
+    a.f = dbuf;
+    a.nx = d.nx; a.ny = d.ny; a.nz = d.nz; a.pitch = dom->pitch;
+    a.plane = dom->plane; a.field = dom->field;
+    a.nm = dom->nm;
+    a.mode = mode;
+    memcpy(a.scale, dom->scale, sizeof(a.scale));
+    memcpy(a.iscale, dom->iscale, sizeof(a.iscale));
+    const int threads = 256;
+    const int blocks = (int)std::min<size_t>((n + threads - 1) / threads, 148 * 64);
+    if (d.storage == MRLBM_F32) convert_kernel<float><<<blocks, threads, 0, dom->stream>>>(a);
+    else if (d.storage == MRLBM_F16) convert_kernel<__half><<<blocks, threads, 0, dom->stream>>>(a);
+    else convert_kernel<__nv_bfloat16><<<blocks, threads, 0, dom->stream>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && (mode == 0 || mode == 2))
+        e = cudaMemcpyAsync(hbuf_out, dbuf, n * sizeof(float), cudaMemcpyDeviceToHost, dom->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(dom->stream);
+    if (e != cudaSuccess) return fail(MRLBM_ECUDA, "convert: %s", cudaGetErrorString(e));
+    if (mode == 1 || mode == 3) dom->have_snap = false;
+    return MRLBM_OK;
+}
+
+extern "C" mrlbm_status mrlbm_num_moments(mrlbm_domain* dom, int* nm)
+{
+    if (!dom || !nm) return fail(MRLBM_EINVAL, "null argument");
+    *nm = dom->nm;
+    return MRLBM_OK;
+}
+
+extern "C" mrlbm_status mrlbm_get_moments(mrlbm_domain* dom, float* m)
+{
+    if (!dom || !m) return fail(MRLBM_EINVAL, "null argument");
+    return convert(dom, m, nullptr, 0);
+}
+extern "C" mrlbm_status mrlbm_set_moments(mrlbm_domain* dom, const float* m)
+{
+    if (!dom || !m) return fail(MRLBM_EINVAL, "null argument");
+    return convert(dom, nullptr, m, 1);
+}
+extern "C" mrlbm_status mrlbm_get_moments_ref_layout(mrlbm_domain* dom, float* m)
+{
+    if (!dom || !m) return fail(MRLBM_EINVAL, "null argument");
+    return convert(dom, m, nullptr, 2);
+}
+extern "C" mrlbm_status mrlbm_set_moments_ref_layout(mrlbm_domain* dom, const float* m)
+{
+    if (!dom || !m) return fail(MRLBM_EINVAL, "null argument");
+    return convert(dom, nullptr, m, 3);
+}
+
+extern "C" mrlbm_status mrlbm_get_macr(mrlbm_domain* dom, float* rho, float* ux, float* uy, float* uz, float* omega)
+{
+    if (!dom) return fail(MRLBM_EINVAL, "null domain");
+    const mrlbm_desc& d = dom->d;
+    const size_t n = (size_t)d.nx * d.ny * d.nz;
+    std::vector<float> all(n * dom->nm);
+    mrlbm_status st = convert(dom, all.data(), nullptr, 0);
+    if (st) return st;
+    if (rho)
+        for (size_t k = 0; k < n; k++) rho[k] = (float)d.rho0 + all[k];
+    if (ux) memcpy(ux, &all[n], n * sizeof(float));
+    if (uy) memcpy(uy, &all[2 * n], n * sizeof(float));
+    if (uz) memcpy(uz, &all[3 * n], n * sizeof(float));
+    if (omega) {
+        if (dom->nm < 11) return fail(MRLBM_EINVAL, "domain has no omega field");
+        memcpy(omega, &all[10 * n], n * sizeof(float));
+    }
+    return MRLBM_OK;
+}
+
+// ------------------------------------------------------------- reductions
+
+mrlbm_status mrlbm::enqueue_reduce(mrlbm_domain* dom, double* partial, double* out, int residual_mode,
+                                   cudaStream_t s)
+{
+    const mrlbm_desc& d = dom->d;
+    RedArgs a{};
+    a.m = dom->m[dom->cur];
+    a.cls = dom->cls;
+    a.has_cls = dom->has_bc && dom->cls;
+    a.nx = d.nx; a.ny = d.ny; a.nz = d.nz; a.pitch = dom->pitch;
+    a.plane = dom->plane; a.field = dom->field;
+    a.nm = dom->nm;
+    a.rho0 = (float)d.rho0;
+    memcpy(a.iscale, dom->iscale, sizeof(a.iscale));
+    a.partial = partial;
+    a.out = out;
+    a.nblocks = dom->red_blocks;
+    a.usnap = dom->usnap;
+    a.residual_mode = residual_mode;
+    if (d.storage == MRLBM_F32) reduce_kernel<float><<<a.nblocks, RED_THREADS, 0, s>>>(a);
+    else if (d.storage == MRLBM_F16) reduce_kernel<__half><<<a.nblocks, RED_THREADS, 0, s>>>(a);
+    else reduce_kernel<__nv_bfloat16><<<a.nblocks, RED_THREADS, 0, s>>>(a);
+    reduce_finish<<<1, 32, 0, s>>>(partial, a.nblocks, out);
+    CK(cudaGetLastError());
+    return MRLBM_OK;
+}
+
+extern "C" mrlbm_status mrlbm_reduce_fp64(mrlbm_domain* dom, mrlbm_sums* out)
+{
+    if (!dom || !out) return fail(MRLBM_EINVAL, "null argument");
+    double* partial = dom->red_scratch;
+    double* res = dom->red_scratch + dom->red_blocks * 8;
+    mrlbm_status st = enqueue_reduce(dom, partial, res, 0, dom->stream);
+    if (st) return st;
+    CK(cudaMemcpyAsync(dom->red_host, res, 8 * sizeof(double), cudaMemcpyDeviceToHost, dom->stream));
+    CK(cudaStreamSynchronize(dom->stream));
+    const double* h = dom->red_host;
+    out->mass = h[0];
+    out->momentum[0] = h[1]; out->momentum[1] = h[2]; out->momentum[2] = h[3];
+    out->kinetic_energy = h[4];
+    out->fluid_nodes = h[5];
+    out->max_speed = h[6];
+    out->nonfinite = h[7];
+    return MRLBM_OK;
+}
+
+extern "C" mrlbm_status mrlbm_residual(mrlbm_domain* dom, double* residual)
+{
+    if (!dom || !residual) return fail(MRLBM_EINVAL, "null argument");
+    const size_t n = (size_t)dom->d.nx * dom->d.ny * dom->d.nz;
+    if (!dom->usnap) CK(cudaMalloc(&dom->usnap, 3 * n * sizeof(float)));
+    double* partial = dom->red_scratch;
+    double* res = dom->red_scratch + dom->red_blocks * 8;
+    const int mode = dom->have_snap ? 1 : 2;
+    mrlbm_status st = enqueue_reduce(dom, partial, res, mode, dom->stream);
+    if (st) return st;
+    CK(cudaMemcpyAsync(dom->red_host, res, 8 * sizeof(double), cudaMemcpyDeviceToHost, dom->stream));
+    CK(cudaStreamSynchronize(dom->stream));
+    if (mode == 2) {
+        dom->have_snap = true;
+        *residual = 1.0;
+    } else {
+        *residual = std::sqrt(dom->red_host[0]) / (std::sqrt(dom->red_host[1]) + 1e-30);
+    }
+    return MRLBM_OK;
+}

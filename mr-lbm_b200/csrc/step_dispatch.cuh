@@ -1,0 +1,47 @@
+// step_dispatch.cuh -- launch of the z-marching step kernel for one
+// (lattice, storage) pair; instantiated in step_q*_*.cu so the 36 kernel
+// variants compile in parallel translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "domain.h"
+#include "kernels.cuh"
+
+namespace mrlbm {
+
+template <int Q, typename T, int FLAGS>
+static mrlbm_status launch_step_t(const StepArgs& a, cudaStream_t s)
+{
+    constexpr int NW = TILE_Y + 2;
+    const size_t smem = 2u * lat_num_cy(Q) * NW * 32 * sizeof(float);
+    auto kern = zmarch_step<Q, T, FLAGS, TILE_Y>;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static int attr_done_mask = 0;  // one bit per device (up to 32)
+    if (!(attr_done_mask & (1 << (dev & 31)))) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return fail(MRLBM_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+        attr_done_mask |= 1 << (dev & 31);
+    }
+    dim3 grid((a.nx + TILE_X - 1) / TILE_X, (a.ny + TILE_Y - 1) / TILE_Y, (a.nz + a.lz - 1) / a.lz);
+    kern<<<grid, 32 * NW, smem, s>>>(a);
+    return MRLBM_OK;
+}
+
+template <int Q, typename T>
+mrlbm_status dispatch_step(const StepArgs& a, int flags, cudaStream_t s)
+{
+    switch (flags) {
+        case 0: return launch_step_t<Q, T, 0>(a, s);
+        case F_BC: return launch_step_t<Q, T, F_BC>(a, s);
+        case F_FORCE: return launch_step_t<Q, T, F_FORCE>(a, s);
+        case F_BC | F_FORCE: return launch_step_t<Q, T, F_BC | F_FORCE>(a, s);
+        case F_BC | F_POWERLAW: return launch_step_t<Q, T, F_BC | F_POWERLAW>(a, s);
+        case F_BC | F_FORCE | F_POWERLAW: return launch_step_t<Q, T, F_BC | F_FORCE | F_POWERLAW>(a, s);
+        case F_BC | F_BINGHAM: return launch_step_t<Q, T, F_BC | F_BINGHAM>(a, s);
+        case F_BC | F_FORCE | F_BINGHAM: return launch_step_t<Q, T, F_BC | F_FORCE | F_BINGHAM>(a, s);
+        default: return fail(MRLBM_EINVAL, "unsupported step flag combination %d", flags);
+    }
+}
+
+}  // namespace mrlbm

@@ -1,0 +1,347 @@
+"""ctypes binding of libmrlbm.so (the C ABI declared in include/mrlbm.h).
+
+This is the host-side mirror of the reference's case interface for Python
+callers (tests, bench, scripts).  It loads the in-tree CUDA library and fails
+loudly when it is missing; there is no CPU fallback.
+
+Arrays are numpy, x fastest: scalar fields have shape (nz, ny, nx); moment
+arrays have shape (nm, nz, ny, nx).
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmrlbm.so")
+
+D3Q19, D3Q27 = 19, 27
+F32, F16, BF16 = 0, 1, 2
+NEWTONIAN, POWERLAW, BINGHAM = 0, 1, 2
+
+NODE_BULK = 0x00
+NODE_SOLID = 0xFF
+BC_VELOCITY_WALL = 1 << 8
+
+
+def BC_VELOCITY_INDEX(k):
+    return (int(k) & 3) << 11
+
+
+# octant masks of the reference's nodeTypeMap (src/nodeTypeMap.h:10-44)
+WEST, EAST, SOUTH, NORTH, BACK, FRONT = 0x55, 0xAA, 0x33, 0xCC, 0x0F, 0xF0
+
+STATUS = {0: "OK", 1: "EINVAL", 2: "ENOMEM", 3: "ECUDA", 4: "EIO", 5: "EDIVERGED", 6: "ETIMEDOUT",
+          7: "ENOTFOUND", 8: "EBUSY"}
+
+
+class MrlbmError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("%s: %s" % (STATUS.get(status, status), msg))
+        self.status = status
+
+
+class Desc(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("lattice", C.c_int), ("storage", C.c_int),
+        ("periodic", C.c_int * 3),
+        ("tau", C.c_double), ("rho0", C.c_double),
+        ("force", C.c_double * 3),
+        ("bc_velocity", (C.c_double * 3) * 4),
+        ("rheology", C.c_int),
+        ("nnf_n", C.c_double), ("nnf_k", C.c_double),
+        ("nnf_yield", C.c_double), ("nnf_omega_p", C.c_double),
+        ("bc_matrix_q", C.c_int),
+        ("reserved", C.c_int * 7),
+    ]
+
+
+class Sums(C.Structure):
+    _fields_ = [("mass", C.c_double), ("momentum", C.c_double * 3), ("kinetic_energy", C.c_double),
+                ("fluid_nodes", C.c_double), ("max_speed", C.c_double), ("nonfinite", C.c_double)]
+
+    def as_dict(self):
+        return {"mass": self.mass, "momentum": tuple(self.momentum), "kinetic_energy": self.kinetic_energy,
+                "fluid_nodes": self.fluid_nodes, "max_speed": self.max_speed, "nonfinite": self.nonfinite}
+
+
+_lib = None
+FP = C.POINTER(C.c_float)
+VP = C.c_void_p
+
+
+def lib():
+    """Load libmrlbm.so; raises if it has not been built (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libmrlbm.so not built: run python mr-lbm_b200/build.py")
+        L = C.CDLL(LIB_PATH)
+        L.mrlbm_last_error.restype = C.c_char_p
+        L.mrlbm_version.restype = C.c_char_p
+        sigs = {
+            "mrlbm_set_device": [C.c_int],
+            "mrlbm_device_count": [C.POINTER(C.c_int)],
+            "mrlbm_host_alloc": [C.c_size_t, C.POINTER(VP)],
+            "mrlbm_host_free": [VP],
+            "mrlbm_domain_create": [C.POINTER(Desc), C.POINTER(VP)],
+            "mrlbm_domain_destroy": [VP],
+            "mrlbm_domain_bytes": [C.POINTER(Desc), C.POINTER(C.c_size_t)],
+            "mrlbm_set_node_types": [VP, C.POINTER(C.c_uint32)],
+            "mrlbm_init_flow": [VP, FP, FP, FP, FP],
+            "mrlbm_init_uniform": [VP, C.POINTER(C.c_double)],
+            "mrlbm_init_taylor_green": [VP, C.c_double, C.c_double],
+            "mrlbm_step": [VP, C.c_int],
+            "mrlbm_step_graph": [VP, C.c_int],
+            "mrlbm_time_steps": [VP, C.c_int, FP],
+            "mrlbm_synchronize": [VP],
+            "mrlbm_get_step": [VP, C.POINTER(C.c_int)],
+            "mrlbm_num_moments": [VP, C.POINTER(C.c_int)],
+            "mrlbm_get_moments_ref_layout": [VP, FP],
+            "mrlbm_set_moments_ref_layout": [VP, FP],
+            "mrlbm_get_moments": [VP, FP],
+            "mrlbm_set_moments": [VP, FP],
+            "mrlbm_get_macr": [VP, FP, FP, FP, FP, FP],
+            "mrlbm_reduce_fp64": [VP, C.POINTER(Sums)],
+            "mrlbm_residual": [VP, C.POINTER(C.c_double)],
+            "mrlbm_save_checkpoint": [VP, C.c_char_p, C.c_char_p, C.c_int],
+            "mrlbm_load_checkpoint": [VP, C.c_char_p, C.c_char_p, C.POINTER(C.c_int)],
+            "mrlbm_save_macr_bin": [VP, C.c_char_p, C.c_char_p, C.c_int],
+            "mrlbm_save_info": [VP, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, C.c_double],
+            "mrlbm_voxel_node_types": [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint8), C.POINTER(C.c_int),
+                                       C.POINTER(C.c_uint32)],
+            "mrlbm_lid_cavity_node_types": [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint32)],
+            "mrlbm_bc_class_info": [C.c_int, C.c_int, C.c_uint32, C.POINTER((C.c_double * 3) * 4), C.c_double,
+                                    FP, C.POINTER(C.c_uint32)],
+        }
+        for name, args in sigs.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def check(status):
+    if status != 0:
+        raise MrlbmError(status, lib().mrlbm_last_error().decode())
+
+
+def _fp(a):
+    return a.ctypes.data_as(FP)
+
+
+def set_device(dev):
+    check(lib().mrlbm_set_device(int(dev)))
+
+
+def device_count():
+    n = C.c_int()
+    check(lib().mrlbm_device_count(C.byref(n)))
+    return n.value
+
+
+class PinnedArray:
+    """numpy view over page-locked host memory from mrlbm_host_alloc."""
+
+    def __init__(self, shape, dtype=np.float32):
+        self.nbytes = int(np.prod(shape)) * np.dtype(dtype).itemsize
+        self.ptr = VP()
+        check(lib().mrlbm_host_alloc(self.nbytes, C.byref(self.ptr)))
+        buf = (C.c_char * self.nbytes).from_address(self.ptr.value)
+        self.array = np.frombuffer(buf, dtype=dtype).reshape(shape)
+
+    def free(self):
+        if self.ptr:
+            self.array = None
+            lib().mrlbm_host_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        self.free()
+
+
+def make_desc(nx, ny, nz, lattice=D3Q19, storage=F32, periodic=(1, 1, 1), tau=0.8, rho0=1.0,
+              force=(0.0, 0.0, 0.0), bc_velocity=None, rheology=NEWTONIAN, nnf_n=1.0, nnf_k=0.0,
+              nnf_yield=0.0, nnf_omega_p=0.0, bc_matrix_q=0):
+    d = Desc()
+    d.nx, d.ny, d.nz = nx, ny, nz
+    d.lattice, d.storage = lattice, storage
+    for a in range(3):
+        d.periodic[a] = int(periodic[a])
+        d.force[a] = float(force[a])
+    d.tau, d.rho0 = float(tau), float(rho0)
+    if bc_velocity is not None:
+        for k, v in enumerate(bc_velocity):
+            for a in range(3):
+                d.bc_velocity[k][a] = float(v[a])
+    d.rheology = rheology
+    d.nnf_n, d.nnf_k, d.nnf_yield, d.nnf_omega_p = nnf_n, nnf_k, nnf_yield, nnf_omega_p
+    d.bc_matrix_q = bc_matrix_q
+    return d
+
+
+def domain_bytes(desc):
+    n = C.c_size_t()
+    check(lib().mrlbm_domain_bytes(C.byref(desc), C.byref(n)))
+    return n.value
+
+
+class Domain:
+    """One MR-LBM domain resident on the current GPU."""
+
+    def __init__(self, desc):
+        self.L = lib()
+        self.desc = desc
+        h = VP()
+        check(self.L.mrlbm_domain_create(C.byref(desc), C.byref(h)))
+        self.h = h
+        nm = C.c_int()
+        check(self.L.mrlbm_num_moments(self.h, C.byref(nm)))
+        self.nm = nm.value
+        self.shape = (desc.nz, desc.ny, desc.nx)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.mrlbm_domain_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- setup
+    def set_node_types(self, nt):
+        nt = np.ascontiguousarray(nt, dtype=np.uint32)
+        assert nt.size == np.prod(self.shape)
+        check(self.L.mrlbm_set_node_types(self.h, nt.ctypes.data_as(C.POINTER(C.c_uint32))))
+
+    def init_flow(self, rho, ux, uy, uz):
+        a = [np.ascontiguousarray(v, dtype=np.float32).reshape(-1) for v in (rho, ux, uy, uz)]
+        check(self.L.mrlbm_init_flow(self.h, *[_fp(v) for v in a]))
+
+    def init_uniform(self, u0=(0.0, 0.0, 0.0)):
+        u = (C.c_double * 3)(*u0)
+        check(self.L.mrlbm_init_uniform(self.h, u))
+
+    def init_taylor_green(self, u0, L):
+        check(self.L.mrlbm_init_taylor_green(self.h, float(u0), float(L)))
+
+    # -- stepping
+    def step(self, n=1):
+        check(self.L.mrlbm_step(self.h, int(n)))
+
+    def step_graph(self, n):
+        check(self.L.mrlbm_step_graph(self.h, int(n)))
+
+    def time_steps(self, n):
+        ms = C.c_float()
+        check(self.L.mrlbm_time_steps(self.h, int(n), C.byref(ms)))
+        return ms.value
+
+    def synchronize(self):
+        check(self.L.mrlbm_synchronize(self.h))
+
+    @property
+    def step_count(self):
+        s = C.c_int()
+        check(self.L.mrlbm_get_step(self.h, C.byref(s)))
+        return s.value
+
+    # -- data
+    def moments(self):
+        m = np.empty((self.nm,) + self.shape, dtype=np.float32)
+        check(self.L.mrlbm_get_moments(self.h, _fp(m)))
+        return m
+
+    def set_moments(self, m):
+        m = np.ascontiguousarray(m, dtype=np.float32)
+        check(self.L.mrlbm_set_moments(self.h, _fp(m)))
+
+    def moments_ref_layout(self):
+        m = np.empty(self.nm * int(np.prod(self.shape)), dtype=np.float32)
+        check(self.L.mrlbm_get_moments_ref_layout(self.h, _fp(m)))
+        return m
+
+    def set_moments_ref_layout(self, m):
+        m = np.ascontiguousarray(m, dtype=np.float32)
+        check(self.L.mrlbm_set_moments_ref_layout(self.h, _fp(m)))
+
+    def macr(self):
+        out = [np.empty(self.shape, dtype=np.float32) for _ in range(4)]
+        check(self.L.mrlbm_get_macr(self.h, *[_fp(v) for v in out], None))
+        return out
+
+    def sums(self):
+        s = Sums()
+        check(self.L.mrlbm_reduce_fp64(self.h, C.byref(s)))
+        return s.as_dict()
+
+    def residual(self):
+        r = C.c_double()
+        check(self.L.mrlbm_residual(self.h, C.byref(r)))
+        return r.value
+
+    # -- files
+    def save_checkpoint(self, path, sim_id, step):
+        check(self.L.mrlbm_save_checkpoint(self.h, path.encode(), sim_id.encode(), int(step)))
+
+    def load_checkpoint(self, path, sim_id):
+        s = C.c_int()
+        check(self.L.mrlbm_load_checkpoint(self.h, path.encode(), sim_id.encode(), C.byref(s)))
+        return s.value
+
+    def save_macr_bin(self, path, sim_id, step):
+        check(self.L.mrlbm_save_macr_bin(self.h, path.encode(), sim_id.encode(), int(step)))
+
+    def save_info(self, path, sim_id, case_name, nsteps, mlups):
+        check(self.L.mrlbm_save_info(self.h, path.encode(), sim_id.encode(), case_name.encode(), int(nsteps),
+                                     float(mlups)))
+
+
+def bc_class_info(lattice, node_type, bc_velocity, omega0, bc_matrix_q=0):
+    """Host-built moment-BC data of one node type (see mrlbm_bc_class_info)."""
+    uv = ((C.c_double * 3) * 4)()
+    for k, v in enumerate(bc_velocity or []):
+        for a in range(3):
+            uv[k][a] = float(v[a])
+    out = np.zeros(67, dtype=np.float32)
+    known = C.c_uint32()
+    check(lib().mrlbm_bc_class_info(lattice, bc_matrix_q, int(node_type), C.byref(uv), float(omega0), _fp(out),
+                                    C.byref(known)))
+    return out, known.value
+
+
+def lid_cavity_node_types(nx, ny, nz, lid_velocity_index=1):
+    out = np.empty((nz, ny, nx), dtype=np.uint32)
+    check(lib().mrlbm_lid_cavity_node_types(nx, ny, nz, lid_velocity_index,
+                                           out.ctypes.data_as(C.POINTER(C.c_uint32))))
+    return out
+
+
+def voxel_node_types(solid, periodic):
+    solid = np.ascontiguousarray(solid, dtype=np.uint8)
+    nz, ny, nx = solid.shape
+    out = np.empty((nz, ny, nx), dtype=np.uint32)
+    per = (C.c_int * 3)(*[int(p) for p in periodic])
+    check(lib().mrlbm_voxel_node_types(nx, ny, nz, solid.ctypes.data_as(C.POINTER(C.c_uint8)), per,
+                                      out.ctypes.data_as(C.POINTER(C.c_uint32))))
+    return out
+
+
+def lid_cavity_desc(n, re=100.0, lid_u=0.05, storage=F32, lattice=D3Q19, ny=None, nz=None):
+    """The reference's lid-driven cavity constants (src/cases/lidDrivenCavity_3D/
+    constants.inc:35-36): nu = U * NX / Re, tau = 1/2 + 3 nu."""
+    nx = n
+    ny = ny or n
+    nz = nz or n
+    visc = lid_u * nx / re
+    tau = 0.5 + 3.0 * visc
+    return make_desc(nx, ny, nz, lattice=lattice, storage=storage, periodic=(0, 0, 0), tau=tau,
+                     bc_velocity=[(0, 0, 0), (lid_u, 0, 0), (0, 0, 0), (0, 0, 0)])

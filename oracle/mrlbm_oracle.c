@@ -1,0 +1,459 @@
+/*
+ * mrlbm_oracle.c -- TEST INFRASTRUCTURE ONLY.
+ *
+ * FP64 CPU restatement of the moment-representation LBM (MR-LBM) step of the
+ * reference solver, written from the method's equations.  It is the checker
+ * for the CUDA library (tests/, __graft_entry__.smoke() and bench.py's
+ * cpu_baseline leg use it) and is never linked into or called by the product.
+ *
+ * What it restates (reference file:line it follows):
+ *   - lattice ordering / weights      src/includeFiles/velocitySets/D3Q19.inc:8-24,
+ *                                     src/includeFiles/velocitySets/D3Q27.inc:9-28
+ *   - stored scaled moments           src/arrayIndex.h:8-17,186-187
+ *   - reconstruction                  src/colrec/MR_LBM/reconstruction.inc:1-35
+ *   - pull streaming (ghost exchange) src/mlbm.cu:388-454, src/includeFiles/popLoad.inc:1-86
+ *   - bulk moments + scaling          src/mlbm.cu:462-509
+ *   - moment-space BC (known set I)   src/cases/lidDrivenCavity_3D/bc_definition.inc:14-717,
+ *                                     src/cases/voxel/bc_definition.inc:16-7891
+ *     solved here as the linear system those closed forms come from:
+ *       sum_{i in I} f_i          = sum_{i in I} f^reg_i(rho, u, (1-w)Pi + w uu)
+ *       sum_{i in I} f_i h_k(c_i) = sum_{i in I} h_k(c_i) f^reg_i(rho, u, Pi)
+ *   - octant-mask known-set rule      src/lbmInitialization.cu:1080-1227, src/nodeTypeMap.h:10-80
+ *   - collision (with force terms)    src/colrec/MR_LBM/collision.inc:2-14
+ *   - shear magnitude + nnf omega     src/mlbm.cu:526-563, src/nnf.h:61-98
+ *     (power law with the reference's three compile defects fixed: the
+ *      POWERLAW/POWER_LAW guard, the undeclared `omega`, POW_FUNCTION = pow)
+ *   - initial moments                 src/lbmInitialization.cu:28-131
+ *   - kinetic energy                  src/reduction.cu:128-155, src/treatData.cu:105-165
+ *
+ * Parity pins: per-node functions are checked against the reference's own
+ * snippets compiled on the host (oracle/ref_kat.cpp -> oracle/_ref); full runs
+ * are checked against analytic solutions and against the reference CUDA build.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define ORC_MAXQ 27
+
+/* D3Q27 ordering; the first 19 entries are D3Q19 (same order as the reference). */
+static const int CX[27] = {0, 1,-1, 0, 0, 0, 0, 1,-1, 1,-1, 0, 0, 1,-1, 1,-1, 0, 0, 1,-1, 1,-1, 1,-1,-1, 1};
+static const int CY[27] = {0, 0, 0, 1,-1, 0, 0, 1,-1, 0, 0, 1,-1,-1, 1, 0, 0, 1,-1, 1,-1, 1,-1,-1, 1, 1,-1};
+static const int CZ[27] = {0, 0, 0, 0, 0, 1,-1, 0, 0, 1,-1, 1,-1, 0, 0,-1, 1,-1, 1, 1,-1,-1, 1, 1,-1, 1,-1};
+
+static double weight(int q, int i)
+{
+    int n = CX[i] * CX[i] + CY[i] * CY[i] + CZ[i] * CZ[i];
+    if (q == 19) {
+        static const double w19[3] = {1.0 / 3.0, 1.0 / 18.0, 1.0 / 36.0};
+        return w19[n];
+    }
+    static const double w27[4] = {8.0 / 27.0, 2.0 / 27.0, 1.0 / 54.0, 1.0 / 216.0};
+    return w27[n];
+}
+
+enum { ORC_NEWTONIAN = 0, ORC_POWERLAW = 1, ORC_BINGHAM = 2 };
+
+typedef struct {
+    int nx, ny, nz, q;
+    int periodic[3];
+    double tau, rho0;
+    double force[3];
+    double bc_velocity[4][3];
+    int rheology;          /* ORC_* */
+    double n_index, k_consistency, yield_stress, omega_p;
+    double exterior[10];   /* stored-moment state used for sources outside wall axes */
+    int bc_matrix_q;       /* lattice of the BC system matrix (19 or q) */
+} orc_desc;
+
+typedef struct {
+    orc_desc d;
+    int nm;                /* 10, or 11 with an omega field */
+    size_t n;
+    double *m, *m2;        /* [node][nm], node = x + nx*(y + ny*z) */
+    uint32_t *type;        /* reference nodeTypeMap words, same node order */
+    double *pop;           /* [node][q] post-collision populations scratch */
+} orc_domain;
+
+/* ----------------------------------------------------------------- per node */
+
+/* f_i = rho w_i [1 - cs2 tr(m2) + c.u3 + sum c_a^2 m_aa + sum c_a c_b m_ab]
+ * with m in the stored scaled form (reconstruction.inc:1-35). */
+void orc_reconstruct(int q, double rho0, const double *m, double *f)
+{
+    double rho = rho0 + m[0];
+    double ux = m[1], uy = m[2], uz = m[3];
+    double mxx = m[4], mxy = m[5], mxz = m[6], myy = m[7], myz = m[8], mzz = m[9];
+    double pics2 = 1.0 - (mxx + myy + mzz) / 3.0;
+    for (int i = 0; i < q; i++) {
+        double cx = CX[i], cy = CY[i], cz = CZ[i];
+        double t = pics2 + cx * ux + cy * uy + cz * uz + cx * cx * mxx + cy * cy * myy + cz * cz * mzz
+                 + cx * cy * mxy + cx * cz * mxz + cy * cz * myz;
+        f[i] = rho * weight(q, i) * t;
+    }
+}
+
+/* Bulk macroscopics, unscaled: rho, u, Pi_hat = sum f cc / rho - cs2 delta (mlbm.cu:462-497). */
+void orc_bulk_moments(int q, const double *f, double *out /* rho,ux,uy,uz,pxx,pxy,pxz,pyy,pyz,pzz */)
+{
+    double r = 0, jx = 0, jy = 0, jz = 0, pxx = 0, pxy = 0, pxz = 0, pyy = 0, pyz = 0, pzz = 0;
+    for (int i = 0; i < q; i++) {
+        double cx = CX[i], cy = CY[i], cz = CZ[i], v = f[i];
+        r += v;
+        jx += v * cx; jy += v * cy; jz += v * cz;
+        pxx += v * cx * cx; pxy += v * cx * cy; pxz += v * cx * cz;
+        pyy += v * cy * cy; pyz += v * cy * cz; pzz += v * cz * cz;
+    }
+    double ir = 1.0 / r;
+    out[0] = r;
+    out[1] = jx * ir; out[2] = jy * ir; out[3] = jz * ir;
+    out[4] = pxx * ir - 1.0 / 3.0; out[5] = pxy * ir; out[6] = pxz * ir;
+    out[7] = pyy * ir - 1.0 / 3.0; out[8] = pyz * ir; out[9] = pzz * ir - 1.0 / 3.0;
+}
+
+/* Known-set rule for the octant mask (low 8 bits of the node type):
+ * octant o = ox + 2*oy + 4*oz (o_a = 1 is the + side).  The source x - c_i is
+ * treated as solid when every octant consistent with the offset -c_i is marked
+ * (this is how bc_id marks a solid neighbour, lbmInitialization.cu:1080-1227). */
+uint32_t orc_known_mask(int q, uint32_t octants)
+{
+    uint32_t known = 0;
+    for (int i = 0; i < q; i++) {
+        int d[3] = {-CX[i], -CY[i], -CZ[i]};
+        int all = 1;
+        for (int o = 0; o < 8; o++) {
+            int s[3] = {(o & 1) ? 1 : -1, (o & 2) ? 1 : -1, (o & 4) ? 1 : -1};
+            int consistent = 1;
+            for (int a = 0; a < 3; a++)
+                if (d[a] != 0 && d[a] != s[a]) consistent = 0;
+            if (consistent && !((octants >> o) & 1u)) { all = 0; break; }
+        }
+        if (!all) known |= (1u << i);
+    }
+    return known;
+}
+
+static void h_vec(int i, double *h)
+{
+    double cx = CX[i], cy = CY[i], cz = CZ[i];
+    h[0] = cx * cx - 1.0 / 3.0; h[1] = cx * cy; h[2] = cx * cz;
+    h[3] = cy * cy - 1.0 / 3.0; h[4] = cy * cz; h[5] = cz * cz - 1.0 / 3.0;
+}
+
+/* coefficient of Pi_k inside 4.5 * H_i : Pi  (off-diagonals counted twice) */
+static void g_vec(int i, double *g)
+{
+    double cx = CX[i], cy = CY[i], cz = CZ[i];
+    g[0] = 4.5 * (cx * cx - 1.0 / 3.0); g[1] = 9.0 * cx * cy; g[2] = 9.0 * cx * cz;
+    g[3] = 4.5 * (cy * cy - 1.0 / 3.0); g[4] = 9.0 * cy * cz; g[5] = 4.5 * (cz * cz - 1.0 / 3.0);
+}
+
+static int solve7(double A[7][7], double *b, double *x)
+{
+    int p[7];
+    for (int i = 0; i < 7; i++) p[i] = i;
+    for (int c = 0; c < 7; c++) {
+        int best = c;
+        for (int r = c + 1; r < 7; r++)
+            if (fabs(A[p[r]][c]) > fabs(A[p[best]][c])) best = r;
+        int t = p[c]; p[c] = p[best]; p[best] = t;
+        double piv = A[p[c]][c];
+        if (fabs(piv) < 1e-300) return -1;
+        for (int r = c + 1; r < 7; r++) {
+            double f = A[p[r]][c] / piv;
+            if (f == 0.0) continue;
+            for (int k = c; k < 7; k++) A[p[r]][k] -= f * A[p[c]][k];
+            b[p[r]] -= f * b[p[c]];
+        }
+    }
+    for (int c = 6; c >= 0; c--) {
+        double s = b[p[c]];
+        for (int k = c + 1; k < 7; k++) s -= A[p[c]][k] * x[k];
+        x[c] = s / A[p[c]][c];
+    }
+    return 0;
+}
+
+/* Moment-based wall BC.  Inputs: post-stream pops f (only `known` entries are
+ * read), prescribed velocity u (unscaled), omega.  Output: rho and the
+ * unscaled Pi_hat (xx,xy,xz,yy,yz,zz) -> out[0], out[4..9]; out[1..3] = u.
+ * The right-hand side sums the known pops of the q-velocity lattice; the
+ * system matrix is assembled over the first mq velocities (mq = 19 on a
+ * D3Q27 lattice reproduces the reference's D3Q27 wall formulas, which are the
+ * D3Q19 closed forms fed with D3Q27 known-set moments,
+ * src/cases/parallelPlates_D3Q27/bc_definition.inc:18-44). */
+int orc_bc_solve(int q, int mq, uint32_t known, const double *u, double omega, const double *f, double *out)
+{
+    double A[7][7], b[7], x[7];
+    memset(A, 0, sizeof(A));
+    memset(b, 0, sizeof(b));
+    double uu[6] = {u[0] * u[0], u[0] * u[1], u[0] * u[2], u[1] * u[1], u[1] * u[2], u[2] * u[2]};
+    for (int i = 0; i < q; i++) {
+        if (!((known >> i) & 1u)) continue;
+        double h[6], g[6];
+        h_vec(i, h);
+        b[0] += f[i];
+        for (int r = 0; r < 6; r++) b[1 + r] += f[i] * h[r];
+    }
+    for (int i = 0; i < mq; i++) {
+        if (!((known >> i) & 1u)) continue;
+        double w = weight(mq, i), h[6], g[6];
+        h_vec(i, h);
+        g_vec(i, g);
+        double cu = 3.0 * (CX[i] * u[0] + CY[i] * u[1] + CZ[i] * u[2]);
+        double guu = 0.0;
+        for (int k = 0; k < 6; k++) guu += g[k] * uu[k];
+        /* row 0: sum_I f^reg(rho, u, (1-w)Pi + w uu) */
+        A[0][0] += w * (1.0 + cu + omega * guu);
+        for (int k = 0; k < 6; k++) A[0][1 + k] += (1.0 - omega) * w * g[k];
+        /* rows 1..6: sum_I h_k f^reg(rho, u, Pi) */
+        for (int r = 0; r < 6; r++) {
+            A[1 + r][0] += w * h[r] * (1.0 + cu);
+            for (int k = 0; k < 6; k++) A[1 + r][1 + k] += w * h[r] * g[k];
+        }
+    }
+    if (solve7(A, b, x) != 0) return -1;
+    out[0] = x[0];
+    out[1] = u[0]; out[2] = u[1]; out[3] = u[2];
+    for (int k = 0; k < 6; k++) out[4 + k] = x[1 + k] / x[0];
+    return 0;
+}
+
+/* Power-law omega by Newton iteration (nnf.h:61-89), defects fixed. */
+double orc_nnf_powerlaw(double omega_old, double smag, double n_index, double k_cons, double rho0)
+{
+    double omega = omega_old;
+    double a = k_cons * pow(smag / (rho0 / 3.0), n_index);
+    double b = 0.5 * smag, c = -smag;
+    if (smag < 1e-6) return 0.0;
+    for (int it = 0; it < 7; it++) {
+        double fx = a * pow(omega, n_index) + b * omega + c;
+        double dfx = a * n_index * pow(omega, n_index - 1.0) + b;
+        if (fabs(fx / dfx) < 1e-6) break;
+        omega = omega - fx / dfx;
+    }
+    return omega;
+}
+
+double orc_nnf_bingham(double smag, double omega_p, double yield_stress)
+{
+    double v = 1.0 - yield_stress / smag;
+    return omega_p * (v > 0.0 ? v : 0.0);
+}
+
+/* Scale, (shear, nnf), collide.  mac = rho,u,Pi unscaled in/out; m = stored
+ * scaled moments out (nm entries).  Follows mlbm.cu:500-591 + collision.inc. */
+static void collide_store(const orc_desc *d, int nm, const double *mac, double omega_in, double *m)
+{
+    double rho = mac[0];
+    double ux = 3.0 * mac[1], uy = 3.0 * mac[2], uz = 3.0 * mac[3];
+    double mxx = 4.5 * mac[4], mxy = 9.0 * mac[5], mxz = 9.0 * mac[6];
+    double myy = 4.5 * mac[7], myz = 9.0 * mac[8], mzz = 4.5 * mac[9];
+    double Fx = d->force[0], Fy = d->force[1], Fz = d->force[2];
+    double omega = omega_in;
+    if (d->rheology != ORC_NEWTONIAN) {
+        double sxx = rho * (mxx / 4.5 - ux * ux / 9.0), syy = rho * (myy / 4.5 - uy * uy / 9.0);
+        double szz = rho * (mzz / 4.5 - uz * uz / 9.0), sxy = rho * (mxy / 9.0 - ux * uy / 9.0);
+        double sxz = rho * (mxz / 9.0 - ux * uz / 9.0), syz = rho * (myz / 9.0 - uy * uz / 9.0);
+        double fxx = ux * Fx / 3.0, fyy = uy * Fy / 3.0, fzz = uz * Fz / 3.0;
+        double fxy = (ux * Fy + uy * Fx) / 6.0, fxz = (ux * Fz + uz * Fx) / 6.0, fyz = (uy * Fz + uz * Fy) / 6.0;
+        double smag = sqrt(0.5 * ((sxx + fxx) * (sxx + fxx) + (syy + fyy) * (syy + fyy) + (szz + fzz) * (szz + fzz)
+                                  + 2.0 * ((sxy + fxy) * (sxy + fxy) + (sxz + fxz) * (sxz + fxz) + (syz + fyz) * (syz + fyz))));
+        if (d->rheology == ORC_POWERLAW)
+            omega = orc_nnf_powerlaw(omega_in, smag, d->n_index, d->k_consistency, d->rho0);
+        else
+            omega = orc_nnf_bingham(smag, d->omega_p, d->yield_stress);
+    }
+    double ir = 1.0 / rho;
+    double t_om = 1.0 - omega, tt_om = 1.0 - 0.5 * omega, om_d2 = 0.5 * omega, tt_om_t3 = 3.0 * tt_om;
+    ux += 3.0 * ir * Fx; uy += 3.0 * ir * Fy; uz += 3.0 * ir * Fz;
+    double ir15 = 1.5 * ir;
+    mxx = t_om * mxx + om_d2 * ux * ux + ir15 * tt_om * (2.0 * Fx * ux);
+    myy = t_om * myy + om_d2 * uy * uy + ir15 * tt_om * (2.0 * Fy * uy);
+    mzz = t_om * mzz + om_d2 * uz * uz + ir15 * tt_om * (2.0 * Fz * uz);
+    mxy = t_om * mxy + omega * ux * uy + tt_om_t3 * ir * (Fx * uy + Fy * ux);
+    mxz = t_om * mxz + omega * ux * uz + tt_om_t3 * ir * (Fx * uz + Fz * ux);
+    myz = t_om * myz + omega * uy * uz + tt_om_t3 * ir * (Fy * uz + Fz * uy);
+    m[0] = rho - d->rho0;
+    m[1] = ux; m[2] = uy; m[3] = uz;
+    m[4] = mxx; m[5] = mxy; m[6] = mxz; m[7] = myy; m[8] = myz; m[9] = mzz;
+    if (nm > 10) m[10] = omega;
+}
+
+/* exposed for KATs: unscaled macroscopics + omega -> stored post-collision moments */
+void orc_collide(const orc_desc *d, const double *mac, double omega, double *m_out, int nm)
+{
+    collide_store(d, nm, mac, omega, m_out);
+}
+
+/* ------------------------------------------------------------------ domain */
+
+void *orc_create(const orc_desc *d)
+{
+    orc_domain *o = (orc_domain *)calloc(1, sizeof(orc_domain));
+    if (!o) return NULL;
+    o->d = *d;
+    o->nm = (d->rheology != ORC_NEWTONIAN) ? 11 : 10;
+    o->n = (size_t)d->nx * d->ny * d->nz;
+    o->m = (double *)calloc(o->n * o->nm, sizeof(double));
+    o->m2 = (double *)calloc(o->n * o->nm, sizeof(double));
+    o->type = (uint32_t *)calloc(o->n, sizeof(uint32_t));
+    o->pop = (double *)malloc(o->n * d->q * sizeof(double));
+    if (!o->m || !o->m2 || !o->type || !o->pop) {
+        free(o->m); free(o->m2); free(o->type); free(o->pop); free(o);
+        return NULL;
+    }
+    return o;
+}
+
+void orc_destroy(void *h)
+{
+    orc_domain *o = (orc_domain *)h;
+    if (!o) return;
+    free(o->m); free(o->m2); free(o->type); free(o->pop); free(o);
+}
+
+int orc_num_moments(void *h) { return ((orc_domain *)h)->nm; }
+
+void orc_set_node_types(void *h, const uint32_t *t)
+{
+    orc_domain *o = (orc_domain *)h;
+    memcpy(o->type, t, o->n * sizeof(uint32_t));
+}
+
+void orc_set_moments(void *h, const double *m)
+{
+    orc_domain *o = (orc_domain *)h;
+    memcpy(o->m, m, o->n * o->nm * sizeof(double));
+    memcpy(o->m2, m, o->n * o->nm * sizeof(double));
+}
+
+void orc_get_moments(void *h, double *m)
+{
+    orc_domain *o = (orc_domain *)h;
+    memcpy(m, o->m, o->n * o->nm * sizeof(double));
+}
+
+/* Initial moments from physical rho,u (x-fastest) exactly as
+ * gpuInitialization_mom (lbmInitialization.cu:28-131): the second moments are
+ * built from an equilibrium with weight*RHO_0 and the D3Q19 index sums even for
+ * D3Q27 (when d3q19_sums != 0; 0 uses the full lattice sums). */
+void orc_init_from_macro(void *h, const double *rho, const double *ux, const double *uy, const double *uz,
+                         int d3q19_sums)
+{
+    orc_domain *o = (orc_domain *)h;
+    int q = o->d.q, qs = d3q19_sums ? 19 : q;
+    double omega = 1.0 / o->d.tau;
+    for (size_t k = 0; k < o->n; k++) {
+        double f[ORC_MAXQ];
+        double u[3] = {ux[k], uy[k], uz[k]};
+        double uu = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+        for (int i = 0; i < q; i++) {
+            double uc3 = 3.0 * (u[0] * CX[i] + u[1] * CY[i] + u[2] * CZ[i]);
+            f[i] = weight(q, i) * o->d.rho0 * ((1.0 - 1.5 * uu) + uc3 * (1.0 + 0.5 * uc3));
+        }
+        double ir = 1.0 / rho[k], p[6] = {0, 0, 0, 0, 0, 0};
+        for (int i = 0; i < qs; i++) {
+            double cx = CX[i], cy = CY[i], cz = CZ[i];
+            p[0] += f[i] * cx * cx; p[1] += f[i] * cx * cy; p[2] += f[i] * cx * cz;
+            p[3] += f[i] * cy * cy; p[4] += f[i] * cy * cz; p[5] += f[i] * cz * cz;
+        }
+        double *m = o->m + k * o->nm;
+        m[0] = rho[k] - o->d.rho0;
+        m[1] = 3.0 * u[0]; m[2] = 3.0 * u[1]; m[3] = 3.0 * u[2];
+        m[4] = 4.5 * (p[0] * ir - 1.0 / 3.0);
+        m[5] = 9.0 * (p[1] * ir);
+        m[6] = 9.0 * (p[2] * ir);
+        m[7] = 4.5 * (p[3] * ir - 1.0 / 3.0);
+        m[8] = 9.0 * (p[4] * ir);
+        m[9] = 4.5 * (p[5] * ir - 1.0 / 3.0);
+        if (o->nm > 10) m[10] = omega;
+    }
+    memcpy(o->m2, o->m, o->n * o->nm * sizeof(double));
+}
+
+static inline int resolve(int v, int n, int periodic, int *outside)
+{
+    if (v >= 0 && v < n) return v;
+    if (periodic) return (v + n) % n;
+    *outside = 1;
+    return 0;
+}
+
+void orc_step(void *h, int nsteps)
+{
+    orc_domain *o = (orc_domain *)h;
+    const orc_desc *d = &o->d;
+    const int q = d->q, nm = o->nm, nx = d->nx, ny = d->ny, nz = d->nz;
+    const double omega0 = 1.0 / d->tau;
+    double fext[ORC_MAXQ];
+    orc_reconstruct(q, d->rho0, d->exterior, fext);
+    for (int s = 0; s < nsteps; s++) {
+        /* post-collision populations of every node, from its stored moments */
+#pragma omp parallel for schedule(static)
+        for (long k = 0; k < (long)o->n; k++) orc_reconstruct(q, d->rho0, o->m + k * nm, o->pop + k * q);
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int z = 0; z < nz; z++)
+            for (int y = 0; y < ny; y++)
+                for (int x = 0; x < nx; x++) {
+                    size_t k = (size_t)x + (size_t)nx * (y + (size_t)ny * z);
+                    uint32_t t = o->type[k];
+                    double *mo = o->m2 + k * nm;
+                    const double *mi = o->m + k * nm;
+                    if ((t & 0xFFu) == 0xFFu) { memcpy(mo, mi, nm * sizeof(double)); continue; }
+                    double f[ORC_MAXQ];
+                    for (int i = 0; i < q; i++) {
+                        int out = 0;
+                        int sx = resolve(x - CX[i], nx, d->periodic[0], &out);
+                        int sy = resolve(y - CY[i], ny, d->periodic[1], &out);
+                        int sz = resolve(z - CZ[i], nz, d->periodic[2], &out);
+                        f[i] = out ? fext[i] : o->pop[((size_t)sx + (size_t)nx * (sy + (size_t)ny * sz)) * q + i];
+                    }
+                    double omega = (nm > 10) ? mi[10] : omega0;
+                    double mac[10];
+                    if ((t & 0xFFu) == 0) {
+                        orc_bulk_moments(q, f, mac);
+                    } else {
+                        int vidx = (t >> 11) & 3u;
+                        int kind = (t >> 8) & 7u;
+                        double u[3] = {0, 0, 0};
+                        if (kind == 1) { u[0] = d->bc_velocity[vidx][0]; u[1] = d->bc_velocity[vidx][1]; u[2] = d->bc_velocity[vidx][2]; }
+                        orc_bc_solve(q, d->bc_matrix_q ? d->bc_matrix_q : q, orc_known_mask(q, t & 0xFFu), u, omega, f, mac);
+                    }
+                    collide_store(d, nm, mac, omega, mo);
+                }
+        double *tmp = o->m; o->m = o->m2; o->m2 = tmp;
+    }
+}
+
+/* FP64 sums over non-solid nodes: [0] sum rho, [1..3] sum rho u, [4] sum KE
+ * where KE per node = rho |u|^2 / 2 (reduction.cu:145 uses (rho0+m0)|3u|^2/18),
+ * [5] fluid node count. */
+void orc_sums(void *h, double *out)
+{
+    orc_domain *o = (orc_domain *)h;
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    for (size_t k = 0; k < o->n; k++) {
+        if ((o->type[k] & 0xFFu) == 0xFFu) continue;
+        const double *m = o->m + k * o->nm;
+        double rho = o->d.rho0 + m[0];
+        double ux = m[1] / 3.0, uy = m[2] / 3.0, uz = m[3] / 3.0;
+        s[0] += rho; s[1] += rho * ux; s[2] += rho * uy; s[3] += rho * uz;
+        s[4] += 0.5 * rho * (ux * ux + uy * uy + uz * uz);
+        s[5] += 1.0;
+    }
+    memcpy(out, s, sizeof(s));
+}
+
+int orc_threads(void)
+{
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}

@@ -1,0 +1,142 @@
+"""C-ABI library on the CPU: it loads, exports every declared symbol, and its
+host-side logic (node-type builders, moment-BC matrices) matches the oracle.
+No device work is done here."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import lattice_np
+import oracle_ffi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _lib():
+    import mrlbm
+    return mrlbm
+
+
+def declared_symbols():
+    txt = open(os.path.join(ROOT, "include", "mrlbm.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(mrlbm_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol():
+    mrlbm = _lib()
+    L = mrlbm.lib()
+    names = declared_symbols()
+    assert len(names) >= 29
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    assert b"sm_100a" in L.mrlbm_version()
+
+
+def test_lid_cavity_typing_matches_reference_rules():
+    mrlbm = _lib()
+    nx, ny, nz = 10, 9, 8
+    t = mrlbm.lid_cavity_node_types(nx, ny, nz, 1)
+    F = lattice_np.FACES
+    lid = F["NORTH"] | mrlbm.BC_VELOCITY_WALL | mrlbm.BC_VELOCITY_INDEX(1)
+    # restatement of src/cases/lidDrivenCavity_3D/bc_initialization.inc
+    for z in range(nz):
+        for y in range(ny):
+            for x in range(nx):
+                if y == ny - 1:
+                    want = lid
+                else:
+                    want = 0
+                    if y == 0: want |= F["SOUTH"]
+                    if x == 0: want |= F["WEST"]
+                    if x == nx - 1: want |= F["EAST"]
+                    if z == 0: want |= F["BACK"]
+                    if z == nz - 1: want |= F["FRONT"]
+                assert t[z, y, x] == want, (x, y, z)
+    # corner masks equal the reference's named constants
+    assert t[0, 0, 0] == 0b01111111           # SOUTH_WEST_BACK
+    assert t[nz - 1, 0, nx - 1] == 0b11111011  # SOUTH_EAST_FRONT
+
+
+def bc_id_restated(solid, x, y, z):
+    """Octant marking of src/lbmInitialization.cu:1080-1227 (periodic wrap)."""
+    nz, ny, nx = solid.shape
+    m = 0
+    for dz in (-1, 0, 1):
+        for dy in (-1, 0, 1):
+            for dx in (-1, 0, 1):
+                if not (dx or dy or dz):
+                    continue
+                if solid[(z + dz) % nz, (y + dy) % ny, (x + dx) % nx]:
+                    for o in range(8):
+                        s = ((1 if o & 1 else -1), (1 if o & 2 else -1), (1 if o & 4 else -1))
+                        if all(d == 0 or d == sv for d, sv in zip((dx, dy, dz), s)):
+                            m |= 1 << o
+    return m
+
+
+def test_voxel_typing_matches_bc_id():
+    mrlbm = _lib()
+    rng = np.random.default_rng(3)
+    solid = (rng.random((7, 8, 9)) < 0.15).astype(np.uint8)
+    t = mrlbm.voxel_node_types(solid, (1, 1, 1))
+    for z in range(7):
+        for y in range(8):
+            for x in range(9):
+                if solid[z, y, x]:
+                    assert t[z, y, x] == 0xFF
+                else:
+                    want = bc_id_restated(solid, x, y, z)
+                    assert t[z, y, x] == (0xFE if want == 0xFF else want)
+
+
+def test_voxel_typing_walls_on_nonperiodic_axes():
+    mrlbm = _lib()
+    solid = np.zeros((6, 5, 4), dtype=np.uint8)
+    t = mrlbm.voxel_node_types(solid, (0, 0, 1))
+    F = lattice_np.FACES
+    assert t[2, 0, 2] == F["SOUTH"]
+    assert t[2, 0, 0] == F["SOUTH"] | F["WEST"]
+    assert t[2, 2, 3] == F["EAST"]
+    assert t[2, 2, 2] == 0
+
+
+@pytest.mark.parametrize("lattice,mq", [(19, 19), (27, 19), (27, 27)])
+def test_bc_matrices_match_oracle(lattice, mq):
+    """The Sherman-Morrison form the kernel evaluates equals the oracle's
+    direct 7x7 solve, for omegas away from the expansion point."""
+    mrlbm = _lib()
+    L = oracle_ffi.lib()
+    P = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
+    rng = np.random.default_rng(11)
+    omega0 = 1.0 / 0.596
+    uvel = [(0, 0, 0), (0.05, 0.0, 0.0), (0.0, 0.01, -0.02), (0, 0, 0)]
+    types = list(lattice_np.wall_types().values()) + [0x13, 0x80, 0xC3]
+    for t in types:
+        for vel in (0, 1, 2):
+            word = t | (mrlbm.BC_VELOCITY_WALL | mrlbm.BC_VELOCITY_INDEX(vel) if vel else 0)
+            data, known = mrlbm.bc_class_info(lattice, word, uvel, omega0, bc_matrix_q=mq)
+            assert known == L.orc_known_mask(lattice, t)
+            Ainv = data[:49].reshape(7, 7).astype(np.float64)
+            v, qa, s = data[49:56], data[56:63], data[63]
+            m = rng.normal(0, 0.05, 10)
+            f = np.zeros(lattice)
+            L.orc_reconstruct(lattice, 1.0, P(m), P(f))
+            f *= 1 + rng.normal(0, 1e-3, lattice)
+            kb = np.array([(known >> i) & 1 for i in range(lattice)], dtype=bool)
+            fk = np.where(kb, f, 0.0)
+            cx, cy, cz = lattice_np.CX[:lattice], lattice_np.CY[:lattice], lattice_np.CZ[:lattice]
+            b0 = fk.sum()
+            b = np.array([b0, (fk * cx * cx).sum() - b0 / 3, (fk * cx * cy).sum(), (fk * cx * cz).sum(),
+                          (fk * cy * cy).sum() - b0 / 3, (fk * cy * cz).sum(), (fk * cz * cz).sum() - b0 / 3])
+            u = np.array(uvel[vel] if vel else (0, 0, 0), dtype=np.float64)
+            for om in (omega0, 0.9, 1.4, 1.9):
+                X = Ainv @ b
+                dw = om - omega0
+                X = X - v * (dw * (qa @ b) / (1 + dw * s))
+                ref = np.zeros(10)
+                assert L.orc_bc_solve(lattice, mq, known, P(u), om, P(f), P(ref)) == 0
+                np.testing.assert_allclose(X[0], ref[0], rtol=2e-6)
+                np.testing.assert_allclose(X[1:] / X[0], ref[4:], rtol=2e-4, atol=2e-7)

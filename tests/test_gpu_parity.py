@@ -1,0 +1,171 @@
+"""CUDA fused step vs the FP64 oracle, through the C ABI (libmrlbm.so).
+
+Tolerances (FP32 storage and arithmetic against FP64): per-moment relative
+L2 <= 2e-5 and relative Linf <= 2e-4 after the stated number of steps, unless
+a test states otherwise.  Both sides start from the same stored moments (the
+GPU's own initial state copied into the oracle), so the comparison isolates
+the step.
+"""
+import numpy as np
+import pytest
+
+import mrlbm
+import parity_util as pu
+
+pytestmark = pytest.mark.gpu
+
+TOL_L2, TOL_LINF = 2e-5, 2e-4
+
+
+def run_pair(desc, steps, node_types=None, init=None, fluid=None):
+    dom = mrlbm.Domain(desc)
+    if node_types is not None:
+        dom.set_node_types(node_types)
+    if init is None:
+        dom.init_uniform()
+    else:
+        init(dom)
+    m0 = dom.moments()
+    orc = pu.oracle_for(desc, node_types)
+    orc.set_moments(pu.gpu_to_oracle_layout(m0))
+    dom.step(steps)
+    orc.step(steps)
+    g = dom.moments()
+    o = orc.moments()
+    dom.close()
+    return g, o, pu.compare(g, o, fluid)
+
+
+def assert_close(res, l2=TOL_L2, linf=TOL_LINF, skip=()):
+    for k, (e2, einf) in res.items():
+        if k in skip:
+            continue
+        assert e2 <= l2 and einf <= linf, "moment %d: rel L2 %.3e, rel Linf %.3e" % (k, e2, einf)
+
+
+def tg_init(u0, L):
+    return lambda dom: dom.init_taylor_green(u0, L)
+
+
+@pytest.mark.parametrize("lattice", [19, 27])
+def test_taylor_green_periodic(lattice):
+    n = 32
+    d = mrlbm.make_desc(n, n, n, lattice=lattice, tau=0.55)
+    g, o, res = run_pair(d, 40, init=tg_init(0.04, n / (2 * np.pi)))
+    assert_close(res)
+
+
+def test_random_field_partial_tiles():
+    """Sizes that are not multiples of the 30 x 14 x LZ tile, random initial field."""
+    nx, ny, nz = 37, 29, 23
+    d = mrlbm.make_desc(nx, ny, nz, lattice=19, tau=0.7)
+    rng = np.random.default_rng(5)
+    rho = 1 + 0.01 * rng.standard_normal((nz, ny, nx))
+    u = 0.02 * rng.standard_normal((3, nz, ny, nx))
+    g, o, res = run_pair(d, 25, init=lambda dom: dom.init_flow(rho, u[0], u[1], u[2]))
+    assert_close(res)
+
+
+@pytest.mark.parametrize("lattice", [19, 27])
+def test_lid_cavity(lattice):
+    nx, ny, nz = 24, 20, 16
+    d = mrlbm.lid_cavity_desc(nx, re=100.0, lid_u=0.05, lattice=lattice, ny=ny, nz=nz)
+    nt = mrlbm.lid_cavity_node_types(nx, ny, nz, 1)
+    g, o, res = run_pair(d, 300, node_types=nt)
+    assert_close(res, l2=5e-5, linf=5e-4)
+
+
+def test_duct_voxels_force_powerlaw():
+    nx, ny, nz = 20, 18, 24
+    rng = np.random.default_rng(9)
+    solid = np.zeros((nz, ny, nx), dtype=np.uint8)
+    solid[:, 1:-1, 1:-1] = rng.random((nz, ny - 2, nx - 2)) < 0.05
+    nt = mrlbm.voxel_node_types(solid, (0, 0, 1))
+    d = mrlbm.make_desc(nx, ny, nz, lattice=19, periodic=(0, 0, 1), tau=0.8, force=(0, 0, 2e-5),
+                        rheology=mrlbm.POWERLAW, nnf_n=0.8)
+    g, o, res = run_pair(d, 150, node_types=nt, fluid=solid == 0)
+    assert_close(res, l2=2e-4, linf=2e-3)
+
+
+def test_bingham_plates():
+    nx, ny, nz = 16, 22, 16
+    solid = np.zeros((nz, ny, nx), dtype=np.uint8)
+    nt = mrlbm.voxel_node_types(solid, (1, 0, 1))
+    d = mrlbm.make_desc(nx, ny, nz, lattice=19, periodic=(1, 0, 1), tau=0.9, force=(5e-5, 0, 0),
+                        rheology=mrlbm.BINGHAM, nnf_yield=1e-5)
+    g, o, res = run_pair(d, 150, node_types=nt)
+    assert_close(res, l2=2e-4, linf=2e-3)
+
+
+@pytest.mark.parametrize("storage,tol", [(mrlbm.F16, 5e-3), (mrlbm.BF16, 4e-2)])
+def test_half_storage_taylor_green(storage, tol):
+    """16-bit storage, FP32 arithmetic: velocity error vs FP64 stays bounded."""
+    n = 32
+    d = mrlbm.make_desc(n, n, n, lattice=27, storage=storage, tau=0.55)
+    g, o, res = run_pair(d, 40, init=tg_init(0.04, n / (2 * np.pi)))
+    err = pu.velocity_rel_l2(g, o)
+    assert err < tol, err
+
+
+def test_graph_equals_eager():
+    n = 24
+    d = mrlbm.make_desc(n, n, n, lattice=19, tau=0.6)
+    a = mrlbm.Domain(d)
+    b = mrlbm.Domain(d)
+    for dom in (a, b):
+        dom.init_taylor_green(0.05, n / (2 * np.pi))
+    a.step(37)
+    b.step_graph(37)
+    assert b.step_count == 37
+    np.testing.assert_array_equal(a.moments(), b.moments())
+
+
+def test_reference_layout_roundtrip():
+    nx, ny, nz = 16, 24, 8
+    d = mrlbm.make_desc(nx, ny, nz, lattice=19)
+    dom = mrlbm.Domain(d)
+    rng = np.random.default_rng(1)
+    m = rng.standard_normal((10, nz, ny, nx)).astype(np.float32) * 0.01
+    dom.set_moments(m)
+    ref = dom.moments_ref_layout()
+    # idxMom = tx + 8(ty + 8(tz + 8(mom + NM(bx + NBX(by + NBY bz)))))
+    z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    for k in range(10):
+        idx = (x % 8) + 8 * ((y % 8) + 8 * ((z % 8) + 8 * (k + 10 * ((x // 8) + (nx // 8) * ((y // 8) + (ny // 8) * (z // 8))))))
+        np.testing.assert_array_equal(ref[idx], m[k])
+    dom.set_moments_ref_layout(ref)
+    np.testing.assert_array_equal(dom.moments(), m)
+
+
+def test_fp64_reductions():
+    n = 24
+    d = mrlbm.make_desc(n, n, n, lattice=19)
+    dom = mrlbm.Domain(d)
+    dom.init_taylor_green(0.05, n / (2 * np.pi))
+    dom.step(5)
+    m = dom.moments().astype(np.float64)
+    s = dom.sums()
+    rho = 1.0 + m[0]
+    u = m[1:4] / 3.0
+    np.testing.assert_allclose(s["mass"], rho.sum(), rtol=1e-12)
+    np.testing.assert_allclose(s["kinetic_energy"], 0.5 * (rho * (u ** 2).sum(0)).sum(), rtol=1e-12)
+    np.testing.assert_allclose(s["momentum"], (rho * u).reshape(3, -1).sum(1), atol=1e-9)
+    assert s["fluid_nodes"] == n ** 3 and s["nonfinite"] == 0
+    r0 = dom.residual()
+    dom.step(3)
+    r1 = dom.residual()
+    assert r0 == 1.0 and 0 < r1 < 1
+
+
+def test_kinetic_energy_decay_matches_oracle():
+    """The reference's TGV report (src/cases/taylorGreen/treat_data.inc)."""
+    n = 32
+    d = mrlbm.make_desc(n, n, n, lattice=27, tau=0.52)
+    dom = mrlbm.Domain(d)
+    dom.init_taylor_green(0.04, n / (2 * np.pi))
+    orc = pu.oracle_for(d)
+    orc.set_moments(pu.gpu_to_oracle_layout(dom.moments()))
+    for _ in range(4):
+        dom.step(25)
+        orc.step(25)
+        np.testing.assert_allclose(dom.sums()["kinetic_energy"], orc.sums()[4], rtol=1e-5)
