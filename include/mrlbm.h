@@ -170,6 +170,42 @@ mrlbm_status mrlbm_save_macr_bin(mrlbm_domain* dom, const char* path_files, cons
 mrlbm_status mrlbm_save_info(mrlbm_domain* dom, const char* path_files, const char* id_sim,
                              const char* case_name, int nsteps, double mlups);
 
+/* ------------------------------------------------------------------ batches
+ * Many independent domains of uneven sizes advanced together by one
+ * persistent kernel per step: every domain's (x, y) columns and z chunks form
+ * one work list; persistent CTAs take work items from a device-side ticket
+ * counter; the step launches are captured once in a CUDA graph and replayed.
+ * The reference runs one domain per process (src/main.cu); this has no
+ * counterpart there.  All domains of a batch share the lattice and the storage
+ * precision; the supported physics per domain are periodic/no-BC, walls and
+ * velocity walls (with or without body force), and power-law walls with body
+ * force (the serving mix).  Domain ids stay valid until removed. */
+typedef struct mrlbm_batch mrlbm_batch;
+
+mrlbm_status mrlbm_batch_create(int lattice, int storage, mrlbm_batch** out);
+mrlbm_status mrlbm_batch_destroy(mrlbm_batch* batch);
+/* Adds a domain (allocates its moment buffers); *id receives its handle. */
+mrlbm_status mrlbm_batch_add(mrlbm_batch* batch, const mrlbm_desc* desc, int* id);
+mrlbm_status mrlbm_batch_remove(mrlbm_batch* batch, int id);
+/* The domain object of a member, for set-up and read-back with the
+ * single-domain calls above (node types, init, moments, reductions, files).
+ * Do not step it directly while it belongs to the batch. */
+mrlbm_status mrlbm_batch_domain(mrlbm_batch* batch, int id, mrlbm_domain** dom);
+/* Advance every member by nsteps (graph replay; eager launches for a short
+ * remainder). */
+mrlbm_status mrlbm_batch_step(mrlbm_batch* batch, int nsteps);
+mrlbm_status mrlbm_batch_synchronize(mrlbm_batch* batch);
+/* Device-timed nsteps of the whole batch (CUDA events around the launches). */
+mrlbm_status mrlbm_batch_time_steps(mrlbm_batch* batch, int nsteps, float* ms);
+/* Work items (columns) in the current list, lattice nodes of all members. */
+mrlbm_status mrlbm_batch_info(mrlbm_batch* batch, int* members, int* items, long long* nodes);
+/* Autotuner: measures the z-chunk length per domain-size class on this GPU
+ * (a few timed steps per candidate on a scratch domain) and uses the winner
+ * for every member of that class.  Without it a size rule is used. */
+mrlbm_status mrlbm_batch_autotune(mrlbm_batch* batch);
+/* The z-chunk length the batch uses for a domain of this size. */
+mrlbm_status mrlbm_batch_chunk_for(mrlbm_batch* batch, int nx, int ny, int nz, int* lz);
+
 /* Host-side node-type builders (no device work).
  * Voxel geometry: solid (x-fastest, nonzero = solid) -> nodeTypeMap words: solid
  * nodes 0xFF, fluid nodes the octant mask of their solid neighbours; neighbours

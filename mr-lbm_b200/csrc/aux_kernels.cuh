@@ -75,7 +75,7 @@ __global__ void init_kernel(const InitArgs a)
         float m[11];
         init_moments<Q>(rho, ux, uy, uz, a.rho0, a.qs, m);
         m[10] = a.omega0;
-        const long long idx = (long long)z * a.plane + (long long)y * a.pitch + x;
+        const long long idx = pidx(x, y, z, a.pitch, a.plane);
         T* p0 = reinterpret_cast<T*>(a.m0);
         T* p1 = reinterpret_cast<T*>(a.m1);
         for (int k = 0; k < a.nm; k++) {
@@ -111,7 +111,7 @@ __global__ void convert_kernel(const ConvArgs a)
         const int x = (int)(node % a.nx);
         const int y = (int)((node / a.nx) % a.ny);
         const int z = (int)(node / ((long long)a.nx * a.ny));
-        const long long idx = k * a.field + (long long)z * a.plane + (long long)y * a.pitch + x;
+        const long long idx = k * a.field + pidx(x, y, z, a.pitch, a.plane);
         long long fi;
         if (a.mode < 2) {
             fi = g;
@@ -127,6 +127,55 @@ __global__ void convert_kernel(const ConvArgs a)
             const float v = is_f32<T>() ? a.f[fi] : a.f[fi] * a.scale[k];
             Stor<T>::st(reinterpret_cast<T*>(a.m0) + idx, v);
             Stor<T>::st(reinterpret_cast<T*>(a.m1) + idx, v);
+        }
+    }
+}
+
+// Ghost shell of the padded layout: periodic axes copy the wrapped interior,
+// wall axes hold the exterior state (the reference's stale initial ghost
+// populations at walls, src/includeFiles/interface.h:6-19).  Applied to both
+// ping-pong buffers after any host-side change of the moments.
+struct GhostArgs {
+    void* m0;
+    void* m1;
+    int nx, ny, nz, pitch;
+    long long plane, field;
+    int nm, periodic;
+    float ext[11];
+    float scale[11];
+};
+
+template <typename T>
+__global__ void ghost_fill_kernel(const GhostArgs a)
+{
+    const long long ex = a.nx + 2, ey = a.ny + 2, ez = a.nz + 2;
+    const long long n = ex * ey * ez;
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < n; g += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(g % ex) - 1;
+        const int y = (int)((g / ex) % ey) - 1;
+        const int z = (int)(g / (ex * ey)) - 1;
+        const bool in_x = x >= 0 && x < a.nx, in_y = y >= 0 && y < a.ny, in_z = z >= 0 && z < a.nz;
+        if (in_x && in_y && in_z) continue;
+        bool wall = false;
+        int sx = x, sy = y, sz = z;
+        if (!in_x) { if (a.periodic & 1) sx = (x + a.nx) % a.nx; else wall = true; }
+        if (!in_y) { if (a.periodic & 2) sy = (y + a.ny) % a.ny; else wall = true; }
+        if (!in_z) { if (a.periodic & 4) sz = (z + a.nz) % a.nz; else wall = true; }
+        const long long di = pidx(x, y, z, a.pitch, a.plane);
+        T* p0 = reinterpret_cast<T*>(a.m0);
+        T* p1 = reinterpret_cast<T*>(a.m1);
+        if (wall) {
+            for (int k = 0; k < a.nm; k++) {
+                const float v = is_f32<T>() ? a.ext[k] : a.ext[k] * a.scale[k];
+                Stor<T>::st(p0 + k * a.field + di, v);
+                Stor<T>::st(p1 + k * a.field + di, v);
+            }
+        } else {
+            const long long si = pidx(sx, sy, sz, a.pitch, a.plane);
+            for (int k = 0; k < a.nm; k++) {
+                p0[k * a.field + di] = p0[k * a.field + si];
+                p1[k * a.field + di] = p0[k * a.field + si];
+            }
         }
     }
 }
@@ -166,7 +215,7 @@ __global__ void __launch_bounds__(RED_THREADS) reduce_kernel(const RedArgs a)
         const int x = (int)(g % a.nx);
         const int y = (int)((g / a.nx) % a.ny);
         const int z = (int)(g / ((long long)a.nx * a.ny));
-        const long long idx = (long long)z * a.plane + (long long)y * a.pitch + x;
+        const long long idx = pidx(x, y, z, a.pitch, a.plane);
         if (a.has_cls && a.cls[idx] == CLS_SOLID) continue;
         float v[4];
         bool finite = true;

@@ -1,0 +1,427 @@
+// batch.cu -- C ABI of domain batches (include/mrlbm.h, "batches").
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <vector>
+
+#include "../../include/mrlbm.h"
+#include "batch_kernel.cuh"
+#include "domain.h"
+
+using namespace mrlbm;
+
+#define CK(call)                                                                                               \
+    do {                                                                                                       \
+        cudaError_t e_ = (call);                                                                               \
+        if (e_ != cudaSuccess)                                                                                 \
+            return fail(MRLBM_ECUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+struct mrlbm_batch {
+    int lattice = 19, storage = MRLBM_F32;
+    std::vector<mrlbm_domain*> members;  // id -> domain (nullptr: removed)
+    std::vector<int> offsets;            // id -> parity offset
+    std::vector<BatchDomain> h_doms;
+    BatchDomain* d_doms = nullptr;
+    int dom_cap = 0;
+    BatchItem* d_items = nullptr;
+    int item_cap = 0;
+    int nitems = 0;
+    std::vector<BatchItem> h_items;
+    BatchCtl* d_ctl = nullptr;
+    long long step = 0;  // host mirror of the device step counter
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int grid = 148;
+    size_t smem = 0;
+    std::map<int, int> lz_by_class;  // autotuned z-chunk per size class
+};
+
+namespace {
+
+template <int Q, typename T>
+mrlbm_status set_attr(size_t& smem)
+{
+    smem = ZSmem<Q, T, BATCH_TYI>::bytes;
+    cudaError_t e = cudaFuncSetAttribute(batch_step<Q, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return fail(MRLBM_ECUDA, "batch attribute: %s", cudaGetErrorString(e));
+    return MRLBM_OK;
+}
+
+template <int Q, typename T>
+void launch(mrlbm_batch* b)
+{
+    batch_step<Q, T><<<b->grid, 32 * (BATCH_TYI + 2), b->smem, b->stream>>>(b->d_doms, b->d_items, b->d_ctl);
+}
+
+void launch_any(mrlbm_batch* b)
+{
+    if (b->lattice == 19) {
+        if (b->storage == MRLBM_F32) launch<19, float>(b); else launch<19, __half>(b);
+    } else {
+        if (b->storage == MRLBM_F32) launch<27, float>(b); else launch<27, __half>(b);
+    }
+}
+
+int size_class(int nx, int ny, int nz)
+{
+    const int e = std::max(nx, std::max(ny, nz));
+    if (e < 32) return 0;
+    if (e < 48) return 1;
+    if (e < 64) return 2;
+    if (e < 96) return 3;
+    if (e < 128) return 4;
+    if (e < 192) return 5;
+    return 6;
+}
+
+int chunk_for(const mrlbm_batch* b, int nx, int ny, int nz)
+{
+    auto it = b->lz_by_class.find(size_class(nx, ny, nz));
+    int lz = it != b->lz_by_class.end() ? it->second : 32;
+    return std::max(1, std::min(lz, nz));
+}
+
+int batch_flags(const mrlbm_domain* dom)
+{
+    StepArgs a;
+    int flags;
+    fill_step_args(dom, a, 0, flags);
+    if (flags & (F_FORCE | F_POWERLAW | F_BINGHAM)) flags |= F_BC;
+    return flags;
+}
+
+bool flags_supported(int f)
+{
+    return f == 0 || f == F_BC || f == (F_BC | F_FORCE) || f == (F_BC | F_FORCE | F_POWERLAW);
+}
+
+// Rebuild the per-domain records and the work list from the members; upload
+// what changed.  Items are ordered by cost, largest first.
+mrlbm_status refresh(mrlbm_batch* b)
+{
+    const int n = (int)b->members.size();
+    if (n > b->dom_cap) {
+        const int cap = std::max(2 * n, 64);
+        BatchDomain* nd = nullptr;
+        CK(cudaMalloc(&nd, cap * sizeof(BatchDomain)));
+        cudaFree(b->d_doms);
+        b->d_doms = nd;
+        b->dom_cap = cap;
+        b->h_doms.clear();
+        if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+    }
+    std::vector<BatchDomain> hd(n);
+    std::vector<BatchItem> items;
+    for (int id = 0; id < n; id++) {
+        memset(&hd[id], 0, sizeof(BatchDomain));
+        mrlbm_domain* dom = b->members[id];
+        if (!dom) continue;
+        dom->lz = chunk_for(b, dom->d.nx, dom->d.ny, dom->d.nz);
+        int f;
+        for (int p = 0; p < 2; p++) fill_step_args(dom, hd[id].args[p], p, f);
+        hd[id].flags = batch_flags(dom);
+        if (!flags_supported(hd[id].flags))
+            return fail(MRLBM_EINVAL, "batch member %d: physics flag set %d not supported in batches", id, hd[id].flags);
+        hd[id].map[0] = dom->tmap[0];
+        hd[id].map[1] = dom->tmap[1];
+        hd[id].parity_offset = b->offsets[id];
+        const int gx = (dom->d.nx + TILE_X - 1) / TILE_X, gy = (dom->d.ny + BATCH_TYI - 1) / BATCH_TYI;
+        for (int z0 = 0; z0 < dom->d.nz; z0 += dom->lz)
+            for (int by = 0; by < gy; by++)
+                for (int bx = 0; bx < gx; bx++) items.push_back({id, bx * TILE_X, by * BATCH_TYI, z0});
+    }
+    std::stable_sort(items.begin(), items.end(), [&](const BatchItem& u, const BatchItem& v) {
+        const mrlbm_domain* du = b->members[u.dom];
+        const mrlbm_domain* dv = b->members[v.dom];
+        const int cu = std::min(du->lz, du->d.nz - u.z0), cv = std::min(dv->lz, dv->d.nz - v.z0);
+        return cu > cv;
+    });
+    if (b->h_doms.size() != hd.size() || memcmp(b->h_doms.data(), hd.data(), hd.size() * sizeof(BatchDomain)) != 0) {
+        if (!hd.empty())
+            CK(cudaMemcpyAsync(b->d_doms, hd.data(), hd.size() * sizeof(BatchDomain), cudaMemcpyHostToDevice, b->stream));
+        b->h_doms = hd;
+    }
+    const int ni = (int)items.size();
+    if (ni > b->item_cap) {
+        const int cap = std::max(2 * ni, 1024);
+        BatchItem* nitm = nullptr;
+        CK(cudaMalloc(&nitm, cap * sizeof(BatchItem)));
+        cudaFree(b->d_items);
+        b->d_items = nitm;
+        b->item_cap = cap;
+        b->h_items.clear();
+        if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+    }
+    if (b->h_items.size() != items.size() ||
+        memcmp(b->h_items.data(), items.data(), items.size() * sizeof(BatchItem)) != 0) {
+        if (ni) CK(cudaMemcpyAsync(b->d_items, items.data(), ni * sizeof(BatchItem), cudaMemcpyHostToDevice, b->stream));
+        b->h_items = items;
+    }
+    if (ni != b->nitems) {
+        CK(cudaMemcpyAsync(&b->d_ctl->nitems, &ni, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+        CK(cudaStreamSynchronize(b->stream));  // ni lives on the host stack
+        b->nitems = ni;
+    }
+    return MRLBM_OK;
+}
+
+void advance_members(mrlbm_batch* b, int nsteps)
+{
+    b->step += nsteps;
+    for (size_t id = 0; id < b->members.size(); id++) {
+        mrlbm_domain* dom = b->members[id];
+        if (!dom) continue;
+        dom->cur = (int)((b->step + b->offsets[id]) & 1);
+        dom->step += nsteps;
+    }
+}
+
+mrlbm_status enqueue_steps(mrlbm_batch* b, int nsteps)
+{
+    if (b->nitems == 0) {
+        advance_members(b, 0);
+        return MRLBM_OK;
+    }
+    int left = nsteps;
+    if (left >= GRAPH_STEPS) {
+        if (!b->graph) {
+            cudaGraph_t g;
+            CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+            for (int s = 0; s < GRAPH_STEPS; s++) launch_any(b);
+            CK(cudaStreamEndCapture(b->stream, &g));
+            CK(cudaGraphInstantiate(&b->graph, g, 0));
+            cudaGraphDestroy(g);
+        }
+        while (left >= GRAPH_STEPS) {
+            CK(cudaGraphLaunch(b->graph, b->stream));
+            left -= GRAPH_STEPS;
+        }
+    }
+    for (; left > 0; left--) launch_any(b);
+    CK(cudaGetLastError());
+    advance_members(b, nsteps);
+    return MRLBM_OK;
+}
+
+mrlbm_status check_members(mrlbm_batch* b)
+{
+    for (mrlbm_domain* dom : b->members) {
+        if (!dom) continue;
+        mrlbm_status st = check_device_error(dom);
+        if (st) return st;
+    }
+    return MRLBM_OK;
+}
+
+}  // namespace
+
+extern "C" mrlbm_status mrlbm_batch_create(int lattice, int storage, mrlbm_batch** out)
+{
+    if (!out) return fail(MRLBM_EINVAL, "null output handle");
+    *out = nullptr;
+    if (lattice != 19 && lattice != 27) return fail(MRLBM_EINVAL, "lattice must be 19 or 27");
+    if (storage != MRLBM_F32 && storage != MRLBM_F16)
+        return fail(MRLBM_EINVAL, "batches store moments in fp32 or fp16");
+    mrlbm_batch* b = new mrlbm_batch();
+    b->lattice = lattice;
+    b->storage = storage;
+    mrlbm_status st;
+    if (lattice == 19) st = storage == MRLBM_F32 ? set_attr<19, float>(b->smem) : set_attr<19, __half>(b->smem);
+    else st = storage == MRLBM_F32 ? set_attr<27, float>(b->smem) : set_attr<27, __half>(b->smem);
+    if (st) { delete b; return st; }
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (lattice == 19)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, storage == MRLBM_F32 ? batch_step<19, float> : batch_step<19, __half>,
+                                                      32 * (BATCH_TYI + 2), b->smem);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, storage == MRLBM_F32 ? batch_step<27, float> : batch_step<27, __half>,
+                                                      32 * (BATCH_TYI + 2), b->smem);
+    b->grid = sms * std::max(per_sm, 1);
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
+        cudaMalloc(&b->d_ctl, sizeof(BatchCtl)) != cudaSuccess ||
+        cudaMemset(b->d_ctl, 0, sizeof(BatchCtl)) != cudaSuccess) {
+        mrlbm_batch_destroy(b);
+        return fail(MRLBM_ECUDA, "batch setup failed");
+    }
+    *out = b;
+    return MRLBM_OK;
+}
+
+extern "C" mrlbm_status mrlbm_batch_destroy(mrlbm_batch* b)
+{
+    if (!b) return MRLBM_OK;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    for (mrlbm_domain* d : b->members)
+        if (d) mrlbm_domain_destroy(d);
+    cudaFree(b->d_doms);
+    cudaFree(b->d_items);
+    cudaFree(b->d_ctl);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return MRLBM_OK;
+}
+
+extern "C" mrlbm_status mrlbm_batch_add(mrlbm_batch* b, const mrlbm_desc* desc, int* id)
+{
+    if (!b || !desc || !id) return fail(MRLBM_EINVAL, "null argument");
+    if (desc->lattice != b->lattice || desc->storage != b->storage)
+        return fail(MRLBM_EINVAL, "member lattice/storage must match the batch");
+    mrlbm_domain* dom = nullptr;
+    mrlbm_status st = mrlbm_domain_create(desc, &dom);
+    if (st) return st;
+    if (!flags_supported(batch_flags(dom))) {
+        mrlbm_domain_destroy(dom);
+        return fail(MRLBM_EINVAL, "physics of this domain are not supported in batches");
+    }
+    // reuse a free slot
+    int slot = -1;
+    for (size_t k = 0; k < b->members.size(); k++)
+        if (!b->members[k]) { slot = (int)k; break; }
+    if (slot < 0) {
+        slot = (int)b->members.size();
+        b->members.push_back(nullptr);
+        b->offsets.push_back(0);
+    }
+    b->members[slot] = dom;
+    b->offsets[slot] = (int)((dom->cur - b->step) & 1);
+    *id = slot;
+    return MRLBM_OK;
+}
+
+extern "C" mrlbm_status mrlbm_batch_remove(mrlbm_batch* b, int id)
+{
+    if (!b || id < 0 || id >= (int)b->members.size() || !b->members[id]) return fail(MRLBM_ENOTFOUND, "no member %d", id);
+    CK(cudaStreamSynchronize(b->stream));
+    mrlbm_domain_destroy(b->members[id]);
+    b->members[id] = nullptr;
+    return MRLBM_OK;
+}
+
+extern "C" mrlbm_status mrlbm_batch_domain(mrlbm_batch* b, int id, mrlbm_domain** dom)
+{
+    if (!b || !dom || id < 0 || id >= (int)b->members.size() || !b->members[id])
+        return fail(MRLBM_ENOTFOUND, "no member %d", id);
+    // work queued on the batch stream must finish before single-domain calls
+    CK(cudaStreamSynchronize(b->stream));
+    *dom = b->members[id];
+    return MRLBM_OK;
+}
+
+extern "C" mrlbm_status mrlbm_batch_step(mrlbm_batch* b, int nsteps)
+{
+    if (!b || nsteps < 0) return fail(MRLBM_EINVAL, "bad argument");
+    // members may have been re-initialised through their domain handles
+    for (size_t id = 0; id < b->members.size(); id++)
+        if (b->members[id]) {
+            CK(cudaStreamSynchronize(b->members[id]->stream));
+            b->offsets[id] = (int)((b->members[id]->cur - b->step) & 1);
+        }
+    mrlbm_status st = refresh(b);
+    if (st) return st;
+    return enqueue_steps(b, nsteps);
+}
+
+extern "C" mrlbm_status mrlbm_batch_synchronize(mrlbm_batch* b)
+{
+    if (!b) return fail(MRLBM_EINVAL, "null batch");
+    CK(cudaStreamSynchronize(b->stream));
+    return check_members(b);
+}
+
+extern "C" mrlbm_status mrlbm_batch_time_steps(mrlbm_batch* b, int nsteps, float* ms)
+{
+    if (!b || !ms) return fail(MRLBM_EINVAL, "null argument");
+    for (size_t id = 0; id < b->members.size(); id++)
+        if (b->members[id]) {
+            CK(cudaStreamSynchronize(b->members[id]->stream));
+            b->offsets[id] = (int)((b->members[id]->cur - b->step) & 1);
+        }
+    mrlbm_status st = refresh(b);
+    if (st) return st;
+    CK(cudaEventRecord(b->ev0, b->stream));
+    st = enqueue_steps(b, nsteps);
+    if (st) return st;
+    CK(cudaEventRecord(b->ev1, b->stream));
+    CK(cudaEventSynchronize(b->ev1));
+    CK(cudaEventElapsedTime(ms, b->ev0, b->ev1));
+    return check_members(b);
+}
+
+extern "C" mrlbm_status mrlbm_batch_info(mrlbm_batch* b, int* members, int* items, long long* nodes)
+{
+    if (!b) return fail(MRLBM_EINVAL, "null batch");
+    int m = 0;
+    long long nn = 0;
+    for (mrlbm_domain* d : b->members)
+        if (d) {
+            m++;
+            nn += (long long)d->d.nx * d->d.ny * d->d.nz;
+        }
+    mrlbm_status st = refresh(b);
+    if (st) return st;
+    if (members) *members = m;
+    if (items) *items = b->nitems;
+    if (nodes) *nodes = nn;
+    return MRLBM_OK;
+}
+
+extern "C" mrlbm_status mrlbm_batch_chunk_for(mrlbm_batch* b, int nx, int ny, int nz, int* lz)
+{
+    if (!b || !lz) return fail(MRLBM_EINVAL, "null argument");
+    *lz = chunk_for(b, nx, ny, nz);
+    return MRLBM_OK;
+}
+
+// Coordinate search over the z-chunk length of each size class present, timing
+// the whole batch: the chunk trades z-halo work (2 planes per chunk) against
+// the number of work items available for load balance.
+extern "C" mrlbm_status mrlbm_batch_autotune(mrlbm_batch* b)
+{
+    if (!b) return fail(MRLBM_EINVAL, "null batch");
+    std::vector<int> classes;
+    for (mrlbm_domain* d : b->members)
+        if (d) {
+            const int c = size_class(d->d.nx, d->d.ny, d->d.nz);
+            if (std::find(classes.begin(), classes.end(), c) == classes.end()) classes.push_back(c);
+        }
+    static const int cand[] = {8, 16, 24, 32, 48, 64, 96};
+    auto timed = [&](float* ms) -> mrlbm_status {
+        mrlbm_status st = refresh(b);
+        if (st) return st;
+        st = enqueue_steps(b, 2);
+        if (st) return st;
+        CK(cudaEventRecord(b->ev0, b->stream));
+        st = enqueue_steps(b, 6);
+        if (st) return st;
+        CK(cudaEventRecord(b->ev1, b->stream));
+        CK(cudaEventSynchronize(b->ev1));
+        CK(cudaEventElapsedTime(ms, b->ev0, b->ev1));
+        return MRLBM_OK;
+    };
+    for (int c : classes) {
+        float best = 1e30f;
+        int best_lz = 32;
+        for (int lz : cand) {
+            b->lz_by_class[c] = lz;
+            float ms = 0.f;
+            mrlbm_status st = timed(&ms);
+            if (st) return st;
+            if (ms < best * 0.98f) {
+                best = ms;
+                best_lz = lz;
+            }
+        }
+        b->lz_by_class[c] = best_lz;
+    }
+    return refresh(b);
+}

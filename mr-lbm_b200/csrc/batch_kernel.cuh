@@ -1,0 +1,95 @@
+// batch_kernel.cuh -- persistent z-march over many independent domains.
+//
+// A batch packs the columns of many domains of uneven sizes into one work list.
+// Each persistent CTA (one per SM) takes the next column from a global ticket
+// counter and runs the same z-march as the single-domain kernel on it; the
+// last CTA to finish resets the counter and advances the batch step, so the
+// launch can be replayed from a CUDA graph with no host work between steps.
+#pragma once
+#include "kernels.cuh"
+
+namespace mrlbm {
+
+constexpr int BATCH_TYI = 14;  // rows per CTA of the batched kernel (16 warps)
+
+// Per-domain data the batched kernel needs; both parities are precomputed so
+// the kernel only selects.  64-byte aligned for the tensor maps.
+struct alignas(64) BatchDomain {
+    CUtensorMap map[2];  // TMA maps over moment buffers 0 and 1
+    StepArgs args[2];    // args[p]: read buffer p, write buffer p^1
+    int flags;           // F_* set of this domain
+    int parity_offset;   // parity of buffer read at batch step s: (s + offset) & 1
+    int pad[14];
+};
+
+struct BatchItem {
+    int dom;
+    int X0, Y0, z0;
+};
+
+// Device-side queue control (one per batch).
+struct BatchCtl {
+    int next;    // ticket counter
+    int done;    // CTAs finished in this launch
+    int step;    // batch step count (parity source)
+    int nitems;  // active work items
+};
+
+template <int Q, typename T, int FLAGS>
+__device__ __forceinline__ bool batch_column(const StepArgs& a, const CUtensorMap* map, const BatchItem& it,
+                                             const ZSmem<Q, T, BATCH_TYI>& sm, unsigned& g0)
+{
+    return zmarch_column<Q, T, FLAGS, BATCH_TYI>(a, map, it.X0, it.Y0, it.z0, sm, g0);
+}
+
+template <int Q, typename T>
+__global__ void __launch_bounds__(32 * (BATCH_TYI + 2), 1)
+    batch_step(const BatchDomain* __restrict__ doms, const BatchItem* __restrict__ items, BatchCtl* ctl)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ int s_item;
+    __shared__ __align__(16) StepArgs s_args;
+    const ZSmem<Q, T, BATCH_TYI> sm(smem);
+    zmarch_init_barriers<Q, T, BATCH_TYI>(sm);
+    const int step = *((volatile int*)&ctl->step);
+    const int nitems = *((volatile int*)&ctl->nitems);
+    unsigned g0 = 0;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(&ctl->next, 1);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= nitems) break;
+        const BatchItem item = items[it];
+        const BatchDomain& D = doms[item.dom];
+        const int par = (step + D.parity_offset) & 1;
+        constexpr int NW = (int)(sizeof(StepArgs) / 4);
+        if (threadIdx.x < NW)
+            reinterpret_cast<int*>(&s_args)[threadIdx.x] = reinterpret_cast<const int*>(&D.args[par])[threadIdx.x];
+        __syncthreads();
+        bool ok = true;
+        switch (D.flags) {
+            case 0: ok = batch_column<Q, T, 0>(s_args, &D.map[par], item, sm, g0); break;
+            case F_BC: ok = batch_column<Q, T, F_BC>(s_args, &D.map[par], item, sm, g0); break;
+            case F_BC | F_FORCE: ok = batch_column<Q, T, F_BC | F_FORCE>(s_args, &D.map[par], item, sm, g0); break;
+            case F_BC | F_FORCE | F_POWERLAW:
+                ok = batch_column<Q, T, F_BC | F_FORCE | F_POWERLAW>(s_args, &D.map[par], item, sm, g0);
+                break;
+            default: break;  // rejected on the host when the domain joins
+        }
+        if (!ok) break;
+    }
+    // the last CTA out resets the ticket counter and advances the step; every
+    // CTA has taken its last ticket before it counts itself done
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const int d = atomicAdd(&ctl->done, 1);
+        if (d == (int)gridDim.x - 1) {
+            ctl->next = 0;
+            ctl->done = 0;
+            ctl->step = step + 1;
+            __threadfence();
+        }
+    }
+}
+
+}  // namespace mrlbm

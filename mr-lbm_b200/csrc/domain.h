@@ -15,10 +15,12 @@ constexpr int GRAPH_STEPS = 16;  // launches per captured graph (even: parities 
 
 }  // namespace mrlbm
 
-// HBM layout: each of the nm moments is a plane stack [z][y][pitch] (x
-// fastest, pitch = nx rounded up to 8), stored in the domain's storage type,
-// twice (ping-pong: step n reads m[cur] and writes m[cur^1]).  Node classes
-// are one byte per node in the same padded layout.
+// HBM layout: each of the nm moments is a plane stack [z+1][y+1][x+XOFF]
+// with a one-node ghost shell (z = -1..nz, y = -1..ny, x = -1..nx; pitch =
+// nx + XOFF + 1 rounded up to 8 elements, so rows are 16-byte aligned for
+// TMA), stored in the domain's storage type, twice (ping-pong: step n reads
+// m[cur] and writes m[cur^1]).  Node classes are one byte per node in the
+// same padded layout.
 struct mrlbm_domain {
     mrlbm_desc d{};
     int q = 19, nm = 10;
@@ -30,6 +32,8 @@ struct mrlbm_domain {
     int cur = 0;
     int step = 0;
     uint8_t* cls = nullptr;
+    int* err = nullptr;              // device flag: a bounded wait timed out
+    CUtensorMap tmap[2];             // TMA maps of the two moment buffers
     mrlbm::BcClass* bc = nullptr;
     int nclasses = 0;
     bool has_bc = false;
@@ -60,7 +64,10 @@ int choose_lz(const mrlbm_domain* dom);
 void fill_step_args(const mrlbm_domain* dom, StepArgs& a, int parity, int& flags);
 mrlbm_status enqueue_step(mrlbm_domain* dom, int parity, cudaStream_t s);
 template <int Q, typename T>
-mrlbm_status dispatch_step(const StepArgs& a, int flags, cudaStream_t s);
+mrlbm_status dispatch_step(const CUtensorMap& map, const StepArgs& a, int flags, cudaStream_t s);
+mrlbm_status make_tensor_maps(mrlbm_domain* dom);
+mrlbm_status fill_ghosts(mrlbm_domain* dom);
+mrlbm_status check_device_error(mrlbm_domain* dom);
 mrlbm_status enqueue_reduce(mrlbm_domain* dom, double* partial, double* out, int residual_mode, cudaStream_t s);
 
 }  // namespace mrlbm

@@ -7,24 +7,31 @@
 // then the new moments (bulk sums, or the moment-space wall BC), and collides
 // them in moment space.  Only the 10 (11) moments live in HBM.
 //
-// B200 design (z-marching, ping-pong moments):
+// B200 design (z-marching, ping-pong moments, TMA-fed):
+//   * Moments are stored per moment as padded plane stacks with a one-node
+//     ghost shell (x = -1..nx, y = -1..ny, z = -1..nz).  Periodic axes keep
+//     the shell equal to the wrapped interior: the kernel writes the extra
+//     copies of boundary nodes.  Wall axes keep the shell at the exterior rest
+//     state.  So every halo read is an in-bounds tile read with no wrap logic.
 //   * A CTA owns a column of 30 x TYI interior nodes in (x, y) and a chunk of
 //     LZ planes in z.  Warp w holds row y = Y0 - 1 + w, lane l holds
 //     x = X0 - 1 + l: the outer lanes / warps are the one-node halo.
-//   * Each production step reads the moments of one (x, y) plane (coalesced,
-//     prefetched one plane ahead) and reconstructs the post-collision
-//     populations of every node of the plane in registers.
-//   * Populations that move in x only are exchanged with warp shuffles,
-//     populations that move in y go through a double-buffered shared-memory
-//     row exchange (one __syncthreads per plane), populations that move in z
+//   * One elected thread streams the planes of the column into a 3-stage
+//     shared-memory ring with cp.async.bulk.tensor (TMA) and mbarrier
+//     transaction counts; the waits are bounded and a timeout makes every
+//     thread leave together with an error flag set.
+//   * Each production step reconstructs the post-collision populations of
+//     every node of one plane in registers.  Populations that move in x only
+//     go through warp shuffles, populations that move in y through a
+//     double-buffered shared-memory row exchange packed by (c_x, c_y) into
+//     128-bit words (one __syncthreads per plane), populations that move in z
 //     stay in registers: a plane's c_z=+1 populations are held until the next
 //     plane, its c_z=0 ones until the output of the same plane is formed one
 //     step later.  Output plane z is completed when plane z+1 is produced.
-//   * Moments are read from one buffer and written to the other, so halo
-//     moments are always the previous step's (no ghost-population arrays, no
-//     per-step host sync).  DRAM traffic is the algorithmic 2*M*s bytes per
-//     node plus halo re-reads that mostly hit L2.
+//   * DRAM traffic is the algorithmic 2*M*s bytes per node; halo re-reads of
+//     neighbouring columns hit L2.
 #pragma once
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cstdint>
@@ -40,9 +47,13 @@ enum : int {
     F_BINGHAM = 8,   // omega field, Bingham viscosity
 };
 
-constexpr int TILE_X = 30;  // interior nodes per warp row
+constexpr int TILE_X = 30;   // interior nodes per warp row
+constexpr int XOFF = 4;      // padded column of x = 0 (x = -1 is the ghost column)
+constexpr int BOX_X = 40;    // TMA box width (elements) covering the 32 lanes
+constexpr int NSTAGE = 3;    // TMA ring depth
 constexpr uint8_t CLS_BULK = 0;
 constexpr uint8_t CLS_SOLID = 255;
+constexpr unsigned WAIT_LIMIT = 1u << 26;  // mbarrier polls before giving up (~seconds)
 
 // Moment-space wall BC data of one node class (octant mask + velocity index).
 // The BC is the linear system
@@ -62,10 +73,10 @@ struct BcClass {
 };
 
 struct StepArgs {
-    const void* __restrict__ m_in;  // [nm][nz][ny][pitch] storage type
-    void* __restrict__ m_out;
-    const uint8_t* __restrict__ cls;  // [nz][ny][pitch]
+    void* __restrict__ m_out;         // padded planes [nm][nz+2][ny+2][pitch]
+    const uint8_t* __restrict__ cls;  // padded [nz+2][ny+2][pitch]
     const BcClass* __restrict__ bc;
+    int* err;                         // bit 0: a bounded wait timed out
     int nx, ny, nz, pitch;
     long long plane, field;  // elements
     int periodic;            // bit a set: axis a periodic
@@ -73,10 +84,14 @@ struct StepArgs {
     float rho0, omega0;
     float fx, fy, fz;
     float nnf_n, nnf_k, nnf_yield, nnf_omega_p;
-    float ext[11];     // stored-moment state of sources outside wall axes
     float scale[11];   // storage scale per moment (1 for fp32)
     float iscale[11];
 };
+
+__host__ __device__ __forceinline__ long long pidx(int x, int y, int z, int pitch, long long plane)
+{
+    return (long long)(z + 1) * plane + (long long)(y + 1) * pitch + (x + XOFF);
+}
 
 // ------------------------------------------------------------------ storage
 
@@ -85,16 +100,19 @@ struct Stor;
 template <>
 struct Stor<float> {
     static __device__ __forceinline__ float ld(const float* p) { return __ldg(p); }
+    static __device__ __forceinline__ float lds(const float* p) { return *p; }
     static __device__ __forceinline__ void st(float* p, float v) { *p = v; }
 };
 template <>
 struct Stor<__half> {
     static __device__ __forceinline__ float ld(const __half* p) { return __half2float(__ldg(p)); }
+    static __device__ __forceinline__ float lds(const __half* p) { return __half2float(*p); }
     static __device__ __forceinline__ void st(__half* p, float v) { *p = __float2half_rn(v); }
 };
 template <>
 struct Stor<__nv_bfloat16> {
     static __device__ __forceinline__ float ld(const __nv_bfloat16* p) { return __bfloat162float(__ldg(p)); }
+    static __device__ __forceinline__ float lds(const __nv_bfloat16* p) { return __bfloat162float(*p); }
     static __device__ __forceinline__ void st(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
 };
 
@@ -159,21 +177,21 @@ __device__ __forceinline__ void lattice_sums(const float* p, float& r, float* j,
     j[0] = j[1] = j[2] = 0.f;
 #pragma unroll
     for (int k = 0; k < 6; k++) P[k] = 0.f;
-#pragma unroll
-    for (int i = 1; i < Q; i += 2) {
+    static_for<0, Q / 2>([&](auto h) {
+        constexpr int i = 2 * h + 1;
+        constexpr int cx = lat_cx(i), cy = lat_cy(i), cz = lat_cz(i);
         const float s = p[i] + p[i + 1], d = p[i] - p[i + 1];
-        const int cx = lat_cx(i), cy = lat_cy(i), cz = lat_cz(i);
         r += s;
-        if (cx > 0) j[0] += d; else if (cx < 0) j[0] -= d;
-        if (cy > 0) j[1] += d; else if (cy < 0) j[1] -= d;
-        if (cz > 0) j[2] += d; else if (cz < 0) j[2] -= d;
-        if (cx != 0) P[0] += s;
-        if (cy != 0) P[3] += s;
-        if (cz != 0) P[5] += s;
-        if (cx * cy > 0) P[1] += s; else if (cx * cy < 0) P[1] -= s;
-        if (cx * cz > 0) P[2] += s; else if (cx * cz < 0) P[2] -= s;
-        if (cy * cz > 0) P[4] += s; else if (cy * cz < 0) P[4] -= s;
-    }
+        if constexpr (cx > 0) j[0] += d; else if constexpr (cx < 0) j[0] -= d;
+        if constexpr (cy > 0) j[1] += d; else if constexpr (cy < 0) j[1] -= d;
+        if constexpr (cz > 0) j[2] += d; else if constexpr (cz < 0) j[2] -= d;
+        if constexpr (cx != 0) P[0] += s;
+        if constexpr (cy != 0) P[3] += s;
+        if constexpr (cz != 0) P[5] += s;
+        if constexpr (cx * cy > 0) P[1] += s; else if constexpr (cx * cy < 0) P[1] -= s;
+        if constexpr (cx * cz > 0) P[2] += s; else if constexpr (cx * cz < 0) P[2] -= s;
+        if constexpr (cy * cz > 0) P[4] += s; else if constexpr (cy * cz < 0) P[4] -= s;
+    });
 }
 
 // mac = rho, u (unscaled), Pi_hat (unscaled xx,xy,xz,yy,yz,zz) from the
@@ -186,18 +204,18 @@ __device__ __forceinline__ void bc_moments(const BcClass* __restrict__ c, const 
 {
     const uint32_t known = __ldg(&c->known);
     float b0 = 0.f, sxx = 0.f, sxy = 0.f, sxz = 0.f, syy = 0.f, syz = 0.f, szz = 0.f;
-#pragma unroll
-    for (int i = 0; i < Q; i++) {
+    static_for<0, Q>([&](auto I) {
+        constexpr int i = I;
+        constexpr int cx = lat_cx(i), cy = lat_cy(i), cz = lat_cz(i);
         const float v = ((known >> i) & 1u) ? p[i] : 0.f;
-        const int cx = lat_cx(i), cy = lat_cy(i), cz = lat_cz(i);
         b0 += v;
-        if (cx != 0) sxx += v;
-        if (cy != 0) syy += v;
-        if (cz != 0) szz += v;
-        if (cx * cy > 0) sxy += v; else if (cx * cy < 0) sxy -= v;
-        if (cx * cz > 0) sxz += v; else if (cx * cz < 0) sxz -= v;
-        if (cy * cz > 0) syz += v; else if (cy * cz < 0) syz -= v;
-    }
+        if constexpr (cx != 0) sxx += v;
+        if constexpr (cy != 0) syy += v;
+        if constexpr (cz != 0) szz += v;
+        if constexpr (cx * cy > 0) sxy += v; else if constexpr (cx * cy < 0) sxy -= v;
+        if constexpr (cx * cz > 0) sxz += v; else if constexpr (cx * cz < 0) sxz -= v;
+        if constexpr (cy * cz > 0) syz += v; else if constexpr (cy * cz < 0) syz -= v;
+    });
     const float third = b0 * (1.0f / 3.0f);
     const float b[7] = {b0, sxx - third, sxy, sxz, syy - third, syz, szz - third};
     float X[7];
@@ -284,6 +302,8 @@ __device__ __forceinline__ void collide(const StepArgs& a, const float* mac, flo
         mxz = t_om * mxz + omega * ux * uz + c3 * (Fx * uz + Fz * ux);
         myz = t_om * myz + omega * uy * uz + c3 * (Fy * uz + Fz * uy);
     } else {
+        (void)ir;
+        (void)tt_om;
         mxx = t_om * mxx + om_d2 * ux * ux;
         myy = t_om * myy + om_d2 * uy * uy;
         mzz = t_om * mzz + om_d2 * uz * uz;
@@ -297,154 +317,479 @@ __device__ __forceinline__ void collide(const StepArgs& a, const float* mac, flo
     out[10] = omega;
 }
 
+// ---------------------------------------------------- TMA / mbarrier helpers
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// Bounded wait on the phase with the given parity; returns false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity)
+{
+    const uint32_t a = smem_u32(bar);
+    for (unsigned it = 0; it < WAIT_LIMIT; it++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// 4-D tiled TMA load (x, moment, y, z) into shared memory, completing on bar.
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int x, int m, int y, int z,
+                                            uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(m), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
 // ---------------------------------------------------------- the step kernel
 
-template <typename T, int NM>
-__device__ __forceinline__ void load_node(const StepArgs& a, bool outside, long long idx, float* m)
+// Populations with c_y != 0 are exchanged between warp rows through shared
+// memory, packed by (c_x, c_y): group g = 3*(c_y > 0) + c_x + 1 holds the
+// c_z = -1, 0, +1 members in .x, .y, .z of a float4 (D3Q27: all six groups
+// full; D3Q19: only the c_x = 0 groups are full, the four diagonal ones have
+// one member and use a scalar slot).
+__host__ __device__ constexpr int ex_group(int i) { return 3 * (lat_cy(i) > 0 ? 1 : 0) + lat_cx(i) + 1; }
+__host__ __device__ constexpr bool ex_packed(int Q, int i) { return Q == 27 || lat_cx(i) == 0; }
+// scalar slot for D3Q19 diagonal groups: (cx,cy) = (-1,-1),(1,-1),(-1,1),(1,1) -> 0..3
+__host__ __device__ constexpr int ex_scalar_slot(int i) { return (lat_cy(i) > 0 ? 2 : 0) + (lat_cx(i) > 0 ? 1 : 0); }
+
+template <int Q, int G>
+__host__ __device__ constexpr bool ex_group_used()
 {
-    const T* base = reinterpret_cast<const T*>(a.m_in);
-    if (outside) {
-#pragma unroll
-        for (int k = 0; k < NM; k++) m[k] = a.ext[k];
-    } else {
-#pragma unroll
-        for (int k = 0; k < NM; k++) {
-            const float v = Stor<T>::ld(base + k * a.field + idx);
-            m[k] = is_f32<T>() ? v : v * a.iscale[k];
-        }
+    for (int i = 1; i < Q; i++)
+        if (lat_cy(i) != 0 && ex_group(i) == G && ex_packed(Q, i)) return true;
+    return false;
+}
+
+// store group G of this lane's populations (its c_z = -1, 0, +1 members)
+template <int Q, int G>
+__device__ __forceinline__ void ex_write(const float* f, float4* e4, int NW, int warp, int lane)
+{
+    if constexpr (ex_group_used<Q, G>()) {
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        static_for<1, Q>([&](auto I) {
+            constexpr int i = I;
+            if constexpr (lat_cy(i) != 0 && ex_group(i) == G && ex_packed(Q, i)) {
+                if constexpr (lat_cz(i) < 0) v.x = f[i];
+                else if constexpr (lat_cz(i) == 0) v.y = f[i];
+                else v.z = f[i];
+            }
+        });
+        e4[(G * NW + warp) * 32 + lane] = v;
     }
 }
 
-template <int Q, typename T, int FLAGS, int TYI>
-__global__ void __launch_bounds__(32 * (TYI + 2), 1) zmarch_step(const StepArgs a)
+// fetch group G arriving from row warp - c_y, lane - c_x
+template <int Q, int G>
+__device__ __forceinline__ void ex_read(float* g, const float4* e4, int NW, int warp, int lane)
+{
+    if constexpr (ex_group_used<Q, G>()) {
+        constexpr int cx = (G % 3) - 1, cy = G >= 3 ? 1 : -1;
+        const int w = min(max(warp - cy, 0), NW - 1);
+        const int l = (lane - cx) & 31;
+        const float4 v = e4[(G * NW + w) * 32 + l];
+        static_for<1, Q>([&](auto I) {
+            constexpr int i = I;
+            if constexpr (lat_cy(i) != 0 && ex_group(i) == G && ex_packed(Q, i))
+                g[i] = lat_cz(i) < 0 ? v.x : (lat_cz(i) == 0 ? v.y : v.z);
+        });
+    }
+}
+
+template <int Q, int NW>
+struct Exchange {
+    static constexpr int NPACK = 6;                  // float4 groups
+    static constexpr int NSCAL = Q == 19 ? 4 : 0;    // scalar slots
+    static constexpr size_t bytes_per_buffer = (size_t)NW * 32 * (NPACK * 16 + NSCAL * 4);
+};
+
+// Production of plane k (first half of a pipeline step): the plane's moments
+// come from TMA stage `stage`, its post-collision populations are
+// reconstructed, the c_y != 0 ones are written to exchange buffer k&1 and the
+// c_y = 0 ones are exchanged along x with shuffles into gsh (kept in
+// registers until the plane is consumed, one step later).
+template <int Q, int NM, typename T, int TYI>
+__device__ __forceinline__ void prod_a(const StepArgs& a, const T* stage, int k, float4* ex4, float* ex1, int lane,
+                                       int warp, int col, float (&gsh)[Q], float& om_node)
 {
     constexpr int NW = TYI + 2;
-    constexpr int NCY = lat_num_cy(Q);
-    constexpr int NUP = lat_num_cz(Q, 1);
-    constexpr int NMID = lat_num_cz(Q, 0);
-    constexpr bool OMF = (FLAGS & (F_POWERLAW | F_BINGHAM)) != 0;
-    constexpr int NM = OMF ? 11 : 10;
-    extern __shared__ float s_rows[];  // [2][NCY][NW][32]
+    float mc[NM];
+#pragma unroll
+    for (int m = 0; m < NM; m++) {
+        const float v = Stor<T>::lds(stage + (warp * NM + m) * BOX_X + col);
+        mc[m] = is_f32<T>() ? v : v * a.iscale[m];
+    }
+    float f[Q];
+    reconstruct<Q>(mc, a.rho0, f);
+    float4* e4 = ex4 + (k & 1) * (6 * NW * 32);
+    float* e1 = ex1 + (k & 1) * (4 * NW * 32);
+    ex_write<Q, 0>(f, e4, NW, warp, lane);
+    ex_write<Q, 1>(f, e4, NW, warp, lane);
+    ex_write<Q, 2>(f, e4, NW, warp, lane);
+    ex_write<Q, 3>(f, e4, NW, warp, lane);
+    ex_write<Q, 4>(f, e4, NW, warp, lane);
+    ex_write<Q, 5>(f, e4, NW, warp, lane);
+    if constexpr (Q == 19) {
+        static_for<1, Q>([&](auto I) {
+            constexpr int i = I;
+            if constexpr (lat_cy(i) != 0 && !ex_packed(Q, i)) e1[(ex_scalar_slot(i) * NW + warp) * 32 + lane] = f[i];
+        });
+    }
+    static_for<0, Q>([&](auto I) {
+        constexpr int i = I;
+        if constexpr (lat_cy(i) == 0) {
+            if constexpr (lat_cx(i) > 0) gsh[i] = __shfl_up_sync(0xffffffffu, f[i], 1);
+            else if constexpr (lat_cx(i) < 0) gsh[i] = __shfl_down_sync(0xffffffffu, f[i], 1);
+            else gsh[i] = f[i];
+        }
+    });
+    om_node = mc[NM - 1];
+}
 
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int X0 = blockIdx.x * TILE_X, Y0 = blockIdx.y * TYI, z0 = blockIdx.z * a.lz;
-    const int x = X0 - 1 + lane, y = Y0 - 1 + warp;
-    bool out_xy = false;
-    int xs = x, ys = y;
-    if (x < 0 || x >= a.nx) {
-        if (a.periodic & 1) xs = (x + a.nx) % a.nx; else out_xy = true;
-    }
-    if (y < 0 || y >= a.ny) {
-        if (a.periodic & 2) ys = (y + a.ny) % a.ny; else out_xy = true;
-    }
-    const bool interior = lane >= 1 && lane <= TILE_X && x < a.nx && warp >= 1 && warp <= TYI && y < a.ny;
-    const long long rowoff = out_xy ? 0 : (long long)ys * a.pitch + xs;
-    const int zend = min(z0 + a.lz, a.nz);
-    const int nprod = zend - z0 + 2;
+template <typename T, int NM>
+__device__ __forceinline__ void store_node(const StepArgs& a, long long idx, const float* o)
+{
     T* outp = reinterpret_cast<T*>(a.m_out);
-
-    auto src_index = [&](int zp, bool& outside) -> long long {
-        outside = out_xy;
-        int zs = zp;
-        if (zp < 0 || zp >= a.nz) {
-            if (a.periodic & 4) zs = (zp + a.nz) % a.nz; else outside = true;
-        }
-        return (long long)zs * a.plane + rowoff;
-    };
-
-    float mc[NM], mn[NM];
-    {
-        bool o;
-        const long long id = src_index(z0 - 1, o);
-        load_node<T, NM>(a, o, id, mc);
-    }
-    float up1[NUP], up2[NUP], mid[NMID];
-    float om_prev = a.omega0;
-
-    for (int k = 0; k < nprod; k++) {
-        const int zp = z0 - 1 + k;
-        if (k + 1 < nprod) {
-            bool o;
-            const long long id = src_index(zp + 1, o);
-            load_node<T, NM>(a, o, id, mn);
-        }
-        float f[Q];
-        reconstruct<Q>(mc, a.rho0, f);
-
-        float* buf = s_rows + (k & 1) * (NCY * NW * 32);
 #pragma unroll
-        for (int i = 1; i < Q; i++)
-            if (lat_cy(i) != 0) buf[(lat_cy_slot(Q, i) * NW + warp) * 32 + lane] = f[i];
-        float g[Q];
-#pragma unroll
-        for (int i = 0; i < Q; i++) {
-            if (lat_cy(i) == 0) {
-                if (lat_cx(i) > 0) g[i] = __shfl_up_sync(0xffffffffu, f[i], 1);
-                else if (lat_cx(i) < 0) g[i] = __shfl_down_sync(0xffffffffu, f[i], 1);
-                else g[i] = f[i];
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int i = 1; i < Q; i++) {
-            if (lat_cy(i) != 0) {
+    for (int m = 0; m < NM; m++) Stor<T>::st(outp + m * a.field + idx, o[m]);
+}
+
+// Consumption of plane k (second half): the c_y != 0 populations arriving from
+// the neighbouring rows are read from exchange buffer k&1; with gsh they
+// complete the populations that plane k sends.  Those with c_z = -1 complete
+// output plane k-1 (= zp - 1), which is formed, collided and stored; the
+// c_z = +1 and 0 ones enter the z pipeline.  The arithmetic is branch-free
+// over the warp (so it interleaves with the next production); only the BC
+// solve and the stores are predicated.
+template <int Q, int NM, int NUP, int NMID, typename T, int FLAGS, int TYI>
+__device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const float4* ex4, const float* ex1,
+                                       int lane, int warp, bool interior, int x, int y, const float (&gsh)[Q],
+                                       float (&up_old)[NUP], float (&mid)[NMID], float om_out)
+{
+    constexpr int NW = TYI + 2;
+    const float4* e4 = ex4 + (k & 1) * (6 * NW * 32);
+    const float* e1 = ex1 + (k & 1) * (4 * NW * 32);
+    float g[Q];
+    ex_read<Q, 0>(g, e4, NW, warp, lane);
+    ex_read<Q, 1>(g, e4, NW, warp, lane);
+    ex_read<Q, 2>(g, e4, NW, warp, lane);
+    ex_read<Q, 3>(g, e4, NW, warp, lane);
+    ex_read<Q, 4>(g, e4, NW, warp, lane);
+    ex_read<Q, 5>(g, e4, NW, warp, lane);
+    if constexpr (Q == 19) {
+        static_for<1, Q>([&](auto I) {
+            constexpr int i = I;
+            if constexpr (lat_cy(i) != 0 && !ex_packed(Q, i)) {
                 const int w = min(max(warp - lat_cy(i), 0), NW - 1);
                 const int l = (lane - lat_cx(i)) & 31;
-                g[i] = buf[(lat_cy_slot(Q, i) * NW + w) * 32 + l];
+                g[i] = e1[(ex_scalar_slot(i) * NW + w) * 32 + l];
             }
-        }
-
-        if (k >= 2 && interior) {
-            const int zd = zp - 1;
-            const long long oidx = (long long)zd * a.plane + (long long)y * a.pitch + x;
-            uint8_t cls = CLS_BULK;
-            if constexpr ((FLAGS & F_BC) != 0) cls = __ldg(a.cls + oidx);
-            if (cls != CLS_SOLID) {
-                float p[Q];
-#pragma unroll
-                for (int i = 0; i < Q; i++) {
-                    if (lat_cz(i) > 0) p[i] = up2[lat_cz_slot(Q, i)];
-                    else if (lat_cz(i) == 0) p[i] = mid[lat_cz_slot(Q, i)];
-                    else p[i] = g[i];
-                }
-                const float omega = OMF ? om_prev : a.omega0;
-                float mac[10];
-                if (cls == CLS_BULK) {
-                    float r, j[3], P[6];
-                    lattice_sums<Q>(p, r, j, P);
-                    const float ir = 1.0f / r;
-                    mac[0] = r;
-                    mac[1] = j[0] * ir; mac[2] = j[1] * ir; mac[3] = j[2] * ir;
-                    mac[4] = P[0] * ir - (1.0f / 3.0f);
-                    mac[5] = P[1] * ir;
-                    mac[6] = P[2] * ir;
-                    mac[7] = P[3] * ir - (1.0f / 3.0f);
-                    mac[8] = P[4] * ir;
-                    mac[9] = P[5] * ir - (1.0f / 3.0f);
-                } else {
-                    bc_moments<Q>(a.bc + cls, p, omega, a.omega0, mac);
-                }
-                float o[11];
-                collide<FLAGS>(a, mac, omega, o);
-#pragma unroll
-                for (int m = 0; m < NM; m++) {
-                    const float v = is_f32<T>() ? o[m] : o[m] * a.scale[m];
-                    Stor<T>::st(outp + m * a.field + oidx, v);
-                }
-            }
-        }
-        // rotate the z pipeline
-#pragma unroll
-        for (int s = 0; s < NUP; s++) up2[s] = up1[s];
-#pragma unroll
-        for (int i = 0; i < Q; i++) {
-            if (lat_cz(i) > 0) up1[lat_cz_slot(Q, i)] = g[i];
-            else if (lat_cz(i) == 0) mid[lat_cz_slot(Q, i)] = g[i];
-        }
-        if constexpr (OMF) om_prev = mc[NM - 1];
-#pragma unroll
-        for (int m = 0; m < NM; m++) mc[m] = mn[m];
+        });
     }
+    static_for<0, Q>([&](auto I) {
+        constexpr int i = I;
+        if constexpr (lat_cy(i) == 0) g[i] = gsh[i];
+    });
+
+    if (k >= 2) {
+        const int zd = zp - 1;
+        float p[Q];
+        static_for<0, Q>([&](auto I) {
+            constexpr int i = I;
+            constexpr int slot = lat_cz_slot(Q, i);
+            if constexpr (lat_cz(i) > 0) p[i] = up_old[slot];
+            else if constexpr (lat_cz(i) == 0) p[i] = mid[slot];
+            else p[i] = g[i];
+        });
+        constexpr bool OMF = (FLAGS & (F_POWERLAW | F_BINGHAM)) != 0;
+        const float omega = OMF ? om_out : a.omega0;
+        const long long oidx = pidx(x, y, zd, a.pitch, a.plane);
+        uint8_t cls = CLS_BULK;
+        if constexpr ((FLAGS & F_BC) != 0) cls = interior ? __ldg(a.cls + oidx) : CLS_SOLID;
+        float mac[10];
+        {
+            float r, j[3], P[6];
+            lattice_sums<Q>(p, r, j, P);
+            const float ir = 1.0f / r;
+            mac[0] = r;
+            mac[1] = j[0] * ir; mac[2] = j[1] * ir; mac[3] = j[2] * ir;
+            mac[4] = P[0] * ir - (1.0f / 3.0f);
+            mac[5] = P[1] * ir;
+            mac[6] = P[2] * ir;
+            mac[7] = P[3] * ir - (1.0f / 3.0f);
+            mac[8] = P[4] * ir;
+            mac[9] = P[5] * ir - (1.0f / 3.0f);
+        }
+        if constexpr ((FLAGS & F_BC) != 0) {
+            if (cls != CLS_BULK && cls != CLS_SOLID) bc_moments<Q>(a.bc + cls, p, omega, a.omega0, mac);
+        }
+        float o[11];
+        collide<FLAGS>(a, mac, omega, o);
+        if constexpr (!is_f32<T>()) {
+#pragma unroll
+            for (int m = 0; m < NM; m++) o[m] = o[m] * a.scale[m];
+        }
+        if (interior && cls != CLS_SOLID) {
+            store_node<T, NM>(a, oidx, o);
+            // periodic axes: keep the ghost shell equal to the wrapped interior
+            const bool gx = (a.periodic & 1) && (x == 0 || x == a.nx - 1);
+            const bool gy = (a.periodic & 2) && (y == 0 || y == a.ny - 1);
+            const bool gz = (a.periodic & 4) && (zd == 0 || zd == a.nz - 1);
+            if (gx || gy || gz) {
+                if ((gx && a.nx == 1) || (gy && a.ny == 1) || (gz && a.nz == 1)) {
+                    // degenerate one-node axis: the node has both ghost copies
+#pragma unroll 1
+                    for (int iz = 0; iz < 3; iz++)
+#pragma unroll 1
+                        for (int iy = 0; iy < 3; iy++)
+#pragma unroll 1
+                            for (int ix = 0; ix < 3; ix++) {
+                                const bool vz = iz == 0 || (gz && (iz == 1 ? zd == 0 : zd == a.nz - 1));
+                                const bool vy = iy == 0 || (gy && (iy == 1 ? y == 0 : y == a.ny - 1));
+                                const bool vx = ix == 0 || (gx && (ix == 1 ? x == 0 : x == a.nx - 1));
+                                if (!(vx && vy && vz) || (ix == 0 && iy == 0 && iz == 0)) continue;
+                                const int cz = iz == 0 ? zd : (iz == 1 ? a.nz : -1);
+                                const int cy = iy == 0 ? y : (iy == 1 ? a.ny : -1);
+                                const int cxx = ix == 0 ? x : (ix == 1 ? a.nx : -1);
+                                store_node<T, NM>(a, pidx(cxx, cy, cz, a.pitch, a.plane), o);
+                            }
+                } else {
+                    const int xa = x == 0 ? a.nx : -1, ya = y == 0 ? a.ny : -1, za = zd == 0 ? a.nz : -1;
+                    if (gx) store_node<T, NM>(a, pidx(xa, y, zd, a.pitch, a.plane), o);
+                    if (gy) store_node<T, NM>(a, pidx(x, ya, zd, a.pitch, a.plane), o);
+                    if (gz) store_node<T, NM>(a, pidx(x, y, za, a.pitch, a.plane), o);
+                    if (gx && gy) store_node<T, NM>(a, pidx(xa, ya, zd, a.pitch, a.plane), o);
+                    if (gx && gz) store_node<T, NM>(a, pidx(xa, y, za, a.pitch, a.plane), o);
+                    if (gy && gz) store_node<T, NM>(a, pidx(x, ya, za, a.pitch, a.plane), o);
+                    if (gx && gy && gz) store_node<T, NM>(a, pidx(xa, ya, za, a.pitch, a.plane), o);
+                }
+            }
+        }
+    }
+    // advance the z pipeline: the consumed U(zp-2) slot now holds U(zp)
+    static_for<0, Q>([&](auto I) {
+        constexpr int i = I;
+        constexpr int slot = lat_cz_slot(Q, i);
+        if constexpr (lat_cz(i) > 0) up_old[slot] = g[i];
+        else if constexpr (lat_cz(i) == 0) mid[slot] = g[i];
+    });
+}
+
+// Per-CTA pipeline state and the loop of the z-march over one column.  The
+// TMA ring is indexed by a running production count `g0 + k` so a persistent
+// CTA can chain columns without re-initialising its mbarriers.
+template <int Q, typename T, int FLAGS, int TYI>
+struct ZMarch {
+    static constexpr int NW = TYI + 2;
+    static constexpr int NUP = lat_num_cz(Q, 1);
+    static constexpr int NMID = lat_num_cz(Q, 0);
+    static constexpr bool OMF = (FLAGS & (F_POWERLAW | F_BINGHAM)) != 0;
+    static constexpr int NM = OMF ? 11 : 10;
+    static constexpr size_t stage_bytes = (size_t)NW * NM * BOX_X * sizeof(T);
+    static constexpr size_t stage_al = (stage_bytes + 127) / 128 * 128;
+
+    const StepArgs& a;
+    const CUtensorMap* map;
+    uint64_t* bars;
+    unsigned char* stages;
+    float4* ex4;
+    float* ex1;
+    unsigned g0;
+    int lane, warp, col, x, y, z0, Y0, p0, nprod;
+    bool interior;
+
+    __device__ __forceinline__ int slot(int k) const { return (int)((g0 + (unsigned)k) % NSTAGE); }
+    __device__ __forceinline__ unsigned phase(int k) const { return ((g0 + (unsigned)k) / NSTAGE) & 1u; }
+    // ring stride: the flag-independent maximum (11 moments), see ZSmem
+    static constexpr size_t ring_stride = ((size_t)NW * 11 * BOX_X * sizeof(T) + 127) / 128 * 128;
+    __device__ __forceinline__ const T* stage_of(int k) const
+    {
+        return reinterpret_cast<const T*>(stages + slot(k) * ring_stride);
+    }
+    __device__ __forceinline__ void load(int k) const
+    {
+        const int s = slot(k);
+        mbar_expect_tx(&bars[s], (unsigned)stage_bytes);
+        tma_load_4d(stages + s * ring_stride, map, p0, 0, Y0, z0 + k, &bars[s]);
+    }
+    __device__ __forceinline__ void refill(int k) const
+    {
+        if (threadIdx.x == 0 && k + NSTAGE < nprod) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            load(k + NSTAGE);
+        }
+    }
+
+    // pipeline step j: production j and consumption j-1, one barrier.  The
+    // node output by consumption j-1 lies in the plane of production j-2,
+    // whose stored omega is in om_par (same parity as j) until production j
+    // overwrites it.  Returns false when a bounded wait timed out somewhere
+    // in the CTA.
+    __device__ __forceinline__ bool iter(int j, float (&gsh_new)[Q], const float (&gsh_old)[Q], float (&up)[NUP],
+                                         float (&mid)[NMID], float& om_par) const
+    {
+        const bool ok = mbar_wait(&bars[slot(j)], phase(j));
+        const float om_out = om_par;
+        prod_a<Q, NM, T, TYI>(a, stage_of(j), j, ex4, ex1, lane, warp, col, gsh_new, om_par);
+        prod_b<Q, NM, NUP, NMID, T, FLAGS, TYI>(a, j - 1, z0 - 2 + j, ex4, ex1, lane, warp, interior, x, y, gsh_old,
+                                                up, mid, om_out);
+        if (__syncthreads_or(!ok)) return false;
+        refill(j);
+        return true;
+    }
+};
+
+template <int Q, typename T, int FLAGS, int TYI>
+constexpr size_t zmarch_stage_al()
+{
+    return ZMarch<Q, T, FLAGS, TYI>::stage_al;
+}
+
+// Shared-memory carve-up used by every z-march kernel: barriers, TMA ring,
+// double-buffered exchange.  The ring is sized for 11 moments so kernels that
+// switch between flag sets at run time share one layout.
+template <int Q, typename T, int TYI>
+struct ZSmem {
+    static constexpr int NW = TYI + 2;
+    static constexpr size_t stage_max = ((size_t)NW * 11 * BOX_X * sizeof(T) + 127) / 128 * 128;
+    static constexpr size_t bytes = 128 + NSTAGE * stage_max + 2 * Exchange<Q, NW>::bytes_per_buffer;
+    uint64_t* bars;
+    unsigned char* stages;
+    float4* ex4;
+    float* ex1;
+    __device__ __forceinline__ explicit ZSmem(unsigned char* smem)
+    {
+        bars = reinterpret_cast<uint64_t*>(smem);
+        stages = smem + 128;
+        ex4 = reinterpret_cast<float4*>(stages + NSTAGE * stage_max);
+        ex1 = reinterpret_cast<float*>(ex4 + 2 * 6 * NW * 32);
+    }
+};
+
+// One column (X0, Y0) x planes [z0, z0 + lz) of one domain.  g0 is the
+// CTA's running production count (advanced by the column's productions).
+// Returns false when a bounded wait timed out (the CTA must stop).
+template <int Q, typename T, int FLAGS, int TYI>
+__device__ __forceinline__ bool zmarch_column(const StepArgs& a, const CUtensorMap* map, int X0, int Y0, int z0,
+                                              const ZSmem<Q, T, TYI>& sm, unsigned& g0)
+{
+    using ZM = ZMarch<Q, T, FLAGS, TYI>;
+    constexpr int NUP = ZM::NUP, NMID = ZM::NMID;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int x = X0 - 1 + lane, y = Y0 - 1 + warp;
+    constexpr int ALIGN = 16 / (int)sizeof(T);      // elements per 16 bytes (TMA x alignment)
+    const int p0 = (X0 - 1 + XOFF) & ~(ALIGN - 1);  // aligned box start (padded column)
+    const int zend = min(z0 + a.lz, a.nz);
+    // the ring stride is the flag-independent maximum; ZM's stage_al only
+    // sizes the copies
+    ZM zm{a, map, sm.bars, sm.stages, sm.ex4, sm.ex1, g0, lane, warp, (x + XOFF) - p0, x, y, z0, Y0, p0,
+          zend - z0 + 2 /* planes z0-1 .. zend */,
+          lane >= 1 && lane <= TILE_X && x < a.nx && warp >= 1 && warp <= TYI && y < a.ny};
+
+    if (threadIdx.x == 0)
+        for (int s = 0; s < NSTAGE && s < zm.nprod; s++) zm.load(s);
+
+    float upA[NUP], upB[NUP], mid[NMID], gA[Q], gB[Q];
+#pragma unroll
+    for (int s = 0; s < NUP; s++) upA[s] = upB[s] = 0.f;
+#pragma unroll
+    for (int s = 0; s < NMID; s++) mid[s] = 0.f;
+    float omA = a.omega0, omB = a.omega0;
+
+    int kfail = -1;
+    {
+        // prologue: production 0 only
+        const bool ok = mbar_wait(&sm.bars[zm.slot(0)], zm.phase(0));
+        prod_a<Q, ZM::NM, T, TYI>(a, zm.stage_of(0), 0, sm.ex4, sm.ex1, lane, warp, zm.col, gA, omA);
+        if (__syncthreads_or(!ok)) kfail = 0;
+        else zm.refill(0);
+    }
+    // even productions use gA / upA, odd ones gB / upB: no register copies
+    int j = 1;
+    while (kfail < 0) {
+        // epilogues consume the last production j-1; its output plane is that
+        // of production j-2, whose omega has the parity of j
+        if (j >= zm.nprod) {  // j odd: last production even
+            prod_b<Q, ZM::NM, NUP, NMID, T, FLAGS, TYI>(a, j - 1, z0 - 2 + j, sm.ex4, sm.ex1, lane, warp, zm.interior, x,
+                                                        y, gA, upA, mid, omB);
+            break;
+        }
+        if (!zm.iter(j, gB, gA, upA, mid, omB)) { kfail = j; break; }
+        j++;
+        if (j >= zm.nprod) {  // j even: last production odd
+            prod_b<Q, ZM::NM, NUP, NMID, T, FLAGS, TYI>(a, j - 1, z0 - 2 + j, sm.ex4, sm.ex1, lane, warp, zm.interior, x,
+                                                        y, gB, upB, mid, omA);
+            break;
+        }
+        if (!zm.iter(j, gA, gB, upB, mid, omA)) { kfail = j; break; }
+        j++;
+    }
+    if (kfail >= 0) {
+        // a bounded wait gave up: flag it, give the copies still in flight a
+        // bounded time to land, and leave together
+        if (threadIdx.x == 0) {
+            atomicOr(a.err, 1);
+            for (int q = kfail; q < zm.nprod && q < kfail + NSTAGE; q++) (void)mbar_wait(&sm.bars[zm.slot(q)], zm.phase(q));
+        }
+        __syncthreads();
+        return false;
+    }
+    g0 += (unsigned)zm.nprod;
+    // the last consumption read exchange buffers other warps may overwrite next
+    __syncthreads();
+    return true;
+}
+
+template <int Q, typename T, int TYI>
+__device__ __forceinline__ void zmarch_init_barriers(const ZSmem<Q, T, TYI>& sm)
+{
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < NSTAGE; s++) mbar_init(&sm.bars[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+}
+
+// Single-domain step: one CTA per (x tile, y tile, z chunk).
+template <int Q, typename T, int FLAGS, int TYI>
+__global__ void __launch_bounds__(32 * (TYI + 2), 1)
+    zmarch_step(const __grid_constant__ CUtensorMap map_in, const StepArgs a)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    const ZSmem<Q, T, TYI> sm(smem);
+    zmarch_init_barriers<Q, T, TYI>(sm);
+    unsigned g0 = 0;
+    (void)zmarch_column<Q, T, FLAGS, TYI>(a, &map_in, blockIdx.x * TILE_X, blockIdx.y * TYI, blockIdx.z * a.lz, sm,
+                                          g0);
+}
+
+template <int Q, typename T, int FLAGS, int TYI>
+constexpr size_t step_smem_bytes()
+{
+    return ZSmem<Q, T, TYI>::bytes;
 }
 
 }  // namespace mrlbm

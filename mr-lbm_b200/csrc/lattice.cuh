@@ -7,6 +7,7 @@
 // so it is kept identical.
 #pragma once
 #include <cstdint>
+#include <utility>
 
 namespace mrlbm {
 
@@ -66,6 +67,20 @@ __host__ __device__ constexpr int lat_cz_slot(int Q, int i)
     int n = 0;
     for (int j = 0; j < i; j++) n += lat_cz(j) == lat_cz(i);
     return n;
+}
+
+// Compile-time loop: f(std::integral_constant<int, I>) for I = B .. E-1, so
+// every lattice index (and everything computed from it) is a constant
+// expression and register arrays indexed by it never spill to local memory.
+template <int B, typename F, int... Is>
+__host__ __device__ __forceinline__ void static_for_impl(F&& f, std::integer_sequence<int, Is...>)
+{
+    (f(std::integral_constant<int, B + Is>{}), ...);
+}
+template <int B, int E, typename F>
+__host__ __device__ __forceinline__ void static_for(F&& f)
+{
+    static_for_impl<B>(f, std::make_integer_sequence<int, E - B>{});
 }
 
 }  // namespace mrlbm

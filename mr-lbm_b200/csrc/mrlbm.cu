@@ -221,8 +221,8 @@ extern "C" mrlbm_status mrlbm_domain_bytes(const mrlbm_desc* d, size_t* bytes)
 {
     mrlbm_status st = validate(d);
     if (st) return st;
-    const size_t pitch = (size_t)((d->nx + 7) / 8 * 8);
-    const size_t field = pitch * d->ny * d->nz;
+    const size_t pitch = (size_t)((d->nx + XOFF + 1 + 7) / 8 * 8);
+    const size_t field = pitch * (d->ny + 2) * (d->nz + 2);
     *bytes = 2 * field * moments_of(*d) * elem_size(d->storage) + field;
     return MRLBM_OK;
 }
@@ -233,9 +233,9 @@ mrlbm_status mrlbm::domain_alloc(mrlbm_domain* dom)
     dom->q = d.lattice;
     dom->nm = moments_of(d);
     dom->esize = elem_size(d.storage);
-    dom->pitch = (d.nx + 7) / 8 * 8;
-    dom->plane = (long long)dom->pitch * d.ny;
-    dom->field = dom->plane * d.nz;
+    dom->pitch = (d.nx + XOFF + 1 + 7) / 8 * 8;
+    dom->plane = (long long)dom->pitch * (d.ny + 2);
+    dom->field = dom->plane * (d.nz + 2);
     dom->omega0 = 1.0 / d.tau;
     storage_scales(d.storage, dom->scale, dom->iscale);
     const size_t mbytes = (size_t)dom->field * dom->nm * dom->esize;
@@ -266,6 +266,12 @@ mrlbm_status mrlbm::domain_alloc(mrlbm_domain* dom)
     CK(cudaEventCreate(&dom->ev1));
     CK(cudaMalloc(&dom->cls, (size_t)dom->field));
     CK(cudaMemset(dom->cls, 0, (size_t)dom->field));
+    CK(cudaMalloc(&dom->err, sizeof(int)));
+    CK(cudaMemset(dom->err, 0, sizeof(int)));
+    {
+        mrlbm_status st = make_tensor_maps(dom);
+        if (st) return st;
+    }
     CK(cudaMalloc(&dom->bc, sizeof(BcClass)));
     CK(cudaMemset(dom->bc, 0, sizeof(BcClass)));
     dom->red_blocks = 148 * 4;
@@ -320,6 +326,7 @@ extern "C" mrlbm_status mrlbm_domain_destroy(mrlbm_domain* dom)
     cudaFree(dom->m[0]);
     cudaFree(dom->m[1]);
     cudaFree(dom->cls);
+    cudaFree(dom->err);
     cudaFree(dom->bc);
     cudaFree(dom->red_scratch);
     cudaFree(dom->usnap);
@@ -376,7 +383,7 @@ extern "C" mrlbm_status mrlbm_set_node_types(mrlbm_domain* dom, const uint32_t* 
     std::vector<uint8_t> padded((size_t)dom->field, 0);
     for (int z = 0; z < d.nz; z++)
         for (int y = 0; y < d.ny; y++)
-            memcpy(&padded[(size_t)z * dom->plane + (size_t)y * dom->pitch], &cls[((size_t)z * d.ny + y) * d.nx], d.nx);
+            memcpy(&padded[(size_t)pidx(0, y, z, dom->pitch, dom->plane)], &cls[((size_t)z * d.ny + y) * d.nx], d.nx);
     CK(cudaMemcpyAsync(dom->cls, padded.data(), padded.size(), cudaMemcpyHostToDevice, dom->stream));
     cudaFree(dom->bc);
     dom->bc = nullptr;
@@ -419,6 +426,10 @@ static mrlbm_status run_init(mrlbm_domain* dom, InitArgs& a)
     memcpy(a.scale, dom->scale, sizeof(a.scale));
     if (d.lattice == 19) launch_init<19>(dom, a); else launch_init<27>(dom, a);
     CK(cudaGetLastError());
+    {
+        mrlbm_status st = fill_ghosts(dom);
+        if (st) return st;
+    }
     CK(cudaStreamSynchronize(dom->stream));
     dom->cur = 0;
     dom->step = 0;
@@ -470,8 +481,8 @@ extern "C" mrlbm_status mrlbm_init_taylor_green(mrlbm_domain* dom, double u0, do
 void mrlbm::fill_step_args(const mrlbm_domain* dom, StepArgs& a, int parity, int& flags)
 {
     const mrlbm_desc& d = dom->d;
-    a.m_in = dom->m[parity];
     a.m_out = dom->m[parity ^ 1];
+    a.err = dom->err;
     a.cls = dom->cls;
     a.bc = dom->bc;
     a.nx = d.nx; a.ny = d.ny; a.nz = d.nz; a.pitch = dom->pitch;
@@ -483,7 +494,6 @@ void mrlbm::fill_step_args(const mrlbm_domain* dom, StepArgs& a, int parity, int
     a.fx = (float)d.force[0]; a.fy = (float)d.force[1]; a.fz = (float)d.force[2];
     a.nnf_n = (float)d.nnf_n; a.nnf_k = (float)d.nnf_k;
     a.nnf_yield = (float)d.nnf_yield; a.nnf_omega_p = (float)d.nnf_omega_p;
-    memcpy(a.ext, dom->ext, sizeof(a.ext));
     memcpy(a.scale, dom->scale, sizeof(a.scale));
     memcpy(a.iscale, dom->iscale, sizeof(a.iscale));
     flags = 0;
@@ -502,14 +512,15 @@ mrlbm_status mrlbm::enqueue_step(mrlbm_domain* dom, int parity, cudaStream_t s)
     const int q = dom->q;
     const int stg = dom->d.storage;
     mrlbm_status st;
+    const CUtensorMap& map = dom->tmap[parity];
     if (q == 19) {
-        if (stg == MRLBM_F32) st = dispatch_step<19, float>(a, flags, s);
-        else if (stg == MRLBM_F16) st = dispatch_step<19, __half>(a, flags, s);
-        else st = dispatch_step<19, __nv_bfloat16>(a, flags, s);
+        if (stg == MRLBM_F32) st = dispatch_step<19, float>(map, a, flags, s);
+        else if (stg == MRLBM_F16) st = dispatch_step<19, __half>(map, a, flags, s);
+        else st = dispatch_step<19, __nv_bfloat16>(map, a, flags, s);
     } else {
-        if (stg == MRLBM_F32) st = dispatch_step<27, float>(a, flags, s);
-        else if (stg == MRLBM_F16) st = dispatch_step<27, __half>(a, flags, s);
-        else st = dispatch_step<27, __nv_bfloat16>(a, flags, s);
+        if (stg == MRLBM_F32) st = dispatch_step<27, float>(map, a, flags, s);
+        else if (stg == MRLBM_F16) st = dispatch_step<27, __half>(map, a, flags, s);
+        else st = dispatch_step<27, __nv_bfloat16>(map, a, flags, s);
     }
     return st;
 }
@@ -572,6 +583,18 @@ extern "C" mrlbm_status mrlbm_time_steps(mrlbm_domain* dom, int nsteps, float* m
     CK(cudaEventRecord(dom->ev1, dom->stream));
     CK(cudaEventSynchronize(dom->ev1));
     CK(cudaEventElapsedTime(ms, dom->ev0, dom->ev1));
+    return check_device_error(dom);
+}
+
+mrlbm_status mrlbm::check_device_error(mrlbm_domain* dom)
+{
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, dom->err, sizeof(int), cudaMemcpyDeviceToHost, dom->stream));
+    CK(cudaStreamSynchronize(dom->stream));
+    if (h) {
+        CK(cudaMemsetAsync(dom->err, 0, sizeof(int), dom->stream));
+        return fail(MRLBM_ETIMEDOUT, "a step kernel gave up waiting for its tile loads (flag 0x%x)", h);
+    }
     return MRLBM_OK;
 }
 
@@ -579,7 +602,7 @@ extern "C" mrlbm_status mrlbm_synchronize(mrlbm_domain* dom)
 {
     if (!dom) return fail(MRLBM_EINVAL, "null domain");
     CK(cudaStreamSynchronize(dom->stream));
-    return MRLBM_OK;
+    return check_device_error(dom);
 }
 
 extern "C" mrlbm_status mrlbm_get_step(mrlbm_domain* dom, int* step)
@@ -621,7 +644,12 @@ static mrlbm_status convert(mrlbm_domain* dom, float* hbuf_out, const float* hbu
         e = cudaMemcpyAsync(hbuf_out, dbuf, n * sizeof(float), cudaMemcpyDeviceToHost, dom->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(dom->stream);
     if (e != cudaSuccess) return fail(MRLBM_ECUDA, "convert: %s", cudaGetErrorString(e));
-    if (mode == 1 || mode == 3) dom->have_snap = false;
+    if (mode == 1 || mode == 3) {
+        dom->have_snap = false;
+        mrlbm_status st = fill_ghosts(dom);
+        if (st) return st;
+        CK(cudaStreamSynchronize(dom->stream));
+    }
     return MRLBM_OK;
 }
 
@@ -670,6 +698,79 @@ extern "C" mrlbm_status mrlbm_get_macr(mrlbm_domain* dom, float* rho, float* ux,
         if (dom->nm < 11) return fail(MRLBM_EINVAL, "domain has no omega field");
         memcpy(omega, &all[10 * n], n * sizeof(float));
     }
+    return MRLBM_OK;
+}
+
+// ------------------------------------------------------- TMA tensor maps
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn()
+{
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+// 4-D map over one padded moment buffer with dimension order (x, moment, y, z)
+// so that a box of (40, nm, TILE_Y+2, 1) lands in shared memory as
+// [row][moment][x]: one plane of a CTA column per copy.
+mrlbm_status mrlbm::make_tensor_maps(mrlbm_domain* dom)
+{
+    EncodeTiledFn enc = encode_fn();
+    if (!enc) return fail(MRLBM_ECUDA, "cuTensorMapEncodeTiled unavailable");
+    const mrlbm_desc& d = dom->d;
+    const CUtensorMapDataType dt = d.storage == MRLBM_F32   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                   : d.storage == MRLBM_F16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                                            : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    const cuuint64_t es = dom->esize;
+    const cuuint64_t dims[4] = {(cuuint64_t)dom->pitch, (cuuint64_t)dom->nm, (cuuint64_t)(d.ny + 2),
+                                (cuuint64_t)(d.nz + 2)};
+    const cuuint64_t strides[3] = {(cuuint64_t)dom->field * es, (cuuint64_t)dom->pitch * es,
+                                   (cuuint64_t)dom->plane * es};
+    const cuuint32_t box[4] = {(cuuint32_t)BOX_X, (cuuint32_t)dom->nm, (cuuint32_t)(TILE_Y + 2), 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    for (int b = 0; b < 2; b++) {
+        CUresult r = enc(&dom->tmap[b], dt, 4, dom->m[b], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return fail(MRLBM_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    }
+    return MRLBM_OK;
+}
+
+mrlbm_status mrlbm::fill_ghosts(mrlbm_domain* dom)
+{
+    const mrlbm_desc& d = dom->d;
+    GhostArgs g{};
+    g.m0 = dom->m[0];
+    g.m1 = dom->m[1];
+    g.nx = d.nx; g.ny = d.ny; g.nz = d.nz; g.pitch = dom->pitch;
+    g.plane = dom->plane; g.field = dom->field;
+    g.nm = dom->nm;
+    g.periodic = (d.periodic[0] ? 1 : 0) | (d.periodic[1] ? 2 : 0) | (d.periodic[2] ? 4 : 0);
+    memcpy(g.ext, dom->ext, sizeof(g.ext));
+    memcpy(g.scale, dom->scale, sizeof(g.scale));
+    const long long n = (long long)(d.nx + 2) * (d.ny + 2) * (d.nz + 2);
+    const int threads = 256;
+    const int blocks = (int)std::min<long long>((n + threads - 1) / threads, 148LL * 16);
+    // the copy reads buffer 0 and writes both: buffer 0 must be the current state
+    if (dom->cur != 0) {
+        g.m0 = dom->m[1];
+        g.m1 = dom->m[0];
+    }
+    if (d.storage == MRLBM_F32) ghost_fill_kernel<float><<<blocks, threads, 0, dom->stream>>>(g);
+    else if (d.storage == MRLBM_F16) ghost_fill_kernel<__half><<<blocks, threads, 0, dom->stream>>>(g);
+    else ghost_fill_kernel<__nv_bfloat16><<<blocks, threads, 0, dom->stream>>>(g);
+    CK(cudaGetLastError());
     return MRLBM_OK;
 }
 

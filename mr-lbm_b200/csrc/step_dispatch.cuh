@@ -10,10 +10,11 @@
 namespace mrlbm {
 
 template <int Q, typename T, int FLAGS>
-static mrlbm_status launch_step_t(const StepArgs& a, cudaStream_t s)
+static mrlbm_status launch_step_t(const CUtensorMap& map, const StepArgs& a, cudaStream_t s)
 {
     constexpr int NW = TILE_Y + 2;
-    const size_t smem = 2u * lat_num_cy(Q) * NW * 32 * sizeof(float);
+    constexpr size_t smem = step_smem_bytes<Q, T, FLAGS, TILE_Y>();
+    static_assert(smem <= 232448, "shared memory over the sm_100 limit");
     auto kern = zmarch_step<Q, T, FLAGS, TILE_Y>;
     int dev = 0;
     cudaGetDevice(&dev);
@@ -24,22 +25,22 @@ static mrlbm_status launch_step_t(const StepArgs& a, cudaStream_t s)
         attr_done_mask |= 1 << (dev & 31);
     }
     dim3 grid((a.nx + TILE_X - 1) / TILE_X, (a.ny + TILE_Y - 1) / TILE_Y, (a.nz + a.lz - 1) / a.lz);
-    kern<<<grid, 32 * NW, smem, s>>>(a);
+    kern<<<grid, 32 * NW, smem, s>>>(map, a);
     return MRLBM_OK;
 }
 
 template <int Q, typename T>
-mrlbm_status dispatch_step(const StepArgs& a, int flags, cudaStream_t s)
+mrlbm_status dispatch_step(const CUtensorMap& map, const StepArgs& a, int flags, cudaStream_t s)
 {
     switch (flags) {
-        case 0: return launch_step_t<Q, T, 0>(a, s);
-        case F_BC: return launch_step_t<Q, T, F_BC>(a, s);
-        case F_FORCE: return launch_step_t<Q, T, F_FORCE>(a, s);
-        case F_BC | F_FORCE: return launch_step_t<Q, T, F_BC | F_FORCE>(a, s);
-        case F_BC | F_POWERLAW: return launch_step_t<Q, T, F_BC | F_POWERLAW>(a, s);
-        case F_BC | F_FORCE | F_POWERLAW: return launch_step_t<Q, T, F_BC | F_FORCE | F_POWERLAW>(a, s);
-        case F_BC | F_BINGHAM: return launch_step_t<Q, T, F_BC | F_BINGHAM>(a, s);
-        case F_BC | F_FORCE | F_BINGHAM: return launch_step_t<Q, T, F_BC | F_FORCE | F_BINGHAM>(a, s);
+        case 0: return launch_step_t<Q, T, 0>(map, a, s);
+        case F_BC: return launch_step_t<Q, T, F_BC>(map, a, s);
+        case F_FORCE: return launch_step_t<Q, T, F_FORCE>(map, a, s);
+        case F_BC | F_FORCE: return launch_step_t<Q, T, F_BC | F_FORCE>(map, a, s);
+        case F_BC | F_POWERLAW: return launch_step_t<Q, T, F_BC | F_POWERLAW>(map, a, s);
+        case F_BC | F_FORCE | F_POWERLAW: return launch_step_t<Q, T, F_BC | F_FORCE | F_POWERLAW>(map, a, s);
+        case F_BC | F_BINGHAM: return launch_step_t<Q, T, F_BC | F_BINGHAM>(map, a, s);
+        case F_BC | F_FORCE | F_BINGHAM: return launch_step_t<Q, T, F_BC | F_FORCE | F_BINGHAM>(map, a, s);
         default: return fail(MRLBM_EINVAL, "unsupported step flag combination %d", flags);
     }
 }

