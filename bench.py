@@ -302,6 +302,145 @@ def run_gpu_arm(args):
     return 0
 
 
+def run_batch_workload(args):
+    """256 lid cavities, edges U{24..96} per axis, Re U[50, 1000], lid 0.05,
+    advanced together by the persistent batched kernel (graph replay, chunk
+    autotuner), against the same cavities solved one at a time with plain
+    single-domain launches.  Each member's arithmetic is identical in both
+    (bit-identical results, tests/test_gpu_batch.py), so accuracy is equal."""
+    import mrlbm
+
+    mrlbm.set_device(0)
+    rng = np.random.default_rng(20261203)
+    ndom = args.domains
+    sizes = rng.integers(24, 97, size=(ndom, 3))
+    res = rng.uniform(50.0, 1000.0, size=ndom)
+    steps = args.batch_steps
+    out = []
+    for storage, sname in ((mrlbm.F16, "fp16"), (mrlbm.F32, "fp32")):
+        b = mrlbm.Batch(mrlbm.D3Q19, storage)
+        mem = []
+        for k in range(ndom):
+            nx, ny, nz = (int(v) for v in sizes[k])
+            d = mrlbm.lid_cavity_desc(nx, re=float(res[k]), lid_u=0.05, storage=storage, ny=ny, nz=nz)
+            m = b.add(d)
+            m.set_node_types(mrlbm.lid_cavity_node_types(nx, ny, nz, 1))
+            m.init_uniform()
+            mem.append(m)
+        t0 = time.perf_counter()
+        b.autotune()
+        t_tune = time.perf_counter() - t0
+        for m in mem:
+            m.init_uniform()
+        info = b.info()
+        b.step(16)
+        b.synchronize()
+        ms = b.time_steps(steps)
+        nodes = info["nodes"]
+        healthy = all(m.sums()["nonfinite"] == 0 for m in mem)
+        # one at a time: each cavity alone, plain launches, per-step time
+        # measured over `alone_steps` steps and scaled to the run length
+        t_alone = 0.0
+        for k in range(ndom):
+            nx, ny, nz = (int(v) for v in sizes[k])
+            d = mrlbm.lid_cavity_desc(nx, re=float(res[k]), lid_u=0.05, storage=storage, ny=ny, nz=nz)
+            dom = mrlbm.Domain(d)
+            dom.set_node_types(mrlbm.lid_cavity_node_types(nx, ny, nz, 1))
+            dom.init_uniform()
+            dom.step(3)
+            t_alone += dom.time_steps(args.alone_steps) / args.alone_steps * steps
+            dom.close()
+        b.close()
+        out.append({"storage": sname, "solves_per_s": ndom / (ms * 1e-3), "mlups": nodes * steps / (ms * 1e-3) / 1e6,
+                    "ms": ms, "alone_solves_per_s": ndom / (t_alone * 1e-3), "speedup_vs_alone": t_alone / ms,
+                    "items": info["items"], "nodes": nodes, "autotune_s": round(t_tune, 2), "finite": healthy})
+    line = {"metric": "batched solves/s (256 lid cavities, %d steps each)" % steps, "value": round(out[0]["solves_per_s"], 3),
+            "unit": "solves/s", "n_gpus": 1, "steps": steps, "higher_is_better": True, "dtype": "f16 storage, f32 arithmetic",
+            "data": "synthetic (seed 20261203)",
+            "config": {"workload": "batched_cavities_256_d3q19", "edges": "U{24..96} per axis", "re": "U[50,1000]",
+                       "lid": 0.05, "alone_steps_timed": args.alone_steps},
+            "variants": out}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_serve_workload(args):
+    """Poisson arrivals (mean 200/s) of D3Q19 solves, 50/50 lid cavities and
+    power-law ducts with 5 % voxel obstacles, edges U{32..192}, FP16 storage,
+    each until residual <= 1e-6 or 20k steps, HBM budget 150 GB; then the same
+    requests solved one at a time with plain single-domain launches."""
+    import mrlbm
+
+    mrlbm.set_device(0)
+    rng = np.random.default_rng(20261203)
+    count = args.requests
+    gaps = rng.exponential(1.0 / args.rate, size=count)
+    arrivals = np.cumsum(gaps)
+    reqs = []
+    for k in range(count):
+        n = int(rng.integers(32, 193))
+        if rng.random() < 0.5:
+            reqs.append(mrlbm.make_request(mrlbm.REQ_LID_CAVITY, n, re=float(rng.uniform(50, 1000))))
+        else:
+            reqs.append(mrlbm.make_request(mrlbm.REQ_DUCT, n, nnf_n=float(rng.uniform(0.6, 1.2)), solid_fraction=0.05,
+                                           seed=int(rng.integers(1 << 62))))
+    srv = mrlbm.Server(storage=mrlbm.F16, hbm_budget=150e9, max_active=args.max_active, steps_per_tick=100,
+                       residual_tol=1e-6, max_steps=args.max_steps)
+    t0 = srv.now()
+    ids = []
+    for r, a in zip(reqs, arrivals):
+        r.arrival = t0 + float(a)
+        ids.append(srv.submit(r))
+    wall0 = time.perf_counter()
+    while True:
+        active = srv.tick()
+        st = srv.stats()
+        if active == 0 and st["queued"] == 0:
+            break
+        if active == 0:
+            time.sleep(0.001)  # waiting for the next arrival
+    wall = time.perf_counter() - wall0
+    stats = srv.stats()
+    steps_done = [srv.result(i)["steps"] for i in ids]
+    srv.close()
+    # one at a time, plain launches, same convergence rule
+    t_alone = 0.0
+    lat_alone = []
+    clock = 0.0
+    for r, a in zip(reqs, arrivals):
+        dom = mrlbm.request_domain(r, mrlbm.F16)
+        dom.residual()
+        t1 = time.perf_counter()
+        steps = 0
+        while steps < args.max_steps:
+            dom.step(100)
+            steps += 100
+            if dom.residual() <= 1e-6:
+                break
+        dom.synchronize()
+        dt = time.perf_counter() - t1
+        dom.close()
+        t_alone += dt
+        clock = max(clock, float(a)) + dt
+        lat_alone.append(clock - float(a))
+    line = {"metric": "serving solves/s and latency (continuous batching)", "value": round(stats["solves_per_s"], 4),
+            "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f16 storage, f32 arithmetic",
+            "data": "synthetic (seed 20261203)",
+            "config": {"workload": "serving_poisson_d3q19", "rate_per_s": args.rate, "requests": count,
+                       "edges": "U{32..192}", "mix": "50/50 lid cavity / power-law duct (5% obstacles)",
+                       "residual_tol": 1e-6, "max_steps": args.max_steps, "hbm_budget_gb": 150},
+            "p50_latency_s": stats["p50_latency"], "p99_latency_s": stats["p99_latency"],
+            "mean_latency_s": stats["mean_latency"], "done": stats["done"], "failed": stats["failed"],
+            "wall_s": round(wall, 3), "lattice_updates": stats["lattice_updates"],
+            "mlups": stats["lattice_updates"] / wall / 1e6,
+            "alone": {"solves_per_s": count / t_alone, "p50_latency_s": float(np.percentile(lat_alone, 50)),
+                      "p99_latency_s": float(np.percentile(lat_alone, 99))},
+            "speedup_vs_alone": (stats["solves_per_s"] / (count / t_alone)) if t_alone > 0 else None,
+            "steps_per_request": {"min": int(min(steps_done)), "max": int(max(steps_done))}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -310,9 +449,23 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "batch", "serve"],
+                    help="tgv: the headline step benchmark (default); batch / serve: the batched-cavity and "
+                         "serving workloads (longer, run on their own)")
+    ap.add_argument("--domains", type=int, default=256)
+    ap.add_argument("--batch-steps", type=int, default=5000)
+    ap.add_argument("--alone-steps", type=int, default=200)
+    ap.add_argument("--requests", type=int, default=32)
+    ap.add_argument("--rate", type=float, default=200.0)
+    ap.add_argument("--max-active", type=int, default=512)
+    ap.add_argument("--max-steps", type=int, default=20000)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "batch":
+        return run_batch_workload(args)
+    if args.workload == "serve":
+        return run_serve_workload(args)
     return run_gpu_arm(args)
 
 

@@ -41,7 +41,8 @@ typedef enum {
     MRLBM_EDIVERGED = 5,  /* NaN/Inf or |u| above the stability limit */
     MRLBM_ETIMEDOUT = 6,  /* a bounded device wait gave up */
     MRLBM_ENOTFOUND = 7,  /* unknown request / handle */
-    MRLBM_EBUSY = 8       /* no free slot */
+    MRLBM_EBUSY = 8,      /* no free slot / request still queued or running */
+    MRLBM_ECANCELED = 9   /* request cancelled */
 } mrlbm_status;
 
 typedef enum { MRLBM_D3Q19 = 19, MRLBM_D3Q27 = 27 } mrlbm_lattice;
@@ -205,6 +206,75 @@ mrlbm_status mrlbm_batch_info(mrlbm_batch* batch, int* members, int* items, long
 mrlbm_status mrlbm_batch_autotune(mrlbm_batch* batch);
 /* The z-chunk length the batch uses for a domain of this size. */
 mrlbm_status mrlbm_batch_chunk_for(mrlbm_batch* batch, int nx, int ny, int nz, int* lz);
+
+/* ------------------------------------------------------------------ serving
+ * A continuous-batching solve server (no counterpart in the reference, which
+ * runs one case per process).  Requests queue in arrival order; a tick admits
+ * queued requests while their device bytes fit the HBM budget and a slot is
+ * free, advances every active solve by steps_per_tick steps in one batch,
+ * then retires solves whose residual ||u^n - u^(n-k)|| / ||u^n|| (FP64, k =
+ * steps_per_tick) is at most residual_tol, that reached max_steps, or that
+ * diverged (NaN/Inf or |u| > 0.3: status MRLBM_EDIVERGED).  Times are seconds
+ * on the server's monotonic clock; latency = retirement - arrival. */
+typedef struct mrlbm_server mrlbm_server;
+
+typedef enum { MRLBM_REQ_LID_CAVITY = 0, MRLBM_REQ_DUCT = 1 } mrlbm_request_kind;
+
+typedef struct {
+    int kind;               /* mrlbm_request_kind */
+    int n;                  /* cubic edge length */
+    double re;              /* cavity: Reynolds number (lid 0.05, tau from Re) */
+    double lid_u;           /* cavity: lid velocity (0: 0.05) */
+    double nnf_n;           /* duct: power-law index */
+    double tau;             /* duct: tau of the consistency K = rho0 (tau - 1/2) / 3 (0: 0.8) */
+    double force_z;         /* duct: body force along z (0: sized for u_max ~ 0.05) */
+    double solid_fraction;  /* duct: Bernoulli obstacle fraction on interior nodes */
+    uint64_t seed;          /* duct: obstacle mask seed */
+    double arrival;         /* arrival time (seconds, server clock); < 0: now */
+} mrlbm_request;
+
+typedef struct {
+    int status;             /* MRLBM_OK done, MRLBM_EBUSY queued/running, MRLBM_EDIVERGED, ... */
+    int steps;
+    double residual;
+    double arrival, admitted, finished;  /* server clock, seconds */
+} mrlbm_request_result;
+
+typedef struct {
+    int queued, active, done, failed;
+    double hbm_in_use;      /* bytes */
+    double p50_latency, p99_latency, mean_latency;  /* seconds, over finished solves */
+    double solves_per_s;    /* finished solves / (last finish - first arrival) */
+    double lattice_updates; /* total node updates done */
+} mrlbm_server_stats;
+
+mrlbm_status mrlbm_server_create(int storage, double hbm_budget_bytes, int max_active, int steps_per_tick,
+                                 double residual_tol, int max_steps, mrlbm_server** out);
+mrlbm_status mrlbm_server_destroy(mrlbm_server* srv);
+/* Queue a request; *rid receives its id.  Requests that could never fit the
+ * budget are refused with MRLBM_ENOMEM. */
+mrlbm_status mrlbm_server_submit(mrlbm_server* srv, const mrlbm_request* req, int* rid);
+mrlbm_status mrlbm_server_cancel(mrlbm_server* srv, int rid);
+/* One scheduling tick (admit, step, retire).  *active receives the number of
+ * running solves after the tick (0 and an empty queue: idle). */
+mrlbm_status mrlbm_server_tick(mrlbm_server* srv, int* active);
+mrlbm_status mrlbm_server_result(mrlbm_server* srv, int rid, mrlbm_request_result* out);
+/* Final moments of a finished request (float [moment][z][y][x]); kept until
+ * mrlbm_server_release. */
+mrlbm_status mrlbm_server_moments(mrlbm_server* srv, int rid, float* m, size_t count);
+mrlbm_status mrlbm_server_release(mrlbm_server* srv, int rid);
+mrlbm_status mrlbm_server_stats_get(mrlbm_server* srv, mrlbm_server_stats* out);
+mrlbm_status mrlbm_server_now(mrlbm_server* srv, double* t);
+/* Test hook: replace one node's moments of an admitted request with NaN
+ * (host-side fault injection; the divergence watch must retire it). */
+mrlbm_status mrlbm_server_inject_nan(mrlbm_server* srv, int rid);
+/* Keep each finished request's final moments on the host for
+ * mrlbm_server_moments (off by default: large requests are hundreds of MB). */
+mrlbm_status mrlbm_server_keep_results(mrlbm_server* srv, int on);
+/* A standalone domain for a request, set up exactly as the server sets up
+ * its batch member (description, node types, initial state): for solving a
+ * request alone with the single-domain calls. */
+mrlbm_status mrlbm_request_domain(const mrlbm_request* req, int storage, mrlbm_domain** out);
 
 /* Host-side node-type builders (no device work).
  * Voxel geometry: solid (x-fastest, nonzero = solid) -> nodeTypeMap words: solid

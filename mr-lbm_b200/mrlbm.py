@@ -66,6 +66,26 @@ class Sums(C.Structure):
                 "fluid_nodes": self.fluid_nodes, "max_speed": self.max_speed, "nonfinite": self.nonfinite}
 
 
+REQ_LID_CAVITY, REQ_DUCT = 0, 1
+
+
+class Request(C.Structure):
+    _fields_ = [("kind", C.c_int), ("n", C.c_int), ("re", C.c_double), ("lid_u", C.c_double),
+                ("nnf_n", C.c_double), ("tau", C.c_double), ("force_z", C.c_double),
+                ("solid_fraction", C.c_double), ("seed", C.c_uint64), ("arrival", C.c_double)]
+
+
+class RequestResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("steps", C.c_int), ("residual", C.c_double), ("arrival", C.c_double),
+                ("admitted", C.c_double), ("finished", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("queued", C.c_int), ("active", C.c_int), ("done", C.c_int), ("failed", C.c_int),
+                ("hbm_in_use", C.c_double), ("p50_latency", C.c_double), ("p99_latency", C.c_double),
+                ("mean_latency", C.c_double), ("solves_per_s", C.c_double), ("lattice_updates", C.c_double)]
+
+
 _lib = None
 FP = C.POINTER(C.c_float)
 VP = C.c_void_p
@@ -125,6 +145,19 @@ def lib():
             "mrlbm_batch_info": [VP, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_longlong)],
             "mrlbm_batch_autotune": [VP],
             "mrlbm_batch_chunk_for": [VP, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int)],
+            "mrlbm_server_create": [C.c_int, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int, C.POINTER(VP)],
+            "mrlbm_server_destroy": [VP],
+            "mrlbm_server_submit": [VP, C.POINTER(Request), C.POINTER(C.c_int)],
+            "mrlbm_server_cancel": [VP, C.c_int],
+            "mrlbm_server_tick": [VP, C.POINTER(C.c_int)],
+            "mrlbm_server_result": [VP, C.c_int, C.POINTER(RequestResult)],
+            "mrlbm_server_moments": [VP, C.c_int, FP, C.c_size_t],
+            "mrlbm_server_release": [VP, C.c_int],
+            "mrlbm_server_stats_get": [VP, C.POINTER(ServerStats)],
+            "mrlbm_server_now": [VP, C.POINTER(C.c_double)],
+            "mrlbm_server_inject_nan": [VP, C.c_int],
+            "mrlbm_server_keep_results": [VP, C.c_int],
+            "mrlbm_request_domain": [C.POINTER(Request), C.c_int, C.POINTER(VP)],
         }
         for name, args in sigs.items():
             f = getattr(L, name)
@@ -406,6 +439,96 @@ class Batch:
         lz = C.c_int()
         check(self.L.mrlbm_batch_chunk_for(self.h, nx, ny, nz, C.byref(lz)))
         return lz.value
+
+
+def make_request(kind, n, re=100.0, lid_u=0.0, nnf_n=1.0, tau=0.0, force_z=0.0, solid_fraction=0.05, seed=0,
+                 arrival=-1.0):
+    r = Request()
+    r.kind, r.n, r.re, r.lid_u, r.nnf_n, r.tau = kind, n, re, lid_u, nnf_n, tau
+    r.force_z, r.solid_fraction, r.seed, r.arrival = force_z, solid_fraction, seed, arrival
+    return r
+
+
+class _Owned(Domain):
+    """A Domain built by the library from a request description."""
+
+    def __init__(self, handle, n, nm):
+        self.L = lib()
+        self.h = handle
+        self.nm = nm
+        self.shape = (n, n, n)
+        self.desc = None
+
+
+def request_domain(req, storage=F16):
+    """A standalone Domain set up exactly as the server sets up `req`."""
+    h = VP()
+    check(lib().mrlbm_request_domain(C.byref(req), storage, C.byref(h)))
+    nm = C.c_int()
+    check(lib().mrlbm_num_moments(h, C.byref(nm)))
+    return _Owned(h, req.n, nm.value)
+
+
+class Server:
+    """Continuous-batching solve server (mrlbm_server_* in include/mrlbm.h)."""
+
+    def __init__(self, storage=F16, hbm_budget=150e9, max_active=512, steps_per_tick=100, residual_tol=1e-6,
+                 max_steps=20000, keep_results=False):
+        self.L = lib()
+        h = VP()
+        check(self.L.mrlbm_server_create(storage, float(hbm_budget), int(max_active), int(steps_per_tick),
+                                         float(residual_tol), int(max_steps), C.byref(h)))
+        self.h = h
+        if keep_results:
+            check(self.L.mrlbm_server_keep_results(self.h, 1))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.mrlbm_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def submit(self, req):
+        rid = C.c_int()
+        check(self.L.mrlbm_server_submit(self.h, C.byref(req), C.byref(rid)))
+        return rid.value
+
+    def cancel(self, rid):
+        check(self.L.mrlbm_server_cancel(self.h, rid))
+
+    def tick(self):
+        a = C.c_int()
+        check(self.L.mrlbm_server_tick(self.h, C.byref(a)))
+        return a.value
+
+    def result(self, rid):
+        r = RequestResult()
+        check(self.L.mrlbm_server_result(self.h, rid, C.byref(r)))
+        return {"status": r.status, "steps": r.steps, "residual": r.residual, "arrival": r.arrival,
+                "admitted": r.admitted, "finished": r.finished}
+
+    def moments(self, rid, n, nm=10):
+        m = np.empty((nm, n, n, n), dtype=np.float32)
+        check(self.L.mrlbm_server_moments(self.h, rid, _fp(m), m.size))
+        return m
+
+    def release(self, rid):
+        check(self.L.mrlbm_server_release(self.h, rid))
+
+    def stats(self):
+        s = ServerStats()
+        check(self.L.mrlbm_server_stats_get(self.h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in ServerStats._fields_}
+
+    def now(self):
+        t = C.c_double()
+        check(self.L.mrlbm_server_now(self.h, C.byref(t)))
+        return t.value
+
+    def inject_nan(self, rid):
+        check(self.L.mrlbm_server_inject_nan(self.h, rid))
 
 
 def bc_class_info(lattice, node_type, bc_velocity, omega0, bc_matrix_q=0):

@@ -82,6 +82,42 @@ def test_lid_cavity(lattice):
     assert_close(res, l2=5e-5, linf=5e-4)
 
 
+def test_duct_voxels_force_newtonian():
+    nx, ny, nz = 20, 18, 24
+    rng = np.random.default_rng(9)
+    solid = np.zeros((nz, ny, nx), dtype=np.uint8)
+    solid[:, 1:-1, 1:-1] = rng.random((nz, ny - 2, nx - 2)) < 0.05
+    nt = mrlbm.voxel_node_types(solid, (0, 0, 1))
+    d = mrlbm.make_desc(nx, ny, nz, lattice=19, periodic=(0, 0, 1), tau=0.8, force=(0, 0, 2e-5))
+    g, o, res = run_pair(d, 150, node_types=nt, fluid=solid == 0)
+    assert_close(res)
+
+
+def sheared_start(nx, ny, nz, gamma=2e-3):
+    """u_x = gamma (y - ny/2) plus a z wave: |S| is far from the power-law
+    cut-off (1e-6) and from a Bingham yield stress of 1e-5 everywhere."""
+    z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    ux = gamma * (y - ny / 2) + 0.01 * np.sin(2 * np.pi * z / nz)
+    uy = 0.005 * np.sin(2 * np.pi * x / nx)
+    uz = 0.005 * np.cos(2 * np.pi * y / ny)
+    return lambda dom: dom.init_flow(np.ones_like(ux), ux, uy, uz)
+
+
+@pytest.mark.parametrize("rheology,kw", [(mrlbm.POWERLAW, dict(nnf_n=0.7)), (mrlbm.POWERLAW, dict(nnf_n=1.15)),
+                                         (mrlbm.BINGHAM, dict(nnf_yield=1e-5))])
+def test_nonnewtonian_sheared(rheology, kw):
+    """Power law and Bingham away from their switching points: FP32 tolerances."""
+    nx, ny, nz = 22, 20, 18
+    rng = np.random.default_rng(4)
+    solid = np.zeros((nz, ny, nx), dtype=np.uint8)
+    solid[:, 2:-2, 2:-2] = rng.random((nz, ny - 4, nx - 4)) < 0.03
+    nt = mrlbm.voxel_node_types(solid, (1, 0, 1))
+    d = mrlbm.make_desc(nx, ny, nz, lattice=19, periodic=(1, 0, 1), tau=0.8, force=(3e-6, 0, 1e-6),
+                        rheology=rheology, **kw)
+    g, o, res = run_pair(d, 60, node_types=nt, init=sheared_start(nx, ny, nz), fluid=solid == 0)
+    assert_close(res, l2=1e-4, linf=2e-3, l2_2=1e-3, linf_2=1e-2)
+
+
 def test_duct_voxels_force_powerlaw():
     nx, ny, nz = 20, 18, 24
     rng = np.random.default_rng(9)

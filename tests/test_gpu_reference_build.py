@@ -1,10 +1,23 @@
 """The library against the reference's own CUDA program (built for sm_100 by
 oracle/build_ref_cuda.sh into oracle/_ref), on the same case and inputs.
 
-Lid-driven cavity 64^3, D3Q19, Re 100, lid 0.05, 2000 steps (the reference
-binary writes its final macroscopic fields as .bin files, src/saveData.cu):
-per-field relative L2 of the library's rho-1 and u against the reference's.
-Both sides are FP32; the differences come from operation order only.
+Lid-driven cavity 64^3, D3Q19, Re 100, lid 0.05, 2000 steps; the reference
+binary writes its final macroscopic fields as .bin files (src/saveData.cu).
+Both sides are FP32.
+
+Two typings of the lid:
+  * edges as walls (refsim_lid64_edges): the lid's edge and corner nodes carry
+    the edge/corner wall types, so every population a wall node treats as
+    known comes from inside the domain.  The solvers must then agree to FP32
+    operation-order differences: relative L2 of u below 1e-4.
+  * the reference case as shipped (refsim_lid64): every y = NY-1 node is
+    NORTH, so the lid's edge nodes treat some populations from outside the
+    domain as known.  The reference feeds those from its ghost-face arrays:
+    stale initial values for most, but for diagonal populations at its 8^3
+    block boundaries the current values of the periodically wrapped opposite
+    edge (the later y/z ghost load of popLoad.inc overrides the x one).  This
+    solver supplies the rest state for all of them, independent of any block
+    layout, so the flows differ by a fixed ~0.5 % (relative L2 of u).
 """
 import os
 import subprocess
@@ -17,7 +30,8 @@ import mrlbm
 
 pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REFSIM = os.path.join(ROOT, "oracle", "_ref", "refsim_lid64")
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+N = 64
 
 
 def read_bin(path, n):
@@ -26,35 +40,57 @@ def read_bin(path, n):
     return a.reshape(n, n, n)
 
 
-@pytest.fixture(scope="module")
-def reference_lid64(tmp_path_factory):
-    if not os.path.exists(REFSIM):
+def run_reference(binary, workdir):
+    exe = os.path.join(REF_DIR, binary)
+    if not os.path.exists(exe):
         pytest.skip("reference CUDA build missing (oracle/build_ref_cuda.sh needs the reference tree)")
-    work = tmp_path_factory.mktemp("refsim")
-    r = subprocess.run([REFSIM], cwd=work, capture_output=True, text=True, timeout=600)
+    os.makedirs(workdir, exist_ok=True)
+    r = subprocess.run([exe], cwd=workdir, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
-    base = os.path.join(work, "TEST", "000", "000_")
-    n = 64
-    out = {v: read_bin(base + v + "002000.bin", n) for v in ("rho", "ux", "uy", "uz")}
-    out["log"] = r.stdout
-    return out
+    base = os.path.join(workdir, "TEST", "000", "000_")
+    return {v: read_bin(base + v + "002000.bin", N) for v in ("rho", "ux", "uy", "uz")}
 
 
-def test_lid_cavity_64_matches_reference_build(reference_lid64, tmp_path):
-    n = 64
-    d = mrlbm.lid_cavity_desc(n, re=100.0, lid_u=0.05)
+def run_ours(node_types, workdir):
+    d = mrlbm.lid_cavity_desc(N, re=100.0, lid_u=0.05)
     dom = mrlbm.Domain(d)
-    dom.set_node_types(mrlbm.lid_cavity_node_types(n, n, n, 1))
+    dom.set_node_types(node_types)
     dom.init_uniform()
     dom.step(2000)
-    dom.save_macr_bin(str(tmp_path), "000", 2000)
-    ours = {v: read_bin(os.path.join(tmp_path, "000", "000_" + v + "002000.bin"), n) for v in ("rho", "ux", "uy", "uz")}
-    ref = reference_lid64
-    e_rho = lattice_np.rel_l2(ours["rho"] - 1.0, ref["rho"] - 1.0)
-    u_ours = np.stack([ours["ux"], ours["uy"], ours["uz"]])
-    u_ref = np.stack([ref["ux"], ref["uy"], ref["uz"]])
-    e_u = lattice_np.rel_l2(u_ours, u_ref)
-    e_uinf = lattice_np.rel_linf(u_ours, u_ref)
-    print("lid64 vs reference build: rel L2 rho-1 %.3e, u %.3e, u Linf %.3e" % (e_rho, e_u, e_uinf))
-    assert e_u < 1e-4 and e_uinf < 1e-3
-    assert e_rho < 1e-3
+    dom.save_macr_bin(str(workdir), "000", 2000)
+    return {v: read_bin(os.path.join(workdir, "000", "000_" + v + "002000.bin"), N) for v in ("rho", "ux", "uy", "uz")}
+
+
+def errors(ours, ref):
+    u_o = np.stack([ours["ux"], ours["uy"], ours["uz"]])
+    u_r = np.stack([ref["ux"], ref["uy"], ref["uz"]])
+    return (lattice_np.rel_l2(u_o, u_r), lattice_np.rel_linf(u_o, u_r),
+            float(np.max(np.abs(ours["rho"] - ref["rho"]))))
+
+
+def lid_edges_as_walls():
+    nt = mrlbm.lid_cavity_node_types(N, N, N, 1)
+    F = lattice_np.FACES
+    z, x = np.meshgrid(np.arange(N), np.arange(N), indexing="ij")
+    top = nt[:, N - 1, :]
+    edge = (x == 0) | (x == N - 1) | (z == 0) | (z == N - 1)
+    walls = F["NORTH"] | np.where(x == 0, F["WEST"], 0) | np.where(x == N - 1, F["EAST"], 0) | \
+        np.where(z == 0, F["BACK"], 0) | np.where(z == N - 1, F["FRONT"], 0)
+    top[edge] = walls[edge]
+    return nt
+
+
+def test_lid_cavity_64_edges_as_walls_matches_reference(tmp_path):
+    ref = run_reference("refsim_lid64_edges", tmp_path / "ref")
+    ours = run_ours(lid_edges_as_walls(), tmp_path / "ours")
+    e_u, e_uinf, e_rho = errors(ours, ref)
+    print("lid64 (edges as walls) vs reference build: u rel L2 %.3e, rel Linf %.3e, max |drho| %.3e" % (e_u, e_uinf, e_rho))
+    assert e_u < 1e-4 and e_uinf < 1e-3 and e_rho < 1e-5
+
+
+def test_lid_cavity_64_reference_typing(tmp_path):
+    ref = run_reference("refsim_lid64", tmp_path / "ref")
+    ours = run_ours(mrlbm.lid_cavity_node_types(N, N, N, 1), tmp_path / "ours")
+    e_u, e_uinf, e_rho = errors(ours, ref)
+    print("lid64 (reference typing) vs reference build: u rel L2 %.3e, rel Linf %.3e, max |drho| %.3e" % (e_u, e_uinf, e_rho))
+    assert e_u < 1e-2
