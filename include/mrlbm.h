@@ -112,6 +112,12 @@ mrlbm_status mrlbm_domain_bytes(const mrlbm_desc* desc, size_t* bytes);
  * hostInitialization_nodeType / bc_initialization.inc
  * (src/lbmInitialization.cu:958-975). */
 mrlbm_status mrlbm_set_node_types(mrlbm_domain* dom, const uint32_t* node_type);
+/* Case mode: node types whose boundary nodes are handled by a case's own
+ * compiled bc_definition.inc (mr-lbm_b200/casebuild.py); any word is accepted
+ * and handed to the snippet unchanged (the reference's kernel switch,
+ * src/mlbm.cu:457-461).  Only step kernels built by casebuild.py can step
+ * such a domain. */
+mrlbm_status mrlbm_set_node_types_case(mrlbm_domain* dom, const uint32_t* node_type);
 
 /* Initial state from physical rho, u fields (x-fastest, host).  Replaces
  * gpuInitialization_mom + flow_initialization.inc

@@ -57,7 +57,8 @@ mrlbm_status fail(mrlbm_status st, const char* fmt, ...);
 uint32_t known_mask(int q, uint32_t octants);
 mrlbm_status build_bc_class(int q, int mq, uint32_t word, const double uvel[4][3], double omega0, BcClass* out);
 mrlbm_status classify_nodes(int q, int mq, const uint32_t* nt, long long n, const double uvel[4][3], double omega0,
-                            std::vector<uint8_t>& cls, std::vector<BcClass>& table, bool& any_bc);
+                            std::vector<uint8_t>& cls, std::vector<BcClass>& table, bool& any_bc,
+                            bool case_mode = false);
 void storage_scales(int storage, float* scale, float* iscale);
 mrlbm_status domain_alloc(mrlbm_domain* dom);
 int choose_lz(const mrlbm_domain* dom);

@@ -70,6 +70,8 @@ struct BcClass {
     float u[3];        // prescribed wall velocity (unscaled)
     uint32_t known;    // bit i: population i is known (incoming from fluid)
     uint32_t valid;
+    uint32_t word;     // the node-type word of the class (nodeTypeMap encoding)
+    uint32_t pad;
 };
 
 struct StepArgs {
@@ -81,6 +83,7 @@ struct StepArgs {
     long long plane, field;  // elements
     int periodic;            // bit a set: axis a periodic
     int lz;                  // planes per CTA
+    int step;                // step number (read by case-mode boundary snippets)
     float rho0, omega0;
     float fx, fy, fz;
     float nnf_n, nnf_k, nnf_yield, nnf_omega_p;
@@ -242,6 +245,18 @@ __device__ __forceinline__ void bc_moments(const BcClass* __restrict__ c, const 
 #pragma unroll
     for (int k = 0; k < 6; k++) mac[4 + k] = X[1 + k] * ir;
 }
+
+// Boundary-node policy of the step kernels: the run-time class table solved by
+// bc_moments (the default), or a case's own bc_definition snippet compiled
+// into a policy of the same shape (case mode).
+struct TableBC {
+    template <int Q>
+    static __device__ __forceinline__ void apply(const StepArgs& a, uint8_t cls, const float* p, float omega,
+                                                 int x, int y, int z, float* mac)
+    {
+        bc_moments<Q>(a.bc + cls, p, omega, a.omega0, mac);
+    }
+};
 
 // Power-law omega by Newton iteration (src/nnf.h:61-89 with its compile
 // defects fixed) and Bingham (src/nnf.h:92-98).
@@ -484,7 +499,7 @@ __device__ __forceinline__ void store_node(const StepArgs& a, long long idx, con
 // c_z = +1 and 0 ones enter the z pipeline.  The arithmetic is branch-free
 // over the warp (so it interleaves with the next production); only the BC
 // solve and the stores are predicated.
-template <int Q, int NM, int NUP, int NMID, typename T, int FLAGS, int TYI>
+template <int Q, int NM, int NUP, int NMID, typename T, int FLAGS, int TYI, typename BCP>
 __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const float4* ex4, const float* ex1,
                                        int lane, int warp, bool interior, int x, int y, const float (&gsh)[Q],
                                        float (&up_old)[NUP], float (&mid)[NMID], float om_out)
@@ -544,7 +559,7 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
             mac[9] = P[5] * ir - (1.0f / 3.0f);
         }
         if constexpr ((FLAGS & F_BC) != 0) {
-            if (cls != CLS_BULK && cls != CLS_SOLID) bc_moments<Q>(a.bc + cls, p, omega, a.omega0, mac);
+            if (cls != CLS_BULK && cls != CLS_SOLID) BCP::template apply<Q>(a, cls, p, omega, x, y, zd, mac);
         }
         float o[11];
         collide<FLAGS>(a, mac, omega, o);
@@ -601,7 +616,7 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
 // Per-CTA pipeline state and the loop of the z-march over one column.  The
 // TMA ring is indexed by a running production count `g0 + k` so a persistent
 // CTA can chain columns without re-initialising its mbarriers.
-template <int Q, typename T, int FLAGS, int TYI>
+template <int Q, typename T, int FLAGS, int TYI, typename BCP>
 struct ZMarch {
     static constexpr int NW = TYI + 2;
     static constexpr int NUP = lat_num_cz(Q, 1);
@@ -654,7 +669,7 @@ struct ZMarch {
         const bool ok = mbar_wait(&bars[slot(j)], phase(j));
         const float om_out = om_par;
         prod_a<Q, NM, T, TYI>(a, stage_of(j), j, ex4, ex1, lane, warp, col, gsh_new, om_par);
-        prod_b<Q, NM, NUP, NMID, T, FLAGS, TYI>(a, j - 1, z0 - 2 + j, ex4, ex1, lane, warp, interior, x, y, gsh_old,
+        prod_b<Q, NM, NUP, NMID, T, FLAGS, TYI, BCP>(a, j - 1, z0 - 2 + j, ex4, ex1, lane, warp, interior, x, y, gsh_old,
                                                 up, mid, om_out);
         if (__syncthreads_or(!ok)) return false;
         refill(j);
@@ -665,7 +680,7 @@ struct ZMarch {
 template <int Q, typename T, int FLAGS, int TYI>
 constexpr size_t zmarch_stage_al()
 {
-    return ZMarch<Q, T, FLAGS, TYI>::stage_al;
+    return ZMarch<Q, T, FLAGS, TYI, TableBC>::stage_al;
 }
 
 // Shared-memory carve-up used by every z-march kernel: barriers, TMA ring,
@@ -692,11 +707,11 @@ struct ZSmem {
 // One column (X0, Y0) x planes [z0, z0 + lz) of one domain.  g0 is the
 // CTA's running production count (advanced by the column's productions).
 // Returns false when a bounded wait timed out (the CTA must stop).
-template <int Q, typename T, int FLAGS, int TYI>
+template <int Q, typename T, int FLAGS, int TYI, typename BCP = TableBC>
 __device__ __forceinline__ bool zmarch_column(const StepArgs& a, const CUtensorMap* map, int X0, int Y0, int z0,
                                               const ZSmem<Q, T, TYI>& sm, unsigned& g0)
 {
-    using ZM = ZMarch<Q, T, FLAGS, TYI>;
+    using ZM = ZMarch<Q, T, FLAGS, TYI, BCP>;
     constexpr int NUP = ZM::NUP, NMID = ZM::NMID;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int x = X0 - 1 + lane, y = Y0 - 1 + warp;
@@ -733,14 +748,14 @@ __device__ __forceinline__ bool zmarch_column(const StepArgs& a, const CUtensorM
         // epilogues consume the last production j-1; its output plane is that
         // of production j-2, whose omega has the parity of j
         if (j >= zm.nprod) {  // j odd: last production even
-            prod_b<Q, ZM::NM, NUP, NMID, T, FLAGS, TYI>(a, j - 1, z0 - 2 + j, sm.ex4, sm.ex1, lane, warp, zm.interior, x,
+            prod_b<Q, ZM::NM, NUP, NMID, T, FLAGS, TYI, BCP>(a, j - 1, z0 - 2 + j, sm.ex4, sm.ex1, lane, warp, zm.interior, x,
                                                         y, gA, upA, mid, omB);
             break;
         }
         if (!zm.iter(j, gB, gA, upA, mid, omB)) { kfail = j; break; }
         j++;
         if (j >= zm.nprod) {  // j even: last production odd
-            prod_b<Q, ZM::NM, NUP, NMID, T, FLAGS, TYI>(a, j - 1, z0 - 2 + j, sm.ex4, sm.ex1, lane, warp, zm.interior, x,
+            prod_b<Q, ZM::NM, NUP, NMID, T, FLAGS, TYI, BCP>(a, j - 1, z0 - 2 + j, sm.ex4, sm.ex1, lane, warp, zm.interior, x,
                                                         y, gB, upB, mid, omA);
             break;
         }
@@ -774,7 +789,7 @@ __device__ __forceinline__ void zmarch_init_barriers(const ZSmem<Q, T, TYI>& sm)
 }
 
 // Single-domain step: one CTA per (x tile, y tile, z chunk).
-template <int Q, typename T, int FLAGS, int TYI>
+template <int Q, typename T, int FLAGS, int TYI, typename BCP = TableBC>
 __global__ void __launch_bounds__(32 * (TYI + 2), 1)
     zmarch_step(const __grid_constant__ CUtensorMap map_in, const StepArgs a)
 {
@@ -782,7 +797,7 @@ __global__ void __launch_bounds__(32 * (TYI + 2), 1)
     const ZSmem<Q, T, TYI> sm(smem);
     zmarch_init_barriers<Q, T, TYI>(sm);
     unsigned g0 = 0;
-    (void)zmarch_column<Q, T, FLAGS, TYI>(a, &map_in, blockIdx.x * TILE_X, blockIdx.y * TYI, blockIdx.z * a.lz, sm,
+    (void)zmarch_column<Q, T, FLAGS, TYI, BCP>(a, &map_in, blockIdx.x * TILE_X, blockIdx.y * TYI, blockIdx.z * a.lz, sm,
                                           g0);
 }
 

@@ -180,6 +180,7 @@ mrlbm_status mrlbm::build_bc_class(int q, int mq, uint32_t word, const double uv
     for (int a = 0; a < 3; a++) out->u[a] = (float)u[a];
     out->known = known;
     out->valid = 1;
+    out->word = word;
     return MRLBM_OK;
 }
 
@@ -341,7 +342,7 @@ extern "C" mrlbm_status mrlbm_domain_destroy(mrlbm_domain* dom)
 
 mrlbm_status mrlbm::classify_nodes(int q, int mq, const uint32_t* nt, long long n, const double uvel[4][3],
                                    double omega0, std::vector<uint8_t>& cls, std::vector<BcClass>& table,
-                                   bool& any_bc)
+                                   bool& any_bc, bool case_mode)
 {
     std::map<uint32_t, int> ids;
     table.assign(1, BcClass{});  // class 0: bulk (unused entry)
@@ -349,16 +350,22 @@ mrlbm_status mrlbm::classify_nodes(int q, int mq, const uint32_t* nt, long long 
     any_bc = false;
     for (long long k = 0; k < n; k++) {
         const uint32_t w = nt[k];
-        const uint32_t oct = w & 0xFFu;
-        if (oct == 0) { cls[k] = CLS_BULK; continue; }
+        // run-time classes key on the octant mask, BC kind and velocity index;
+        // case mode hands the whole word to the case's own snippet (like the
+        // reference: bulk iff the word is BULK, solid iff it is 0xFF)
+        const bool bulk = case_mode ? w == 0u : (w & 0xFFu) == 0u;
+        const bool solid = case_mode ? w == 0xFFu : (w & 0xFFu) == 0xFFu;
+        if (bulk) { cls[k] = CLS_BULK; continue; }
         any_bc = true;
-        if (oct == 0xFFu) { cls[k] = CLS_SOLID; continue; }
-        const uint32_t key = w & 0x1FFFu;
+        if (solid) { cls[k] = CLS_SOLID; continue; }
+        const uint32_t key = case_mode ? w : (w & 0x1FFFu);
         auto it = ids.find(key);
         if (it == ids.end()) {
             if ((int)table.size() >= 255) return fail(MRLBM_EINVAL, "more than 254 distinct boundary node types");
             BcClass c;
-            mrlbm_status st = build_bc_class(q, mq, key, uvel, omega0, &c);
+            memset(&c, 0, sizeof(c));
+            c.word = key;
+            mrlbm_status st = case_mode ? MRLBM_OK : build_bc_class(q, mq, key, uvel, omega0, &c);
             if (st) return st;
             const int id = (int)table.size();
             table.push_back(c);
@@ -369,7 +376,7 @@ mrlbm_status mrlbm::classify_nodes(int q, int mq, const uint32_t* nt, long long 
     return MRLBM_OK;
 }
 
-extern "C" mrlbm_status mrlbm_set_node_types(mrlbm_domain* dom, const uint32_t* nt)
+static mrlbm_status set_node_types_impl(mrlbm_domain* dom, const uint32_t* nt, bool case_mode)
 {
     if (!dom || !nt) return fail(MRLBM_EINVAL, "null argument");
     const mrlbm_desc& d = dom->d;
@@ -377,7 +384,8 @@ extern "C" mrlbm_status mrlbm_set_node_types(mrlbm_domain* dom, const uint32_t* 
     std::vector<uint8_t> cls;
     std::vector<BcClass> table;
     bool any = false;
-    mrlbm_status st = classify_nodes(dom->q, d.bc_matrix_q, nt, n, d.bc_velocity, dom->omega0, cls, table, any);
+    mrlbm_status st =
+        classify_nodes(dom->q, d.bc_matrix_q, nt, n, d.bc_velocity, dom->omega0, cls, table, any, case_mode);
     if (st) return st;
     // scatter into the padded plane layout
     std::vector<uint8_t> padded((size_t)dom->field, 0);
@@ -394,6 +402,16 @@ extern "C" mrlbm_status mrlbm_set_node_types(mrlbm_domain* dom, const uint32_t* 
     dom->nclasses = (int)table.size();
     if (dom->graph_exec) { cudaGraphExecDestroy(dom->graph_exec); dom->graph_exec = nullptr; }
     return MRLBM_OK;
+}
+
+extern "C" mrlbm_status mrlbm_set_node_types(mrlbm_domain* dom, const uint32_t* nt)
+{
+    return set_node_types_impl(dom, nt, false);
+}
+
+extern "C" mrlbm_status mrlbm_set_node_types_case(mrlbm_domain* dom, const uint32_t* nt)
+{
+    return set_node_types_impl(dom, nt, true);
 }
 
 // ------------------------------------------------------------------- init
@@ -489,6 +507,7 @@ void mrlbm::fill_step_args(const mrlbm_domain* dom, StepArgs& a, int parity, int
     a.plane = dom->plane; a.field = dom->field;
     a.periodic = (d.periodic[0] ? 1 : 0) | (d.periodic[1] ? 2 : 0) | (d.periodic[2] ? 4 : 0);
     a.lz = dom->lz;
+    a.step = dom->step;
     a.rho0 = (float)d.rho0;
     a.omega0 = (float)dom->omega0;
     a.fx = (float)d.force[0]; a.fy = (float)d.force[1]; a.fz = (float)d.force[2];

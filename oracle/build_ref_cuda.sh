@@ -15,6 +15,10 @@
 #   _ref/refsim_lid64        lidDrivenCavity_3D, D3Q19, 64^3, Re 100, lid 0.05, N_STEPS from argv-free constant
 #   _ref/refsim_tgv256_q27   taylorGreen, D3Q27, 256^3, Re 1600, u0 0.04, 1000 steps
 #   _ref/refsim_bench256     benchmark (README table case), D3Q19, 256^3, 1000 steps
+#   _ref/refsim_lid64_edges  C1 with the lid's edges typed as edge walls
+#   _ref/refsim_lid16_trace  16^3 lid cavity writing its fields after every step
+#   _ref/cases/*             the same cases compiled in this library's case mode
+# CASES_ONLY=1 rebuilds only the case-mode programs.
 set -euo pipefail
 REF=${REF:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
@@ -45,6 +49,7 @@ build_case() {
     echo "built $OUT/$name"
 }
 
+if [ -z "${CASES_ONLY:-}" ]; then
 # C1: lid-driven cavity 64^3, Re 100, lid velocity 0.05 (tau from Re, constants.inc:35-36)
 build_case refsim_lid64 lidDrivenCavity_3D D3Q19 2000 64 \
   'sed -i "s/^constexpr dfloat RE = .*/constexpr dfloat RE = 100;/; s/^constexpr dfloat U_MAX = .*/constexpr dfloat U_MAX = 0.05;/" "$c/constants.inc"; sed -i "s/^#define REPORT_SAVE .*/#define REPORT_SAVE (false)/" "$c/output.inc"'
@@ -71,3 +76,20 @@ build_case refsim_tgv256_q27 taylorGreen D3Q27 1000 256 \
 
 # README benchmark case, D3Q19 256^3 (the published MLUPS table), 1000 steps
 build_case refsim_bench256 benchmark D3Q19 1000 256 'true'
+fi
+
+# ---------------------------------------------------------------------------
+# The same reference cases compiled, unchanged, in this library's case mode
+# (mr-lbm_b200/casebuild.py reads the case folder and pastes its snippets into
+# the sm_100a step kernel).  Test fixtures for the drop-in path: they run on the
+# GPU box next to the reference programs above, on identical inputs.
+PY=${PY:-python}
+CB="$HERE/../mr-lbm_b200/casebuild.py"
+mkdir -p "$OUT/cases"
+common_out='--set BIN_SAVE=(true) --set VTK_SAVE=(false) --set ONLY_FINAL_MACRO=(true) --set MACR_SAVE=(false)'
+$PY "$CB" "$REF/src/cases/lidDrivenCavity_3D" -o "$OUT/cases/lid64" --set N=64 --set RE=100 --set U_MAX=0.05 \
+    --set N_STEPS=2000 --set "REPORT_SAVE=(false)" $common_out
+$PY "$CB" "$REF/src/cases/taylorGreen" -o "$OUT/cases/tgv256_q27" --lattice 27 --set N=256 --set RE=1600 \
+    --set U_MAX=0.04 --set N_STEPS=1000 --set "REPORT_SAVE=(100)" --set "SAVEDATA=(true)" $common_out
+$PY "$CB" "$REF/src/cases/benchmark" -o "$OUT/cases/bench256" --set N_STEPS=1000 $common_out
+echo "built case-mode programs in $OUT/cases"

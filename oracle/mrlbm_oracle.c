@@ -40,19 +40,30 @@
 
 #define ORC_MAXQ 27
 
+/* Arithmetic type of the step.  FP64 by default (liboracle.so, the oracle);
+ * `-DORC_REAL=float -fsingle-precision-constant` builds liboracle_f32.so, the
+ * same restatement in FP32 arithmetic and FP32 storage.  The FP32 build is the
+ * yardstick for how far any FP32 implementation of this algorithm drifts from
+ * FP64 on a given case (driven flows accumulate round-off); the exported
+ * interface takes and returns double in both builds. */
+#ifndef ORC_REAL
+#define ORC_REAL double
+#endif
+typedef ORC_REAL real;
+
 /* D3Q27 ordering; the first 19 entries are D3Q19 (same order as the reference). */
 static const int CX[27] = {0, 1,-1, 0, 0, 0, 0, 1,-1, 1,-1, 0, 0, 1,-1, 1,-1, 0, 0, 1,-1, 1,-1, 1,-1,-1, 1};
 static const int CY[27] = {0, 0, 0, 1,-1, 0, 0, 1,-1, 0, 0, 1,-1,-1, 1, 0, 0, 1,-1, 1,-1, 1,-1,-1, 1, 1,-1};
 static const int CZ[27] = {0, 0, 0, 0, 0, 1,-1, 0, 0, 1,-1, 1,-1, 0, 0,-1, 1,-1, 1, 1,-1,-1, 1, 1,-1, 1,-1};
 
-static double weight(int q, int i)
+static real weight(int q, int i)
 {
     int n = CX[i] * CX[i] + CY[i] * CY[i] + CZ[i] * CZ[i];
     if (q == 19) {
-        static const double w19[3] = {1.0 / 3.0, 1.0 / 18.0, 1.0 / 36.0};
+        static const real w19[3] = {1.0 / 3.0, 1.0 / 18.0, 1.0 / 36.0};
         return w19[n];
     }
-    static const double w27[4] = {8.0 / 27.0, 2.0 / 27.0, 1.0 / 54.0, 1.0 / 216.0};
+    static const real w27[4] = {8.0 / 27.0, 2.0 / 27.0, 1.0 / 54.0, 1.0 / 216.0};
     return w27[n];
 }
 
@@ -74,41 +85,41 @@ typedef struct {
     orc_desc d;
     int nm;                /* 10, or 11 with an omega field */
     size_t n;
-    double *m, *m2;        /* [node][nm], node = x + nx*(y + ny*z) */
+    real *m, *m2;        /* [node][nm], node = x + nx*(y + ny*z) */
     uint32_t *type;        /* reference nodeTypeMap words, same node order */
-    double *pop;           /* [node][q] post-collision populations scratch */
+    real *pop;           /* [node][q] post-collision populations scratch */
 } orc_domain;
 
 /* ----------------------------------------------------------------- per node */
 
 /* f_i = rho w_i [1 - cs2 tr(m2) + c.u3 + sum c_a^2 m_aa + sum c_a c_b m_ab]
  * with m in the stored scaled form (reconstruction.inc:1-35). */
-void orc_reconstruct(int q, double rho0, const double *m, double *f)
+void orc_reconstruct(int q, real rho0, const real *m, real *f)
 {
-    double rho = rho0 + m[0];
-    double ux = m[1], uy = m[2], uz = m[3];
-    double mxx = m[4], mxy = m[5], mxz = m[6], myy = m[7], myz = m[8], mzz = m[9];
-    double pics2 = 1.0 - (mxx + myy + mzz) / 3.0;
+    real rho = rho0 + m[0];
+    real ux = m[1], uy = m[2], uz = m[3];
+    real mxx = m[4], mxy = m[5], mxz = m[6], myy = m[7], myz = m[8], mzz = m[9];
+    real pics2 = 1.0 - (mxx + myy + mzz) / 3.0;
     for (int i = 0; i < q; i++) {
-        double cx = CX[i], cy = CY[i], cz = CZ[i];
-        double t = pics2 + cx * ux + cy * uy + cz * uz + cx * cx * mxx + cy * cy * myy + cz * cz * mzz
+        real cx = CX[i], cy = CY[i], cz = CZ[i];
+        real t = pics2 + cx * ux + cy * uy + cz * uz + cx * cx * mxx + cy * cy * myy + cz * cz * mzz
                  + cx * cy * mxy + cx * cz * mxz + cy * cz * myz;
         f[i] = rho * weight(q, i) * t;
     }
 }
 
 /* Bulk macroscopics, unscaled: rho, u, Pi_hat = sum f cc / rho - cs2 delta (mlbm.cu:462-497). */
-void orc_bulk_moments(int q, const double *f, double *out /* rho,ux,uy,uz,pxx,pxy,pxz,pyy,pyz,pzz */)
+void orc_bulk_moments(int q, const real *f, real *out /* rho,ux,uy,uz,pxx,pxy,pxz,pyy,pyz,pzz */)
 {
-    double r = 0, jx = 0, jy = 0, jz = 0, pxx = 0, pxy = 0, pxz = 0, pyy = 0, pyz = 0, pzz = 0;
+    real r = 0, jx = 0, jy = 0, jz = 0, pxx = 0, pxy = 0, pxz = 0, pyy = 0, pyz = 0, pzz = 0;
     for (int i = 0; i < q; i++) {
-        double cx = CX[i], cy = CY[i], cz = CZ[i], v = f[i];
+        real cx = CX[i], cy = CY[i], cz = CZ[i], v = f[i];
         r += v;
         jx += v * cx; jy += v * cy; jz += v * cz;
         pxx += v * cx * cx; pxy += v * cx * cy; pxz += v * cx * cz;
         pyy += v * cy * cy; pyz += v * cy * cz; pzz += v * cz * cz;
     }
-    double ir = 1.0 / r;
+    real ir = 1.0 / r;
     out[0] = r;
     out[1] = jx * ir; out[2] = jy * ir; out[3] = jz * ir;
     out[4] = pxx * ir - 1.0 / 3.0; out[5] = pxy * ir; out[6] = pxz * ir;
@@ -137,22 +148,22 @@ uint32_t orc_known_mask(int q, uint32_t octants)
     return known;
 }
 
-static void h_vec(int i, double *h)
+static void h_vec(int i, real *h)
 {
-    double cx = CX[i], cy = CY[i], cz = CZ[i];
+    real cx = CX[i], cy = CY[i], cz = CZ[i];
     h[0] = cx * cx - 1.0 / 3.0; h[1] = cx * cy; h[2] = cx * cz;
     h[3] = cy * cy - 1.0 / 3.0; h[4] = cy * cz; h[5] = cz * cz - 1.0 / 3.0;
 }
 
 /* coefficient of Pi_k inside 4.5 * H_i : Pi  (off-diagonals counted twice) */
-static void g_vec(int i, double *g)
+static void g_vec(int i, real *g)
 {
-    double cx = CX[i], cy = CY[i], cz = CZ[i];
+    real cx = CX[i], cy = CY[i], cz = CZ[i];
     g[0] = 4.5 * (cx * cx - 1.0 / 3.0); g[1] = 9.0 * cx * cy; g[2] = 9.0 * cx * cz;
     g[3] = 4.5 * (cy * cy - 1.0 / 3.0); g[4] = 9.0 * cy * cz; g[5] = 4.5 * (cz * cz - 1.0 / 3.0);
 }
 
-static int solve7(double A[7][7], double *b, double *x)
+static int solve7(real A[7][7], real *b, real *x)
 {
     int p[7];
     for (int i = 0; i < 7; i++) p[i] = i;
@@ -161,17 +172,17 @@ static int solve7(double A[7][7], double *b, double *x)
         for (int r = c + 1; r < 7; r++)
             if (fabs(A[p[r]][c]) > fabs(A[p[best]][c])) best = r;
         int t = p[c]; p[c] = p[best]; p[best] = t;
-        double piv = A[p[c]][c];
-        if (fabs(piv) < 1e-300) return -1;
+        real piv = A[p[c]][c];
+        if (piv == 0) return -1;
         for (int r = c + 1; r < 7; r++) {
-            double f = A[p[r]][c] / piv;
+            real f = A[p[r]][c] / piv;
             if (f == 0.0) continue;
             for (int k = c; k < 7; k++) A[p[r]][k] -= f * A[p[c]][k];
             b[p[r]] -= f * b[p[c]];
         }
     }
     for (int c = 6; c >= 0; c--) {
-        double s = b[p[c]];
+        real s = b[p[c]];
         for (int k = c + 1; k < 7; k++) s -= A[p[c]][k] * x[k];
         x[c] = s / A[p[c]][c];
     }
@@ -186,26 +197,26 @@ static int solve7(double A[7][7], double *b, double *x)
  * D3Q27 lattice reproduces the reference's D3Q27 wall formulas, which are the
  * D3Q19 closed forms fed with D3Q27 known-set moments,
  * src/cases/parallelPlates_D3Q27/bc_definition.inc:18-44). */
-int orc_bc_solve(int q, int mq, uint32_t known, const double *u, double omega, const double *f, double *out)
+int orc_bc_solve(int q, int mq, uint32_t known, const real *u, real omega, const real *f, real *out)
 {
-    double A[7][7], b[7], x[7];
+    real A[7][7], b[7], x[7];
     memset(A, 0, sizeof(A));
     memset(b, 0, sizeof(b));
-    double uu[6] = {u[0] * u[0], u[0] * u[1], u[0] * u[2], u[1] * u[1], u[1] * u[2], u[2] * u[2]};
+    real uu[6] = {u[0] * u[0], u[0] * u[1], u[0] * u[2], u[1] * u[1], u[1] * u[2], u[2] * u[2]};
     for (int i = 0; i < q; i++) {
         if (!((known >> i) & 1u)) continue;
-        double h[6], g[6];
+        real h[6], g[6];
         h_vec(i, h);
         b[0] += f[i];
         for (int r = 0; r < 6; r++) b[1 + r] += f[i] * h[r];
     }
     for (int i = 0; i < mq; i++) {
         if (!((known >> i) & 1u)) continue;
-        double w = weight(mq, i), h[6], g[6];
+        real w = weight(mq, i), h[6], g[6];
         h_vec(i, h);
         g_vec(i, g);
-        double cu = 3.0 * (CX[i] * u[0] + CY[i] * u[1] + CZ[i] * u[2]);
-        double guu = 0.0;
+        real cu = 3.0 * (CX[i] * u[0] + CY[i] * u[1] + CZ[i] * u[2]);
+        real guu = 0.0;
         for (int k = 0; k < 6; k++) guu += g[k] * uu[k];
         /* row 0: sum_I f^reg(rho, u, (1-w)Pi + w uu) */
         A[0][0] += w * (1.0 + cu + omega * guu);
@@ -224,54 +235,54 @@ int orc_bc_solve(int q, int mq, uint32_t known, const double *u, double omega, c
 }
 
 /* Power-law omega by Newton iteration (nnf.h:61-89), defects fixed. */
-double orc_nnf_powerlaw(double omega_old, double smag, double n_index, double k_cons, double rho0)
+real orc_nnf_powerlaw(real omega_old, real smag, real n_index, real k_cons, real rho0)
 {
-    double omega = omega_old;
-    double a = k_cons * pow(smag / (rho0 / 3.0), n_index);
-    double b = 0.5 * smag, c = -smag;
+    real omega = omega_old;
+    real a = k_cons * pow(smag / (rho0 / 3.0), n_index);
+    real b = 0.5 * smag, c = -smag;
     if (smag < 1e-6) return 0.0;
     for (int it = 0; it < 7; it++) {
-        double fx = a * pow(omega, n_index) + b * omega + c;
-        double dfx = a * n_index * pow(omega, n_index - 1.0) + b;
+        real fx = a * pow(omega, n_index) + b * omega + c;
+        real dfx = a * n_index * pow(omega, n_index - 1.0) + b;
         if (fabs(fx / dfx) < 1e-6) break;
         omega = omega - fx / dfx;
     }
     return omega;
 }
 
-double orc_nnf_bingham(double smag, double omega_p, double yield_stress)
+real orc_nnf_bingham(real smag, real omega_p, real yield_stress)
 {
-    double v = 1.0 - yield_stress / smag;
+    real v = 1.0 - yield_stress / smag;
     return omega_p * (v > 0.0 ? v : 0.0);
 }
 
 /* Scale, (shear, nnf), collide.  mac = rho,u,Pi unscaled in/out; m = stored
  * scaled moments out (nm entries).  Follows mlbm.cu:500-591 + collision.inc. */
-static void collide_store(const orc_desc *d, int nm, const double *mac, double omega_in, double *m)
+static void collide_store(const orc_desc *d, int nm, const real *mac, real omega_in, real *m)
 {
-    double rho = mac[0];
-    double ux = 3.0 * mac[1], uy = 3.0 * mac[2], uz = 3.0 * mac[3];
-    double mxx = 4.5 * mac[4], mxy = 9.0 * mac[5], mxz = 9.0 * mac[6];
-    double myy = 4.5 * mac[7], myz = 9.0 * mac[8], mzz = 4.5 * mac[9];
-    double Fx = d->force[0], Fy = d->force[1], Fz = d->force[2];
-    double omega = omega_in;
+    real rho = mac[0];
+    real ux = 3.0 * mac[1], uy = 3.0 * mac[2], uz = 3.0 * mac[3];
+    real mxx = 4.5 * mac[4], mxy = 9.0 * mac[5], mxz = 9.0 * mac[6];
+    real myy = 4.5 * mac[7], myz = 9.0 * mac[8], mzz = 4.5 * mac[9];
+    real Fx = d->force[0], Fy = d->force[1], Fz = d->force[2];
+    real omega = omega_in;
     if (d->rheology != ORC_NEWTONIAN) {
-        double sxx = rho * (mxx / 4.5 - ux * ux / 9.0), syy = rho * (myy / 4.5 - uy * uy / 9.0);
-        double szz = rho * (mzz / 4.5 - uz * uz / 9.0), sxy = rho * (mxy / 9.0 - ux * uy / 9.0);
-        double sxz = rho * (mxz / 9.0 - ux * uz / 9.0), syz = rho * (myz / 9.0 - uy * uz / 9.0);
-        double fxx = ux * Fx / 3.0, fyy = uy * Fy / 3.0, fzz = uz * Fz / 3.0;
-        double fxy = (ux * Fy + uy * Fx) / 6.0, fxz = (ux * Fz + uz * Fx) / 6.0, fyz = (uy * Fz + uz * Fy) / 6.0;
-        double smag = sqrt(0.5 * ((sxx + fxx) * (sxx + fxx) + (syy + fyy) * (syy + fyy) + (szz + fzz) * (szz + fzz)
+        real sxx = rho * (mxx / 4.5 - ux * ux / 9.0), syy = rho * (myy / 4.5 - uy * uy / 9.0);
+        real szz = rho * (mzz / 4.5 - uz * uz / 9.0), sxy = rho * (mxy / 9.0 - ux * uy / 9.0);
+        real sxz = rho * (mxz / 9.0 - ux * uz / 9.0), syz = rho * (myz / 9.0 - uy * uz / 9.0);
+        real fxx = ux * Fx / 3.0, fyy = uy * Fy / 3.0, fzz = uz * Fz / 3.0;
+        real fxy = (ux * Fy + uy * Fx) / 6.0, fxz = (ux * Fz + uz * Fx) / 6.0, fyz = (uy * Fz + uz * Fy) / 6.0;
+        real smag = sqrt(0.5 * ((sxx + fxx) * (sxx + fxx) + (syy + fyy) * (syy + fyy) + (szz + fzz) * (szz + fzz)
                                   + 2.0 * ((sxy + fxy) * (sxy + fxy) + (sxz + fxz) * (sxz + fxz) + (syz + fyz) * (syz + fyz))));
         if (d->rheology == ORC_POWERLAW)
             omega = orc_nnf_powerlaw(omega_in, smag, d->n_index, d->k_consistency, d->rho0);
         else
             omega = orc_nnf_bingham(smag, d->omega_p, d->yield_stress);
     }
-    double ir = 1.0 / rho;
-    double t_om = 1.0 - omega, tt_om = 1.0 - 0.5 * omega, om_d2 = 0.5 * omega, tt_om_t3 = 3.0 * tt_om;
+    real ir = 1.0 / rho;
+    real t_om = 1.0 - omega, tt_om = 1.0 - 0.5 * omega, om_d2 = 0.5 * omega, tt_om_t3 = 3.0 * tt_om;
     ux += 3.0 * ir * Fx; uy += 3.0 * ir * Fy; uz += 3.0 * ir * Fz;
-    double ir15 = 1.5 * ir;
+    real ir15 = 1.5 * ir;
     mxx = t_om * mxx + om_d2 * ux * ux + ir15 * tt_om * (2.0 * Fx * ux);
     myy = t_om * myy + om_d2 * uy * uy + ir15 * tt_om * (2.0 * Fy * uy);
     mzz = t_om * mzz + om_d2 * uz * uz + ir15 * tt_om * (2.0 * Fz * uz);
@@ -285,7 +296,7 @@ static void collide_store(const orc_desc *d, int nm, const double *mac, double o
 }
 
 /* exposed for KATs: unscaled macroscopics + omega -> stored post-collision moments */
-void orc_collide(const orc_desc *d, const double *mac, double omega, double *m_out, int nm)
+void orc_collide(const orc_desc *d, const real *mac, real omega, real *m_out, int nm)
 {
     collide_store(d, nm, mac, omega, m_out);
 }
@@ -299,10 +310,10 @@ void *orc_create(const orc_desc *d)
     o->d = *d;
     o->nm = (d->rheology != ORC_NEWTONIAN) ? 11 : 10;
     o->n = (size_t)d->nx * d->ny * d->nz;
-    o->m = (double *)calloc(o->n * o->nm, sizeof(double));
-    o->m2 = (double *)calloc(o->n * o->nm, sizeof(double));
+    o->m = (real *)calloc(o->n * o->nm, sizeof(real));
+    o->m2 = (real *)calloc(o->n * o->nm, sizeof(real));
     o->type = (uint32_t *)calloc(o->n, sizeof(uint32_t));
-    o->pop = (double *)malloc(o->n * d->q * sizeof(double));
+    o->pop = (real *)malloc(o->n * d->q * sizeof(real));
     if (!o->m || !o->m2 || !o->type || !o->pop) {
         free(o->m); free(o->m2); free(o->type); free(o->pop); free(o);
         return NULL;
@@ -328,14 +339,13 @@ void orc_set_node_types(void *h, const uint32_t *t)
 void orc_set_moments(void *h, const double *m)
 {
     orc_domain *o = (orc_domain *)h;
-    memcpy(o->m, m, o->n * o->nm * sizeof(double));
-    memcpy(o->m2, m, o->n * o->nm * sizeof(double));
+    for (size_t k = 0; k < o->n * o->nm; k++) o->m[k] = o->m2[k] = (real)m[k];
 }
 
 void orc_get_moments(void *h, double *m)
 {
     orc_domain *o = (orc_domain *)h;
-    memcpy(m, o->m, o->n * o->nm * sizeof(double));
+    for (size_t k = 0; k < o->n * o->nm; k++) m[k] = o->m[k];
 }
 
 /* Initial moments from physical rho,u (x-fastest) exactly as
@@ -347,22 +357,22 @@ void orc_init_from_macro(void *h, const double *rho, const double *ux, const dou
 {
     orc_domain *o = (orc_domain *)h;
     int q = o->d.q, qs = d3q19_sums ? 19 : q;
-    double omega = 1.0 / o->d.tau;
+    real omega = 1.0 / o->d.tau;
     for (size_t k = 0; k < o->n; k++) {
-        double f[ORC_MAXQ];
-        double u[3] = {ux[k], uy[k], uz[k]};
-        double uu = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+        real f[ORC_MAXQ];
+        real u[3] = {ux[k], uy[k], uz[k]};
+        real uu = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
         for (int i = 0; i < q; i++) {
-            double uc3 = 3.0 * (u[0] * CX[i] + u[1] * CY[i] + u[2] * CZ[i]);
+            real uc3 = 3.0 * (u[0] * CX[i] + u[1] * CY[i] + u[2] * CZ[i]);
             f[i] = weight(q, i) * o->d.rho0 * ((1.0 - 1.5 * uu) + uc3 * (1.0 + 0.5 * uc3));
         }
-        double ir = 1.0 / rho[k], p[6] = {0, 0, 0, 0, 0, 0};
+        real ir = 1.0 / rho[k], p[6] = {0, 0, 0, 0, 0, 0};
         for (int i = 0; i < qs; i++) {
-            double cx = CX[i], cy = CY[i], cz = CZ[i];
+            real cx = CX[i], cy = CY[i], cz = CZ[i];
             p[0] += f[i] * cx * cx; p[1] += f[i] * cx * cy; p[2] += f[i] * cx * cz;
             p[3] += f[i] * cy * cy; p[4] += f[i] * cy * cz; p[5] += f[i] * cz * cz;
         }
-        double *m = o->m + k * o->nm;
+        real *m = o->m + k * o->nm;
         m[0] = rho[k] - o->d.rho0;
         m[1] = 3.0 * u[0]; m[2] = 3.0 * u[1]; m[3] = 3.0 * u[2];
         m[4] = 4.5 * (p[0] * ir - 1.0 / 3.0);
@@ -373,7 +383,7 @@ void orc_init_from_macro(void *h, const double *rho, const double *ux, const dou
         m[9] = 4.5 * (p[5] * ir - 1.0 / 3.0);
         if (o->nm > 10) m[10] = omega;
     }
-    memcpy(o->m2, o->m, o->n * o->nm * sizeof(double));
+    memcpy(o->m2, o->m, o->n * o->nm * sizeof(real));
 }
 
 static inline int resolve(int v, int n, int periodic, int *outside)
@@ -389,9 +399,11 @@ void orc_step(void *h, int nsteps)
     orc_domain *o = (orc_domain *)h;
     const orc_desc *d = &o->d;
     const int q = d->q, nm = o->nm, nx = d->nx, ny = d->ny, nz = d->nz;
-    const double omega0 = 1.0 / d->tau;
-    double fext[ORC_MAXQ];
-    orc_reconstruct(q, d->rho0, d->exterior, fext);
+    const real omega0 = 1.0 / d->tau;
+    real fext[ORC_MAXQ];
+    real ext[10];
+    for (int k = 0; k < 10; k++) ext[k] = (real)d->exterior[k];
+    orc_reconstruct(q, d->rho0, ext, fext);
     for (int s = 0; s < nsteps; s++) {
         /* post-collision populations of every node, from its stored moments */
 #pragma omp parallel for schedule(static)
@@ -402,10 +414,10 @@ void orc_step(void *h, int nsteps)
                 for (int x = 0; x < nx; x++) {
                     size_t k = (size_t)x + (size_t)nx * (y + (size_t)ny * z);
                     uint32_t t = o->type[k];
-                    double *mo = o->m2 + k * nm;
-                    const double *mi = o->m + k * nm;
-                    if ((t & 0xFFu) == 0xFFu) { memcpy(mo, mi, nm * sizeof(double)); continue; }
-                    double f[ORC_MAXQ];
+                    real *mo = o->m2 + k * nm;
+                    const real *mi = o->m + k * nm;
+                    if ((t & 0xFFu) == 0xFFu) { memcpy(mo, mi, nm * sizeof(real)); continue; }
+                    real f[ORC_MAXQ];
                     for (int i = 0; i < q; i++) {
                         int out = 0;
                         int sx = resolve(x - CX[i], nx, d->periodic[0], &out);
@@ -413,20 +425,20 @@ void orc_step(void *h, int nsteps)
                         int sz = resolve(z - CZ[i], nz, d->periodic[2], &out);
                         f[i] = out ? fext[i] : o->pop[((size_t)sx + (size_t)nx * (sy + (size_t)ny * sz)) * q + i];
                     }
-                    double omega = (nm > 10) ? mi[10] : omega0;
-                    double mac[10];
+                    real omega = (nm > 10) ? mi[10] : omega0;
+                    real mac[10];
                     if ((t & 0xFFu) == 0) {
                         orc_bulk_moments(q, f, mac);
                     } else {
                         int vidx = (t >> 11) & 3u;
                         int kind = (t >> 8) & 7u;
-                        double u[3] = {0, 0, 0};
+                        real u[3] = {0, 0, 0};
                         if (kind == 1) { u[0] = d->bc_velocity[vidx][0]; u[1] = d->bc_velocity[vidx][1]; u[2] = d->bc_velocity[vidx][2]; }
                         orc_bc_solve(q, d->bc_matrix_q ? d->bc_matrix_q : q, orc_known_mask(q, t & 0xFFu), u, omega, f, mac);
                     }
                     collide_store(d, nm, mac, omega, mo);
                 }
-        double *tmp = o->m; o->m = o->m2; o->m2 = tmp;
+        real *tmp = o->m; o->m = o->m2; o->m2 = tmp;
     }
 }
 
@@ -439,8 +451,8 @@ void orc_sums(void *h, double *out)
     double s[6] = {0, 0, 0, 0, 0, 0};
     for (size_t k = 0; k < o->n; k++) {
         if ((o->type[k] & 0xFFu) == 0xFFu) continue;
-        const double *m = o->m + k * o->nm;
-        double rho = o->d.rho0 + m[0];
+        const real *m = o->m + k * o->nm;
+        double rho = o->d.rho0 + (double)m[0];
         double ux = m[1] / 3.0, uy = m[2] / 3.0, uz = m[3] / 3.0;
         s[0] += rho; s[1] += rho * ux; s[2] += rho * uy; s[3] += rho * uz;
         s[4] += 0.5 * rho * (ux * ux + uy * uy + uz * uz);

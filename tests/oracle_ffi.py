@@ -13,6 +13,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_DIR = os.path.join(ROOT, "oracle")
 ORACLE_SO = os.path.join(ORACLE_DIR, "liboracle.so")
+ORACLE_F32_SO = os.path.join(ORACLE_DIR, "liboracle_f32.so")
 REF_KAT_SO = os.path.join(ORACLE_DIR, "_ref", "libref_kat.so")
 
 NEWTONIAN, POWERLAW, BINGHAM = 0, 1, 2
@@ -39,15 +40,17 @@ def _ptr(a, t=C.c_double):
     return a.ctypes.data_as(C.POINTER(t))
 
 
-_lib = None
+_libs = {}
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(ORACLE_SO):
-            subprocess.check_call(["make", "-s", "liboracle.so"], cwd=ORACLE_DIR)
-        L = C.CDLL(ORACLE_SO)
+def lib(fp32=False):
+    """The FP64 oracle, or with fp32=True the same restatement built with FP32
+    arithmetic and storage (the round-off yardstick)."""
+    so = ORACLE_F32_SO if fp32 else ORACLE_SO
+    if so not in _libs:
+        if not os.path.exists(so):
+            subprocess.check_call(["make", "-s", os.path.basename(so)], cwd=ORACLE_DIR)
+        L = C.CDLL(so)
         L.orc_create.restype = C.c_void_p
         L.orc_create.argtypes = [C.POINTER(OrcDesc)]
         L.orc_destroy.argtypes = [C.c_void_p]
@@ -58,6 +61,10 @@ def lib():
         L.orc_step.argtypes = [C.c_void_p, C.c_int]
         L.orc_init_from_macro.argtypes = [C.c_void_p, D, D, D, D, C.c_int]
         L.orc_sums.argtypes = [C.c_void_p, D]
+        L.orc_threads.restype = C.c_int
+        _libs[so] = L
+        if fp32:   # its per-node functions take float arguments; only the domain API is used
+            return L
         L.orc_reconstruct.argtypes = [C.c_int, C.c_double, D, D]
         L.orc_bulk_moments.argtypes = [C.c_int, D, D]
         L.orc_known_mask.argtypes = [C.c_int, C.c_uint32]
@@ -68,9 +75,7 @@ def lib():
         L.orc_nnf_bingham.argtypes = [C.c_double] * 3
         L.orc_nnf_bingham.restype = C.c_double
         L.orc_collide.argtypes = [C.POINTER(OrcDesc), D, C.c_double, D, C.c_int]
-        L.orc_threads.restype = C.c_int
-        _lib = L
-    return _lib
+    return _libs[so]
 
 
 def ref_kat():
@@ -114,11 +119,13 @@ def make_desc(nx, ny, nz, q=19, periodic=(1, 1, 1), tau=0.8, rho0=1.0, force=(0,
 
 
 class OracleDomain:
-    """FP64 oracle domain; moments are [nz, ny, nx, nm] (x fastest)."""
+    """FP64 oracle domain (fp32=True: the FP32-arithmetic build of the same
+    restatement); moments are [nz, ny, nx, nm] (x fastest), float64 at the
+    interface in both builds."""
 
-    def __init__(self, desc):
+    def __init__(self, desc, fp32=False):
         self.desc = desc
-        self.L = lib()
+        self.L = lib(fp32)
         self.h = self.L.orc_create(C.byref(desc))
         if not self.h:
             raise MemoryError("oracle allocation failed")

@@ -5,8 +5,9 @@ import lattice_np
 import oracle_ffi
 
 
-def oracle_for(desc, node_types=None):
-    """An FP64 oracle domain with the same physics as a library descriptor."""
+def oracle_for(desc, node_types=None, fp32=False):
+    """An FP64 oracle domain with the same physics as a library descriptor
+    (fp32=True: the FP32-arithmetic build of the oracle)."""
     import mrlbm
     bcv = [tuple(desc.bc_velocity[k][a] for a in range(3)) for k in range(4)]
     kw = dict(q=desc.lattice, periodic=tuple(desc.periodic[a] for a in range(3)), tau=desc.tau, rho0=desc.rho0,
@@ -23,7 +24,7 @@ def oracle_for(desc, node_types=None):
     for k, c in ((4, lattice_np.CX), (7, lattice_np.CY), (9, lattice_np.CZ)):
         ext[k] = 4.5 * (sum(w[i] * c[i] ** 2 for i in range(19)) - 1 / 3)
     kw["exterior"] = ext
-    o = oracle_ffi.OracleDomain(oracle_ffi.make_desc(desc.nx, desc.ny, desc.nz, **kw))
+    o = oracle_ffi.OracleDomain(oracle_ffi.make_desc(desc.nx, desc.ny, desc.nz, **kw), fp32=fp32)
     if node_types is not None:
         o.set_node_types(node_types)
     return o

@@ -1,0 +1,91 @@
+"""Case mode: reference case folders compiled unchanged into this library's
+kernels (mr-lbm_b200/casebuild.py; the programs are built into oracle/_ref/cases
+by oracle/build_ref_cuda.sh), run next to the reference's own programs on the
+same inputs.
+
+* benchmark (README table case, D3Q19 256^3, cuRAND-perturbed field, 1000
+  steps): both programs draw the same cuRAND numbers, so their final fields
+  must agree to FP32 operation-order level.
+* taylorGreen switched to D3Q27, 256^3, Re 1600, u0 0.04, 1000 steps: the
+  kinetic-energy reports (every 100 steps) must agree.
+* lidDrivenCavity_3D 64^3: the case's own bc_definition.inc running inside the
+  z-march kernel must agree with the library's generic moment-BC solver.
+"""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import lattice_np
+import mrlbm
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF = os.path.join(ROOT, "oracle", "_ref")
+
+
+def run(exe, workdir):
+    if not os.path.exists(exe):
+        pytest.skip("%s not built (oracle/build_ref_cuda.sh needs the reference tree)" % exe)
+    os.makedirs(workdir, exist_ok=True)
+    r = subprocess.run([exe], cwd=workdir, capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+    m = re.search(r"MLUPS:\s*([0-9.]+)", r.stdout)
+    return float(m.group(1)) if m else None
+
+
+def fields(workdir, n, step):
+    base = os.path.join(workdir, "TEST", "000", "000_")
+    return {v: np.fromfile(base + "%s%06d.bin" % (v, step), dtype=np.float32).reshape(n, n, n)
+            for v in ("rho", "ux", "uy", "uz")}
+
+
+def u_err(a, b):
+    ua = np.stack([a["ux"], a["uy"], a["uz"]])
+    ub = np.stack([b["ux"], b["uy"], b["uz"]])
+    return lattice_np.rel_l2(ua, ub)
+
+
+def test_benchmark_case_matches_reference_program(tmp_path):
+    ml_ref = run(os.path.join(REF, "refsim_bench256"), tmp_path / "ref")
+    ml_ours = run(os.path.join(REF, "cases", "bench256"), tmp_path / "ours")
+    a, b = fields(tmp_path / "ours", 256, 1000), fields(tmp_path / "ref", 256, 1000)
+    e = u_err(a, b)
+    drho = float(np.max(np.abs(a["rho"] - b["rho"])))
+    print("benchmark 256^3 D3Q19: reference %.0f MLUPS, case mode %.0f MLUPS; u rel L2 %.2e, max |drho| %.2e"
+          % (ml_ref, ml_ours, e, drho))
+    assert e < 1e-4 and drho < 1e-5
+
+
+def test_taylor_green_d3q27_case_matches_reference_program(tmp_path):
+    ml_ref = run(os.path.join(REF, "refsim_tgv256_q27"), tmp_path / "ref")
+    ml_ours = run(os.path.join(REF, "cases", "tgv256_q27"), tmp_path / "ours")
+
+    def ke(d):
+        rows = [l.strip().split(",") for l in open(os.path.join(d, "TEST", "000", "000_totalKineticEnergy.txt"))]
+        return {int(r[1]): float(r[2]) for r in rows if len(r) == 3}
+
+    kr, ko = ke(tmp_path / "ref"), ke(tmp_path / "ours")
+    assert sorted(kr) == sorted(ko) and len(kr) == 9
+    worst = max(abs(ko[s] - kr[s]) / kr[s] for s in kr)
+    print("TGV 256^3 D3Q27: reference %.0f MLUPS, case mode %.0f MLUPS; KE worst rel diff %.2e" % (ml_ref, ml_ours, worst))
+    assert worst < 2e-5
+
+
+def test_lid_case_bc_snippet_equals_generic_solver(tmp_path):
+    run(os.path.join(REF, "cases", "lid64"), tmp_path / "case")
+    n = 64
+    d = mrlbm.lid_cavity_desc(n, re=100.0, lid_u=0.05)
+    dom = mrlbm.Domain(d)
+    dom.set_node_types(mrlbm.lid_cavity_node_types(n, n, n, 1))
+    dom.init_uniform()
+    dom.step(2000)
+    dom.save_macr_bin(str(tmp_path / "lib"), "000", 2000)
+    base = os.path.join(tmp_path, "lib", "000", "000_")
+    lib = {v: np.fromfile(base + "%s002000.bin" % v, dtype=np.float32).reshape(n, n, n) for v in ("rho", "ux", "uy", "uz")}
+    case = fields(tmp_path / "case", n, 2000)
+    e = u_err(case, lib)
+    print("lid64: case's own bc_definition vs generic solver, u rel L2 %.2e" % e)
+    assert e < 1e-4

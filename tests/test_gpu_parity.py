@@ -10,6 +10,14 @@ arithmetic against FP64, after the stated number of steps:
   sets their floor, in the reference as here).
 Both sides start from the same stored moments (the GPU's own initial state
 copied into the oracle), so the comparison isolates the step.
+
+Driven flows (a body force from rest, non-Newtonian omega) accumulate FP32
+round-off over the run instead of damping it, so a fixed bound does not fit
+them.  Their yardstick is the oracle's own FP32 build (oracle/liboracle_f32.so:
+the same restatement in FP32 arithmetic and storage) run from the same start:
+the GPU's error against FP64 must stay within twice that build's error (or the
+fixed bound, whichever is larger), i.e. no worse than a plain FP32
+implementation of the algorithm.
 """
 import numpy as np
 import pytest
@@ -23,7 +31,9 @@ TOL_L2, TOL_LINF = 2e-5, 2e-4
 TOL2_L2, TOL2_LINF = 3e-4, 2e-3   # second moments
 
 
-def run_pair(desc, steps, node_types=None, init=None, fluid=None):
+def run_pair(desc, steps, node_types=None, init=None, fluid=None, yardstick=False):
+    """GPU and FP64 oracle from the same stored start; with yardstick=True also
+    the FP32 oracle build, returned as a fourth item (its errors vs FP64)."""
     dom = mrlbm.Domain(desc)
     if node_types is not None:
         dom.set_node_types(node_types)
@@ -31,23 +41,32 @@ def run_pair(desc, steps, node_types=None, init=None, fluid=None):
         dom.init_uniform()
     else:
         init(dom)
-    m0 = dom.moments()
+    m0 = pu.gpu_to_oracle_layout(dom.moments())
     orc = pu.oracle_for(desc, node_types)
-    orc.set_moments(pu.gpu_to_oracle_layout(m0))
+    orc.set_moments(m0)
     dom.step(steps)
     orc.step(steps)
     g = dom.moments()
     o = orc.moments()
     dom.close()
-    return g, o, pu.compare(g, o, fluid)
+    if not yardstick:
+        return g, o, pu.compare(g, o, fluid)
+    o32 = pu.oracle_for(desc, node_types, fp32=True)
+    o32.set_moments(m0)
+    o32.step(steps)
+    y = pu.compare(np.moveaxis(o32.moments(), -1, 0), o, fluid)
+    return g, o, pu.compare(g, o, fluid), y
 
 
-def assert_close(res, l2=TOL_L2, linf=TOL_LINF, l2_2=TOL2_L2, linf_2=TOL2_LINF, skip=()):
+def assert_close(res, l2=TOL_L2, linf=TOL_LINF, l2_2=TOL2_L2, linf_2=TOL2_LINF, skip=(), yard=None):
     for k, (e2, einf) in res.items():
         if k in skip:
             continue
         a2, ainf = (l2_2, linf_2) if 4 <= k <= 9 else (l2, linf)
-        assert e2 <= a2 and einf <= ainf, "moment %d: rel L2 %.3e, rel Linf %.3e" % (k, e2, einf)
+        if yard is not None:
+            a2, ainf = max(a2, 2 * yard[k][0]), max(ainf, 2 * yard[k][1])
+        assert e2 <= a2 and einf <= ainf, "moment %d: rel L2 %.3e (bound %.1e), rel Linf %.3e (bound %.1e)" % (
+            k, e2, a2, einf, ainf)
 
 
 def tg_init(u0, L):
@@ -89,8 +108,11 @@ def test_duct_voxels_force_newtonian():
     solid[:, 1:-1, 1:-1] = rng.random((nz, ny - 2, nx - 2)) < 0.05
     nt = mrlbm.voxel_node_types(solid, (0, 0, 1))
     d = mrlbm.make_desc(nx, ny, nz, lattice=19, periodic=(0, 0, 1), tau=0.8, force=(0, 0, 2e-5))
-    g, o, res = run_pair(d, 150, node_types=nt, fluid=solid == 0)
+    # early: round-off has not built up yet, the fixed FP32 bounds hold
+    g, o, res = run_pair(d, 10, node_types=nt, fluid=solid == 0)
     assert_close(res)
+    g, o, res, yard = run_pair(d, 150, node_types=nt, fluid=solid == 0, yardstick=True)
+    assert_close(res, yard=yard)
 
 
 def sheared_start(nx, ny, nz, gamma=2e-3):
@@ -114,8 +136,9 @@ def test_nonnewtonian_sheared(rheology, kw):
     nt = mrlbm.voxel_node_types(solid, (1, 0, 1))
     d = mrlbm.make_desc(nx, ny, nz, lattice=19, periodic=(1, 0, 1), tau=0.8, force=(3e-6, 0, 1e-6),
                         rheology=rheology, **kw)
-    g, o, res = run_pair(d, 60, node_types=nt, init=sheared_start(nx, ny, nz), fluid=solid == 0)
-    assert_close(res, l2=1e-4, linf=2e-3, l2_2=1e-3, linf_2=1e-2)
+    g, o, res, yard = run_pair(d, 60, node_types=nt, init=sheared_start(nx, ny, nz), fluid=solid == 0,
+                               yardstick=True)
+    assert_close(res, l2=1e-4, linf=2e-3, l2_2=1e-3, linf_2=1e-2, yard=yard)
 
 
 def test_duct_voxels_force_powerlaw():
@@ -126,11 +149,11 @@ def test_duct_voxels_force_powerlaw():
     nt = mrlbm.voxel_node_types(solid, (0, 0, 1))
     d = mrlbm.make_desc(nx, ny, nz, lattice=19, periodic=(0, 0, 1), tau=0.8, force=(0, 0, 2e-5),
                         rheology=mrlbm.POWERLAW, nnf_n=0.8)
-    g, o, res = run_pair(d, 150, node_types=nt, fluid=solid == 0)
+    g, o, res, yard = run_pair(d, 150, node_types=nt, fluid=solid == 0, yardstick=True)
     # the power law sets omega = 0 below |S| = 1e-6 (src/nnf.h:73-74): nodes
     # whose shear crosses that threshold at a different step in FP32 and FP64
     # differ by O(1) in omega, so the bound is looser than for Newtonian flow
-    assert_close(res, l2=3e-3, linf=2e-2, l2_2=3e-3, linf_2=2e-2)
+    assert_close(res, l2=3e-3, linf=2e-2, l2_2=3e-3, linf_2=2e-2, yard=yard)
 
 
 def test_bingham_plates():
@@ -139,10 +162,10 @@ def test_bingham_plates():
     nt = mrlbm.voxel_node_types(solid, (1, 0, 1))
     d = mrlbm.make_desc(nx, ny, nz, lattice=19, periodic=(1, 0, 1), tau=0.9, force=(5e-5, 0, 0),
                         rheology=mrlbm.BINGHAM, nnf_yield=1e-5)
-    g, o, res = run_pair(d, 150, node_types=nt)
+    g, o, res, yard = run_pair(d, 150, node_types=nt, yardstick=True)
     # Bingham: omega = omega_p max(0, 1 - S_Y/|S|) switches at the yield
     # surface; FP32 and FP64 place it one node apart in places
-    assert_close(res, l2=5e-3, linf=3e-2, l2_2=5e-3, linf_2=3e-2)
+    assert_close(res, l2=5e-3, linf=3e-2, l2_2=5e-3, linf_2=3e-2, yard=yard)
 
 
 @pytest.mark.parametrize("storage,tol", [(mrlbm.F16, 5e-3), (mrlbm.BF16, 4e-2)])
