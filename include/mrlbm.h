@@ -165,6 +165,27 @@ mrlbm_status mrlbm_reduce_fp64(mrlbm_domain* dom, mrlbm_sums* out);
  * call takes the snapshot and returns 1). */
 mrlbm_status mrlbm_residual(mrlbm_domain* dom, double* residual);
 
+/* The sums of mrlbm_reduce_fp64 (every node counted: the field carries no node
+ * types) for a caller-owned FP32 field in the reference's idxMom layout
+ * (fmom: device memory of the current device, nx*ny*nz*num_moments floats,
+ * nx, ny, nz multiples of 8; stream may be NULL), computed without allocating
+ * anything.  No counterpart in the reference: its reductions of fMom
+ * (src/auxFunctions.cu:8-58, src/treatData.cu:105-165) cudaMalloc a partials
+ * buffer on every call.
+ * Scratch: a file-scope __device__ array of 37,952 bytes per device (592 block
+ * partials + 8 results); the call always uses 592 blocks and strides over
+ * larger fields, and a request beyond the array's size is rejected with
+ * MRLBM_EINVAL.  Nothing in it has to start at zero (each call writes what it
+ * reads).  The first call on a device looks up the array's address
+ * (cudaGetSymbolAddress, with that device current): make it before any stream
+ * capture begins.  Calls share the array per device, so calls whose
+ * executions overlap on one device (two host threads, or unordered streams)
+ * race and return wrong sums: serialise them.  Synchronises `stream`.  For a
+ * field with the same values as a domain's F32 moments the result equals
+ * mrlbm_reduce_fp64's for that domain (same blocks, same summation order). */
+mrlbm_status mrlbm_reduce_fp64_ref_layout_noalloc(const float* fmom, int nx, int ny, int nz, int num_moments,
+                                                  double rho0, void* stream, mrlbm_sums* out);
+
 /* Files in the reference formats. */
 /* <path>/<id>/checkpoint/_curr_step.bin, _fMom.bin, _fGhost.{X,Y,Z}_{0,1}.bin
  * (src/checkpoint.cu:129-186, 372-382; POSIX separators). */

@@ -158,6 +158,8 @@ def lib():
             "mrlbm_server_inject_nan": [VP, C.c_int],
             "mrlbm_server_keep_results": [VP, C.c_int],
             "mrlbm_request_domain": [C.POINTER(Request), C.c_int, C.POINTER(VP)],
+            "mrlbm_reduce_fp64_ref_layout_noalloc": [VP, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, VP,
+                                                     C.POINTER(Sums)],
         }
         for name, args in sigs.items():
             f = getattr(L, name)
@@ -542,6 +544,17 @@ def bc_class_info(lattice, node_type, bc_velocity, omega0, bc_matrix_q=0):
     check(lib().mrlbm_bc_class_info(lattice, bc_matrix_q, int(node_type), C.byref(uv), float(omega0), _fp(out),
                                     C.byref(known)))
     return out, known.value
+
+
+def reduce_ref_layout_noalloc(fmom_device_ptr, nx, ny, nz, num_moments, rho0=1.0, stream=0):
+    """FP64 sums of a caller-owned FP32 device field in the reference's idxMom
+    layout, computed without any allocation (a static per-device scratch
+    array; calls on one device must not overlap).  fmom_device_ptr and stream
+    are raw addresses (int)."""
+    s = Sums()
+    check(lib().mrlbm_reduce_fp64_ref_layout_noalloc(VP(fmom_device_ptr), int(nx), int(ny), int(nz),
+                                                      int(num_moments), float(rho0), VP(stream), C.byref(s)))
+    return s.as_dict()
 
 
 def lid_cavity_node_types(nx, ny, nz, lid_velocity_index=1):
