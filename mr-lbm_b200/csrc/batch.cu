@@ -45,7 +45,7 @@ namespace {
 template <int Q, typename T>
 mrlbm_status set_attr(size_t& smem)
 {
-    smem = ZSmem<Q, T, BATCH_TYI>::bytes;
+    smem = ZSmem<Q, T, batch_tyi(Q)>::bytes;
     cudaError_t e = cudaFuncSetAttribute(batch_step<Q, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return fail(MRLBM_ECUDA, "batch attribute: %s", cudaGetErrorString(e));
     return MRLBM_OK;
@@ -54,7 +54,7 @@ mrlbm_status set_attr(size_t& smem)
 template <int Q, typename T>
 void launch(mrlbm_batch* b)
 {
-    batch_step<Q, T><<<b->grid, 32 * (BATCH_TYI + 2), b->smem, b->stream>>>(b->d_doms, b->d_items, b->d_ctl);
+    batch_step<Q, T><<<b->grid, 32 * (batch_tyi(Q) + 2), b->smem, b->stream>>>(b->d_doms, b->d_items, b->d_ctl);
 }
 
 void launch_any(mrlbm_batch* b)
@@ -129,10 +129,11 @@ mrlbm_status refresh(mrlbm_batch* b)
         hd[id].map[0] = dom->tmap[0];
         hd[id].map[1] = dom->tmap[1];
         hd[id].parity_offset = b->offsets[id];
-        const int gx = (dom->d.nx + TILE_X - 1) / TILE_X, gy = (dom->d.ny + BATCH_TYI - 1) / BATCH_TYI;
+        const int ty = batch_tyi(dom->q);
+        const int gx = (dom->d.nx + TILE_X - 1) / TILE_X, gy = (dom->d.ny + ty - 1) / ty;
         for (int z0 = 0; z0 < dom->d.nz; z0 += dom->lz)
             for (int by = 0; by < gy; by++)
-                for (int bx = 0; bx < gx; bx++) items.push_back({id, bx * TILE_X, by * BATCH_TYI, z0});
+                for (int bx = 0; bx < gx; bx++) items.push_back({id, bx * TILE_X, by * ty, z0});
     }
     std::stable_sort(items.begin(), items.end(), [&](const BatchItem& u, const BatchItem& v) {
         const mrlbm_domain* du = b->members[u.dom];
@@ -238,10 +239,10 @@ extern "C" mrlbm_status mrlbm_batch_create(int lattice, int storage, mrlbm_batch
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (lattice == 19)
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, storage == MRLBM_F32 ? batch_step<19, float> : batch_step<19, __half>,
-                                                      32 * (BATCH_TYI + 2), b->smem);
+                                                      32 * (batch_tyi(lattice) + 2), b->smem);
     else
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, storage == MRLBM_F32 ? batch_step<27, float> : batch_step<27, __half>,
-                                                      32 * (BATCH_TYI + 2), b->smem);
+                                                      32 * (batch_tyi(lattice) + 2), b->smem);
     b->grid = sms * std::max(per_sm, 1);
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||

@@ -10,7 +10,8 @@
 
 namespace mrlbm {
 
-constexpr int BATCH_TYI = 14;  // rows per CTA of the batched kernel (16 warps)
+// rows per CTA: the single-domain kernel's (members share its tensor maps)
+__host__ __device__ constexpr int batch_tyi(int q) { return tile_y(q); }
 
 // Per-domain data the batched kernel needs; both parities are precomputed so
 // the kernel only selects.  64-byte aligned for the tensor maps.
@@ -37,20 +38,20 @@ struct BatchCtl {
 
 template <int Q, typename T, int FLAGS>
 __device__ __forceinline__ bool batch_column(const StepArgs& a, const CUtensorMap* map, const BatchItem& it,
-                                             const ZSmem<Q, T, BATCH_TYI>& sm, unsigned& g0)
+                                             const ZSmem<Q, T, batch_tyi(Q)>& sm, unsigned& g0)
 {
-    return zmarch_column<Q, T, FLAGS, BATCH_TYI>(a, map, it.X0, it.Y0, it.z0, sm, g0);
+    return zmarch_column<Q, T, FLAGS, batch_tyi(Q)>(a, map, it.X0, it.Y0, it.z0, min(it.z0 + a.lz, a.nz), sm, g0);
 }
 
 template <int Q, typename T>
-__global__ void __launch_bounds__(32 * (BATCH_TYI + 2), 1)
+__global__ void __launch_bounds__(32 * (batch_tyi(Q) + 2), 1)
     batch_step(const BatchDomain* __restrict__ doms, const BatchItem* __restrict__ items, BatchCtl* ctl)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ int s_item;
     __shared__ __align__(16) StepArgs s_args;
-    const ZSmem<Q, T, BATCH_TYI> sm(smem);
-    zmarch_init_barriers<Q, T, BATCH_TYI>(sm);
+    const ZSmem<Q, T, batch_tyi(Q)> sm(smem);
+    zmarch_init_barriers<Q, T, batch_tyi(Q)>(sm);
     const int step = *((volatile int*)&ctl->step);
     const int nitems = *((volatile int*)&ctl->nitems);
     unsigned g0 = 0;

@@ -10,7 +10,6 @@
 
 namespace mrlbm {
 
-constexpr int TILE_Y = 14;       // interior rows per CTA (16 warps with the halo rows)
 constexpr int GRAPH_STEPS = 16;  // launches per captured graph (even: parities chain)
 
 }  // namespace mrlbm
@@ -39,7 +38,8 @@ struct mrlbm_domain {
     bool has_bc = false;
     float ext[11] = {};
     float scale[11] = {}, iscale[11] = {};
-    int lz = 16;
+    int lz = 16;                     // z planes per CTA (batch members: per work item)
+    int nsm = 148;                   // SMs of the device the domain lives on
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double* red_scratch = nullptr;  // block partials + 8 results

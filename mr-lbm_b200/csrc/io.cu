@@ -235,7 +235,7 @@ extern "C" mrlbm_status mrlbm_save_info(mrlbm_domain* dom, const char* path_file
     fprintf(f, "             Nsteps: %d\n", nsteps);
     fprintf(f, "              MLUPS: %.6e\n", mlups);
     fprintf(f, "                 BX: %d\n", TILE_X);
-    fprintf(f, "                 BY: %d\n", TILE_Y);
+    fprintf(f, "                 BY: %d\n", tile_y(dom->q));
     fprintf(f, "                 BZ: %d\n", dom->lz);
     fprintf(f, "--------------------------------------------------------------------------------\n");
     fprintf(f, "\n------------------------------ BOUNDARY CONDITIONS -----------------------------\n");

@@ -51,6 +51,12 @@ constexpr int TILE_X = 30;   // interior nodes per warp row
 constexpr int XOFF = 4;      // padded column of x = 0 (x = -1 is the ghost column)
 constexpr int BOX_X = 40;    // TMA box width (elements) covering the 32 lanes
 constexpr int NSTAGE = 3;    // TMA ring depth
+// interior rows per CTA (warps = rows + 2 halo rows): 16 warps at 128
+// registers fill the register file.  (18 rows at 96 registers measured
+// slower: the compiler's schedule needs the registers more than the SM needs
+// the extra warps.)
+constexpr int TYI19 = 14, TYI27 = 14;
+__host__ __device__ constexpr int tile_y(int q) { return q == 27 ? TYI27 : TYI19; }
 constexpr uint8_t CLS_BULK = 0;
 constexpr uint8_t CLS_SOLID = 255;
 constexpr unsigned WAIT_LIMIT = 1u << 26;  // mbarrier polls before giving up (~seconds)
@@ -82,7 +88,7 @@ struct StepArgs {
     int nx, ny, nz, pitch;
     long long plane, field;  // elements
     int periodic;            // bit a set: axis a periodic
-    int lz;                  // planes per CTA
+    int lz;                  // planes per CTA / per batch work item
     int step;                // step number (read by case-mode boundary snippets)
     float rho0, omega0;
     float fx, fy, fz;
@@ -172,29 +178,61 @@ __device__ __forceinline__ void reconstruct(const float* m, float rho0, float* f
     }
 }
 
-// Raw sums over the lattice, pairwise: rho, j, and sum f c_a c_b.
+// Raw sums over the lattice: rho, j, and sum f c_a c_b (xx, xy, xz, yy, yz,
+// zz), as a tensor product.  Reduce along z first (per (c_x, c_y): the
+// zeroth, first and second z moments), then along y and x, keeping only the
+// per-axis orders that moments up to second order need: 66 additions for
+// D3Q27 and 42 for D3Q19, against 111 and 63 summing opposite pairs.
 template <int Q>
-__device__ __forceinline__ void lattice_sums(const float* p, float& r, float* j, float* P)
+__host__ __device__ __forceinline__ void lattice_sums(const float* p, float& r, float* j, float* P)
 {
-    r = p[0];
-    j[0] = j[1] = j[2] = 0.f;
-#pragma unroll
-    for (int k = 0; k < 6; k++) P[k] = 0.f;
-    static_for<0, Q / 2>([&](auto h) {
-        constexpr int i = 2 * h + 1;
-        constexpr int cx = lat_cx(i), cy = lat_cy(i), cz = lat_cz(i);
-        const float s = p[i] + p[i + 1], d = p[i] - p[i + 1];
-        r += s;
-        if constexpr (cx > 0) j[0] += d; else if constexpr (cx < 0) j[0] -= d;
-        if constexpr (cy > 0) j[1] += d; else if constexpr (cy < 0) j[1] -= d;
-        if constexpr (cz > 0) j[2] += d; else if constexpr (cz < 0) j[2] -= d;
-        if constexpr (cx != 0) P[0] += s;
-        if constexpr (cy != 0) P[3] += s;
-        if constexpr (cz != 0) P[5] += s;
-        if constexpr (cx * cy > 0) P[1] += s; else if constexpr (cx * cy < 0) P[1] -= s;
-        if constexpr (cx * cz > 0) P[2] += s; else if constexpr (cx * cz < 0) P[2] -= s;
-        if constexpr (cy * cz > 0) P[4] += s; else if constexpr (cy * cz < 0) P[4] -= s;
+    // S*[X + 3Y] with X = c_x + 1, Y = c_y + 1
+    float S0[9], S1[9], S2[9];
+    static_for<0, 9>([&](auto C) {
+        constexpr int X = C % 3, Y = C / 3;
+        constexpr int i0 = lat_find(Q, X - 1, Y - 1, 0);
+        constexpr int ip = lat_find(Q, X - 1, Y - 1, 1), im = lat_find(Q, X - 1, Y - 1, -1);
+        if constexpr (ip < 0) {   // D3Q19 (c_x, c_y) corners carry c_z = 0 only
+            S0[C] = p[i0];
+            S1[C] = 0.f;
+            S2[C] = 0.f;
+        } else {
+            const float a = p[ip] + p[im];
+            S0[C] = a + p[i0];
+            S1[C] = p[ip] - p[im];
+            S2[C] = a;
+        }
     });
+    // T<ay><az>[X]: y order ay, z order az, per c_x
+    float T00[3], T10[3], T20[3], T01[3], T11[3], T02[3];
+    static_for<0, 3>([&](auto XX) {
+        constexpr int X = XX;
+        const float a0 = S0[X + 6] + S0[X];
+        T00[X] = a0 + S0[X + 3];
+        T10[X] = S0[X + 6] - S0[X];
+        T20[X] = a0;
+        if constexpr (Q == 27 || X == 1) {
+            const float a1 = S1[X + 6] + S1[X];
+            T01[X] = a1 + S1[X + 3];
+            T11[X] = S1[X + 6] - S1[X];
+            T02[X] = S2[X + 6] + S2[X] + S2[X + 3];
+        } else {
+            T01[X] = S1[X + 3];
+            T11[X] = 0.f;
+            T02[X] = S2[X + 3];
+        }
+    });
+    const float b = T00[2] + T00[0];
+    r = b + T00[1];
+    j[0] = T00[2] - T00[0];
+    j[1] = T10[0] + T10[1] + T10[2];
+    j[2] = T01[0] + T01[1] + T01[2];
+    P[0] = b;
+    P[1] = T10[2] - T10[0];
+    P[2] = T01[2] - T01[0];
+    P[3] = T20[0] + T20[1] + T20[2];
+    P[4] = Q == 27 ? T11[0] + T11[1] + T11[2] : T11[1];
+    P[5] = T02[0] + T02[1] + T02[2];
 }
 
 // mac = rho, u (unscaled), Pi_hat (unscaled xx,xy,xz,yy,yz,zz) from the
@@ -399,6 +437,11 @@ __host__ __device__ constexpr bool ex_group_used()
     return false;
 }
 
+// float4 slot of group G: D3Q27 packs all six groups, D3Q19 only the two
+// c_x = 0 ones (G = 1, 4)
+__host__ __device__ constexpr int ex_npack(int Q) { return Q == 27 ? 6 : 2; }
+__host__ __device__ constexpr int ex_slot4(int Q, int G) { return Q == 27 ? G : (G == 1 ? 0 : 1); }
+
 // store group G of this lane's populations (its c_z = -1, 0, +1 members)
 template <int Q, int G>
 __device__ __forceinline__ void ex_write(const float* f, float4* e4, int NW, int warp, int lane)
@@ -413,7 +456,7 @@ __device__ __forceinline__ void ex_write(const float* f, float4* e4, int NW, int
                 else v.z = f[i];
             }
         });
-        e4[(G * NW + warp) * 32 + lane] = v;
+        e4[(ex_slot4(Q, G) * NW + warp) * 32 + lane] = v;
     }
 }
 
@@ -425,7 +468,7 @@ __device__ __forceinline__ void ex_read(float* g, const float4* e4, int NW, int 
         constexpr int cx = (G % 3) - 1, cy = G >= 3 ? 1 : -1;
         const int w = min(max(warp - cy, 0), NW - 1);
         const int l = (lane - cx) & 31;
-        const float4 v = e4[(G * NW + w) * 32 + l];
+        const float4 v = e4[(ex_slot4(Q, G) * NW + w) * 32 + l];
         static_for<1, Q>([&](auto I) {
             constexpr int i = I;
             if constexpr (lat_cy(i) != 0 && ex_group(i) == G && ex_packed(Q, i))
@@ -436,7 +479,7 @@ __device__ __forceinline__ void ex_read(float* g, const float4* e4, int NW, int 
 
 template <int Q, int NW>
 struct Exchange {
-    static constexpr int NPACK = 6;                  // float4 groups
+    static constexpr int NPACK = ex_npack(Q);        // float4 groups
     static constexpr int NSCAL = Q == 19 ? 4 : 0;    // scalar slots
     static constexpr size_t bytes_per_buffer = (size_t)NW * 32 * (NPACK * 16 + NSCAL * 4);
 };
@@ -459,7 +502,7 @@ __device__ __forceinline__ void prod_a(const StepArgs& a, const T* stage, int k,
     }
     float f[Q];
     reconstruct<Q>(mc, a.rho0, f);
-    float4* e4 = ex4 + (k & 1) * (6 * NW * 32);
+    float4* e4 = ex4 + (k & 1) * (ex_npack(Q) * NW * 32);
     float* e1 = ex1 + (k & 1) * (4 * NW * 32);
     ex_write<Q, 0>(f, e4, NW, warp, lane);
     ex_write<Q, 1>(f, e4, NW, warp, lane);
@@ -505,7 +548,7 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
                                        float (&up_old)[NUP], float (&mid)[NMID], float om_out)
 {
     constexpr int NW = TYI + 2;
-    const float4* e4 = ex4 + (k & 1) * (6 * NW * 32);
+    const float4* e4 = ex4 + (k & 1) * (ex_npack(Q) * NW * 32);
     const float* e1 = ex1 + (k & 1) * (4 * NW * 32);
     float g[Q];
     ex_read<Q, 0>(g, e4, NW, warp, lane);
@@ -529,7 +572,11 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
         if constexpr (lat_cy(i) == 0) g[i] = gsh[i];
     });
 
-    if (k >= 2) {
+    {
+        // consumptions 0 and 1 complete no plane: computed like the others
+        // (one straight block the compiler can interleave with the
+        // production), nothing read from the class map or stored
+        const bool live = interior && k >= 2;
         const int zd = zp - 1;
         float p[Q];
         static_for<0, Q>([&](auto I) {
@@ -543,7 +590,7 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
         const float omega = OMF ? om_out : a.omega0;
         const long long oidx = pidx(x, y, zd, a.pitch, a.plane);
         uint8_t cls = CLS_BULK;
-        if constexpr ((FLAGS & F_BC) != 0) cls = interior ? __ldg(a.cls + oidx) : CLS_SOLID;
+        if constexpr ((FLAGS & F_BC) != 0) cls = live ? __ldg(a.cls + oidx) : CLS_SOLID;
         float mac[10];
         {
             float r, j[3], P[6];
@@ -567,7 +614,7 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
 #pragma unroll
             for (int m = 0; m < NM; m++) o[m] = o[m] * a.scale[m];
         }
-        if (interior && cls != CLS_SOLID) {
+        if (live && cls != CLS_SOLID) {
             store_node<T, NM>(a, oidx, o);
             // periodic axes: keep the ghost shell equal to the wrapped interior
             const bool gx = (a.periodic & 1) && (x == 0 || x == a.nx - 1);
@@ -700,16 +747,16 @@ struct ZSmem {
         bars = reinterpret_cast<uint64_t*>(smem);
         stages = smem + 128;
         ex4 = reinterpret_cast<float4*>(stages + NSTAGE * stage_max);
-        ex1 = reinterpret_cast<float*>(ex4 + 2 * 6 * NW * 32);
+        ex1 = reinterpret_cast<float*>(ex4 + 2 * ex_npack(Q) * NW * 32);
     }
 };
 
-// One column (X0, Y0) x planes [z0, z0 + lz) of one domain.  g0 is the
-// CTA's running production count (advanced by the column's productions).
-// Returns false when a bounded wait timed out (the CTA must stop).
+// One column (X0, Y0) x planes [z0, zend) of one domain.  g0 is the CTA's
+// running production count (advanced by the column's productions).  Returns
+// false when a bounded wait timed out (the CTA must stop).
 template <int Q, typename T, int FLAGS, int TYI, typename BCP = TableBC>
 __device__ __forceinline__ bool zmarch_column(const StepArgs& a, const CUtensorMap* map, int X0, int Y0, int z0,
-                                              const ZSmem<Q, T, TYI>& sm, unsigned& g0)
+                                              int zend, const ZSmem<Q, T, TYI>& sm, unsigned& g0)
 {
     using ZM = ZMarch<Q, T, FLAGS, TYI, BCP>;
     constexpr int NUP = ZM::NUP, NMID = ZM::NMID;
@@ -717,15 +764,17 @@ __device__ __forceinline__ bool zmarch_column(const StepArgs& a, const CUtensorM
     const int x = X0 - 1 + lane, y = Y0 - 1 + warp;
     constexpr int ALIGN = 16 / (int)sizeof(T);      // elements per 16 bytes (TMA x alignment)
     const int p0 = (X0 - 1 + XOFF) & ~(ALIGN - 1);  // aligned box start (padded column)
-    const int zend = min(z0 + a.lz, a.nz);
     // the ring stride is the flag-independent maximum; ZM's stage_al only
     // sizes the copies
     ZM zm{a, map, sm.bars, sm.stages, sm.ex4, sm.ex1, g0, lane, warp, (x + XOFF) - p0, x, y, z0, Y0, p0,
           zend - z0 + 2 /* planes z0-1 .. zend */,
           lane >= 1 && lane <= TILE_X && x < a.nx && warp >= 1 && warp <= TYI && y < a.ny};
 
-    if (threadIdx.x == 0)
+    if (threadIdx.x == 0) {
+        // the ring was last read through the generic proxy (previous column)
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         for (int s = 0; s < NSTAGE && s < zm.nprod; s++) zm.load(s);
+    }
 
     float upA[NUP], upB[NUP], mid[NMID], gA[Q], gB[Q];
 #pragma unroll
@@ -788,7 +837,9 @@ __device__ __forceinline__ void zmarch_init_barriers(const ZSmem<Q, T, TYI>& sm)
     __syncthreads();
 }
 
-// Single-domain step: one CTA per (x tile, y tile, z chunk).
+// Single-domain step: one CTA per (x tile, y tile, z chunk of lz planes).
+// Launch order runs x tiles fastest, so the CTAs resident at one time march
+// neighbouring columns through the same planes and their halo reads hit L2.
 template <int Q, typename T, int FLAGS, int TYI, typename BCP = TableBC>
 __global__ void __launch_bounds__(32 * (TYI + 2), 1)
     zmarch_step(const __grid_constant__ CUtensorMap map_in, const StepArgs a)
@@ -797,8 +848,15 @@ __global__ void __launch_bounds__(32 * (TYI + 2), 1)
     const ZSmem<Q, T, TYI> sm(smem);
     zmarch_init_barriers<Q, T, TYI>(sm);
     unsigned g0 = 0;
-    (void)zmarch_column<Q, T, FLAGS, TYI, BCP>(a, &map_in, blockIdx.x * TILE_X, blockIdx.y * TYI, blockIdx.z * a.lz, sm,
-                                          g0);
+    const int z0 = blockIdx.z * a.lz;
+    (void)zmarch_column<Q, T, FLAGS, TYI, BCP>(a, &map_in, blockIdx.x * TILE_X, blockIdx.y * TYI, z0,
+                                          min(z0 + a.lz, a.nz), sm, g0);
+}
+
+// Grid of the single-domain step.
+__host__ __device__ inline dim3 zmarch_grid(int nx, int ny, int nz, int tyi, int lz)
+{
+    return dim3((nx + TILE_X - 1) / TILE_X, (ny + tyi - 1) / tyi, (nz + lz - 1) / lz);
 }
 
 template <int Q, typename T, int FLAGS, int TYI>

@@ -69,6 +69,14 @@ __host__ __device__ constexpr int lat_cz_slot(int Q, int i)
     return n;
 }
 
+// Index of the direction (cx, cy, cz) in the first Q entries, -1 if absent.
+__host__ __device__ constexpr int lat_find(int Q, int cx, int cy, int cz)
+{
+    for (int i = 0; i < Q; i++)
+        if (lat_cx(i) == cx && lat_cy(i) == cy && lat_cz(i) == cz) return i;
+    return -1;
+}
+
 // Compile-time loop: f(std::integral_constant<int, I>) for I = B .. E-1, so
 // every lattice index (and everything computed from it) is a constant
 // expression and register arrays indexed by it never spill to local memory.

@@ -278,24 +278,38 @@ mrlbm_status mrlbm::domain_alloc(mrlbm_domain* dom)
     dom->red_blocks = 148 * 4;
     CK(cudaMalloc(&dom->red_scratch, (size_t)(dom->red_blocks * 8 + 8) * sizeof(double)));
     CK(cudaMallocHost(&dom->red_host, 8 * sizeof(double)));
+    {
+        int dev = 0, nsm = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        dom->nsm = nsm > 0 ? nsm : 148;
+    }
     dom->lz = choose_lz(dom);
     return MRLBM_OK;
 }
 
+// z planes per CTA.  A CTA (one per SM at a time) produces lz + 2 planes for
+// lz outputs, and the grid runs in ceil(CTAs / SMs) waves, so the step time
+// goes as waves * (lz + 2 + start-up): pick the chunk count that minimises it (the last
+// wave full, few restarts).
 int mrlbm::choose_lz(const mrlbm_domain* dom)
 {
     const mrlbm_desc& d = dom->d;
-    const int gx = (d.nx + TILE_X - 1) / TILE_X;
-    const int gy = (d.ny + TILE_Y - 1) / TILE_Y;
-    const long long cols = (long long)gx * gy;
-    // aim for >= 8 waves of one 512-thread CTA per SM, keep LZ >= 16
-    long long want = 148LL * 8;
-    int nzc = (int)((want + cols - 1) / cols);
-    if (nzc < 1) nzc = 1;
-    int lz = (d.nz + nzc - 1) / nzc;
-    if (lz < 16) lz = 16;
-    if (lz > d.nz) lz = d.nz;
-    return lz;
+    const int ty = tile_y(dom->q);
+    const long long cols = (long long)((d.nx + TILE_X - 1) / TILE_X) * ((d.ny + ty - 1) / ty);
+    long long best_cost = -1;
+    int best = d.nz;
+    for (int nzc = 1; nzc <= d.nz; nzc++) {
+        const int lz = (d.nz + nzc - 1) / nzc;
+        const long long ctas = cols * ((d.nz + lz - 1) / lz);
+        const long long waves = (ctas + dom->nsm - 1) / dom->nsm;
+        const long long cost = waves * (lz + 2 + 3);  // + a CTA start-up of about 3 planes
+        if (best_cost < 0 || cost < best_cost) {
+            best_cost = cost;
+            best = lz;
+        }
+    }
+    return best;
 }
 
 extern "C" mrlbm_status mrlbm_domain_create(const mrlbm_desc* desc, mrlbm_domain** out)
@@ -740,7 +754,7 @@ static EncodeTiledFn encode_fn()
 }
 
 // 4-D map over one padded moment buffer with dimension order (x, moment, y, z)
-// so that a box of (40, nm, TILE_Y+2, 1) lands in shared memory as
+// so that a box of (40, nm, tile_y(q) + 2, 1) lands in shared memory as
 // [row][moment][x]: one plane of a CTA column per copy.
 mrlbm_status mrlbm::make_tensor_maps(mrlbm_domain* dom)
 {
@@ -755,7 +769,7 @@ mrlbm_status mrlbm::make_tensor_maps(mrlbm_domain* dom)
                                 (cuuint64_t)(d.nz + 2)};
     const cuuint64_t strides[3] = {(cuuint64_t)dom->field * es, (cuuint64_t)dom->pitch * es,
                                    (cuuint64_t)dom->plane * es};
-    const cuuint32_t box[4] = {(cuuint32_t)BOX_X, (cuuint32_t)dom->nm, (cuuint32_t)(TILE_Y + 2), 1};
+    const cuuint32_t box[4] = {(cuuint32_t)BOX_X, (cuuint32_t)dom->nm, (cuuint32_t)(tile_y(dom->q) + 2), 1};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     for (int b = 0; b < 2; b++) {
         CUresult r = enc(&dom->tmap[b], dt, 4, dom->m[b], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,

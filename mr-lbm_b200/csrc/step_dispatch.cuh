@@ -12,10 +12,11 @@ namespace mrlbm {
 template <int Q, typename T, int FLAGS>
 static mrlbm_status launch_step_t(const CUtensorMap& map, const StepArgs& a, cudaStream_t s)
 {
-    constexpr int NW = TILE_Y + 2;
-    constexpr size_t smem = step_smem_bytes<Q, T, FLAGS, TILE_Y>();
+    constexpr int TYI = tile_y(Q);
+    constexpr int NW = TYI + 2;
+    constexpr size_t smem = step_smem_bytes<Q, T, FLAGS, TYI>();
     static_assert(smem <= 232448, "shared memory over the sm_100 limit");
-    auto kern = zmarch_step<Q, T, FLAGS, TILE_Y>;
+    auto kern = zmarch_step<Q, T, FLAGS, TYI>;
     int dev = 0;
     cudaGetDevice(&dev);
     static int attr_done_mask = 0;  // one bit per device (up to 32)
@@ -24,7 +25,7 @@ static mrlbm_status launch_step_t(const CUtensorMap& map, const StepArgs& a, cud
         if (e != cudaSuccess) return fail(MRLBM_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
         attr_done_mask |= 1 << (dev & 31);
     }
-    dim3 grid((a.nx + TILE_X - 1) / TILE_X, (a.ny + TILE_Y - 1) / TILE_Y, (a.nz + a.lz - 1) / a.lz);
+    const dim3 grid = zmarch_grid(a.nx, a.ny, a.nz, TYI, a.lz);
     kern<<<grid, 32 * NW, smem, s>>>(map, a);
     return MRLBM_OK;
 }

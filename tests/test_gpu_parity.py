@@ -108,11 +108,12 @@ def test_duct_voxels_force_newtonian():
     solid[:, 1:-1, 1:-1] = rng.random((nz, ny - 2, nx - 2)) < 0.05
     nt = mrlbm.voxel_node_types(solid, (0, 0, 1))
     d = mrlbm.make_desc(nx, ny, nz, lattice=19, periodic=(0, 0, 1), tau=0.8, force=(0, 0, 2e-5))
-    # early: round-off has not built up yet, the fixed FP32 bounds hold
-    g, o, res = run_pair(d, 10, node_types=nt, fluid=solid == 0)
-    assert_close(res)
-    g, o, res, yard = run_pair(d, 150, node_types=nt, fluid=solid == 0, yardstick=True)
-    assert_close(res, yard=yard)
+    # from rest |u| grows from zero, so u carries the round-off of rho ~ 1 at
+    # a tiny magnitude from the first step on: the FP32 yardstick bounds both
+    # an early and a later state
+    for steps in (10, 150):
+        g, o, res, yard = run_pair(d, steps, node_types=nt, fluid=solid == 0, yardstick=True)
+        assert_close(res, yard=yard)
 
 
 def sheared_start(nx, ny, nz, gamma=2e-3):
