@@ -441,6 +441,90 @@ def run_serve_workload(args):
     return 0
 
 
+def moment_errors(a, b, rho0=1.0):
+    """Per-moment relative L2 / Linf of a against b (both [moment][...]),
+    each normalised by its moment group (rho - rho0 by rho, u components by
+    |u|, second moments by the second-moment group), and the relative L2
+    error of the velocity vector."""
+    groups = {0: [0], 1: [1, 2, 3], 4: [4, 5, 6, 7, 8, 9]}
+    gid = {0: 0, 1: 1, 2: 1, 3: 1, 4: 4, 5: 4, 6: 4, 7: 4, 8: 4, 9: 4}
+    norms = {}
+    for g, ks in groups.items():
+        ref = [b[k].astype(np.float64) + (rho0 if k == 0 else 0.0) for k in ks]
+        norms[g] = (np.sqrt(sum(float(np.sum(r * r)) for r in ref) / len(ks)),
+                    max(float(np.max(np.abs(r))) for r in ref))
+    out = {}
+    for k in range(10):
+        d = a[k].astype(np.float64) - b[k].astype(np.float64)
+        n2, ninf = norms[gid[k]]
+        out[k] = (float(np.sqrt(np.sum(d * d))) / n2, float(np.max(np.abs(d))) / ninf)
+    du = sum(float(np.sum((a[k].astype(np.float64) - b[k].astype(np.float64)) ** 2)) for k in (1, 2, 3))
+    uu = sum(float(np.sum(b[k].astype(np.float64) ** 2)) for k in (1, 2, 3))
+    return out, float(np.sqrt(du / uu))
+
+
+def run_precision_workload(args):
+    """Storage precision study: the Taylor-Green vortex, D3Q27, n^3 (512 by
+    default), Re 1600, u0 0.04, 1000 steps, with the moments stored as FP32,
+    FP16 and BF16 (FP32 arithmetic throughout).  Reports device-timed MLUPS of
+    each, and per-moment relative L2 / Linf errors of FP16 / BF16 against FP32
+    over the whole field; with --reference (a file written by
+    oracle/tgv_reference.py) also every storage against the FP64 oracle on the
+    z planes that file holds."""
+    import mrlbm
+
+    mrlbm.set_device(0)
+    n, steps = args.n, args.precision_steps
+    L = n / (2 * np.pi)
+    tau = 0.5 + 3.0 * U0 * L / RE
+    ref = None
+    if args.reference:
+        ref = np.load(args.reference)
+        if int(ref["n"]) != n or int(ref["steps"]) != steps:
+            raise SystemExit("reference file is for n=%d, %d steps" % (int(ref["n"]), int(ref["steps"])))
+    planes = [int(p) for p in ref["planes"]] if ref is not None else []
+    res = {}
+    full32 = None
+    for storage, name in ((mrlbm.F32, "fp32"), (mrlbm.F16, "fp16"), (mrlbm.BF16, "bf16")):
+        d = mrlbm.make_desc(n, n, n, lattice=27, storage=storage, tau=tau)
+        dom = mrlbm.Domain(d)
+        dom.init_taylor_green(U0, L)
+        # 3 warm-up steps, then the timed run restarts from the initial state
+        m0 = dom.moments()
+        dom.step(3)
+        dom.set_moments(m0)
+        del m0
+        with ClockSampler(0) as clk:
+            ms = dom.time_steps(steps)
+        m = dom.moments()
+        r = {"mlups": round(steps * n ** 3 / (ms * 1e-3) / 1e6, 1), "ms": round(ms, 2),
+             "bytes_per_lup": 2 * 10 * (4 if storage == mrlbm.F32 else 2), "clocks": clk.summary()}
+        if ref is not None:
+            o = np.moveaxis(ref["moments"].astype(np.float64), -1, 0)  # [m][planes][y][x]
+            e, ue = moment_errors(m[:, planes], o)
+            r["vs_fp64_planes"] = {"u_rel_l2": ue, "per_moment": {str(k): [v[0], v[1]] for k, v in e.items()}}
+        if storage == mrlbm.F32:
+            full32 = m
+        else:
+            e, ue = moment_errors(m, full32)
+            r["vs_fp32_full"] = {"u_rel_l2": ue, "per_moment": {str(k): [v[0], v[1]] for k, v in e.items()}}
+        s = dom.sums()
+        r["finite"] = bool(s["nonfinite"] == 0)
+        del m
+        dom.close()
+        res[name] = r
+    line = {"metric": "storage precision: MLUPS and error vs FP64 (TGV D3Q27)", "value": res["fp16"]["mlups"],
+            "unit": "MLUPS", "n_gpus": 1, "steps": steps, "higher_is_better": True,
+            "dtype": "fp16/bf16 storage, f32 arithmetic", "data": "synthetic (analytic Taylor-Green initial field)",
+            "config": {"workload": "taylor_green_%d^3_d3q27_precision" % n, "re": RE, "u0": U0, "tau": tau,
+                       "reference": ("FP64 oracle, z planes %s" % planes) if ref is not None else None},
+            "fp16_over_fp32": round(res["fp16"]["mlups"] / res["fp32"]["mlups"], 3),
+            "bf16_over_fp32": round(res["bf16"]["mlups"] / res["fp32"]["mlups"], 3),
+            "storages": res}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -449,9 +533,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
-    ap.add_argument("--workload", default="tgv", choices=["tgv", "batch", "serve"],
-                    help="tgv: the headline step benchmark (default); batch / serve: the batched-cavity and "
-                         "serving workloads (longer, run on their own)")
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "batch", "serve", "precision"],
+                    help="tgv: the headline step benchmark (default); batch / serve / precision: the "
+                         "batched-cavity, serving and storage-precision workloads (longer, run on their own)")
+    ap.add_argument("--n", type=int, default=512, help="precision workload: grid edge")
+    ap.add_argument("--precision-steps", type=int, default=1000)
+    ap.add_argument("--reference", default=None, help="precision workload: FP64 planes from oracle/tgv_reference.py")
     ap.add_argument("--domains", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=5000)
     ap.add_argument("--alone-steps", type=int, default=200)
@@ -466,6 +553,8 @@ def main():
         return run_batch_workload(args)
     if args.workload == "serve":
         return run_serve_workload(args)
+    if args.workload == "precision":
+        return run_precision_workload(args)
     return run_gpu_arm(args)
 
 

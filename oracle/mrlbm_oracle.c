@@ -87,7 +87,8 @@ typedef struct {
     size_t n;
     real *m, *m2;        /* [node][nm], node = x + nx*(y + ny*z) */
     uint32_t *type;        /* reference nodeTypeMap words, same node order */
-    real *pop;           /* [node][q] post-collision populations scratch */
+    real *pop;           /* [3][plane][q] post-collision populations of a 3-plane window */
+    int win[3];            /* z plane held by each window slot, -1 = none */
 } orc_domain;
 
 /* ----------------------------------------------------------------- per node */
@@ -313,7 +314,7 @@ void *orc_create(const orc_desc *d)
     o->m = (real *)calloc(o->n * o->nm, sizeof(real));
     o->m2 = (real *)calloc(o->n * o->nm, sizeof(real));
     o->type = (uint32_t *)calloc(o->n, sizeof(uint32_t));
-    o->pop = (real *)malloc(o->n * d->q * sizeof(real));
+    o->pop = (real *)malloc(3 * (size_t)d->nx * d->ny * d->q * sizeof(real));
     if (!o->m || !o->m2 || !o->type || !o->pop) {
         free(o->m); free(o->m2); free(o->type); free(o->pop); free(o);
         return NULL;
@@ -394,6 +395,32 @@ static inline int resolve(int v, int n, int periodic, int *outside)
     return 0;
 }
 
+/* The window slot holding the populations of plane z, or NULL. */
+static real *window_plane(orc_domain *o, int z)
+{
+    const int q = o->d.q;
+    const size_t pl = (size_t)o->d.nx * o->d.ny;
+    for (int s = 0; s < 3; s++)
+        if (o->win[s] == z) return o->pop + (size_t)s * pl * q;
+    return NULL;
+}
+
+/* Post-collision populations of plane z into a slot that is empty or holds a
+ * plane outside the current window keep[]. */
+static void window_fill(orc_domain *o, int z, const int keep[3])
+{
+    const int q = o->d.q, nm = o->nm;
+    const size_t pl = (size_t)o->d.nx * o->d.ny;
+    if (window_plane(o, z)) return;
+    int s = 0;
+    while (s < 3 && o->win[s] >= 0 && (o->win[s] == keep[0] || o->win[s] == keep[1] || o->win[s] == keep[2])) s++;
+    real *dst = o->pop + (size_t)s * pl * q;
+    const real *src = o->m + (size_t)z * pl * nm;
+#pragma omp parallel for schedule(static)
+    for (long k = 0; k < (long)pl; k++) orc_reconstruct(q, o->d.rho0, src + k * nm, dst + k * q);
+    o->win[s] = z;
+}
+
 void orc_step(void *h, int nsteps)
 {
     orc_domain *o = (orc_domain *)h;
@@ -405,11 +432,22 @@ void orc_step(void *h, int nsteps)
     for (int k = 0; k < 10; k++) ext[k] = (real)d->exterior[k];
     orc_reconstruct(q, d->rho0, ext, fext);
     for (int s = 0; s < nsteps; s++) {
-        /* post-collision populations of every node, from its stored moments */
+        /* output plane z pulls from planes z-1, z, z+1: their post-collision
+         * populations (from the stored moments) are kept in a 3-plane window,
+         * so the scratch is 3 planes, not the whole domain */
+        o->win[0] = o->win[1] = o->win[2] = -1;
+        for (int z = 0; z < nz; z++) {
+            int src[3];
+            for (int dz = -1; dz <= 1; dz++) {
+                int out = 0;
+                int sz = resolve(z + dz, nz, d->periodic[2], &out);
+                src[dz + 1] = out ? -1 : sz;
+            }
+            for (int k = 0; k < 3; k++)
+                if (src[k] >= 0) window_fill(o, src[k], src);
+            const real *wp[3];
+            for (int k = 0; k < 3; k++) wp[k] = src[k] >= 0 ? window_plane(o, src[k]) : NULL;
 #pragma omp parallel for schedule(static)
-        for (long k = 0; k < (long)o->n; k++) orc_reconstruct(q, d->rho0, o->m + k * nm, o->pop + k * q);
-#pragma omp parallel for collapse(2) schedule(static)
-        for (int z = 0; z < nz; z++)
             for (int y = 0; y < ny; y++)
                 for (int x = 0; x < nx; x++) {
                     size_t k = (size_t)x + (size_t)nx * (y + (size_t)ny * z);
@@ -422,8 +460,8 @@ void orc_step(void *h, int nsteps)
                         int out = 0;
                         int sx = resolve(x - CX[i], nx, d->periodic[0], &out);
                         int sy = resolve(y - CY[i], ny, d->periodic[1], &out);
-                        int sz = resolve(z - CZ[i], nz, d->periodic[2], &out);
-                        f[i] = out ? fext[i] : o->pop[((size_t)sx + (size_t)nx * (sy + (size_t)ny * sz)) * q + i];
+                        const real *pl = wp[1 - CZ[i]];
+                        f[i] = (out || !pl) ? fext[i] : pl[((size_t)sx + (size_t)nx * sy) * q + i];
                     }
                     real omega = (nm > 10) ? mi[10] : omega0;
                     real mac[10];
@@ -438,6 +476,7 @@ void orc_step(void *h, int nsteps)
                     }
                     collide_store(d, nm, mac, omega, mo);
                 }
+        }
         real *tmp = o->m; o->m = o->m2; o->m2 = tmp;
     }
 }
