@@ -82,6 +82,7 @@ struct BcClass {
 
 struct StepArgs {
     void* __restrict__ m_out;         // padded planes [nm][nz+2][ny+2][pitch]
+    void* out_m[11];                  // m_out + m * field: each moment's plane stack
     const uint8_t* __restrict__ cls;  // padded [nz+2][ny+2][pitch]
     const BcClass* __restrict__ bc;
     int* err;                         // bit 0: a bounded wait timed out
@@ -442,9 +443,28 @@ __host__ __device__ constexpr bool ex_group_used()
 __host__ __device__ constexpr int ex_npack(int Q) { return Q == 27 ? 6 : 2; }
 __host__ __device__ constexpr int ex_slot4(int Q, int G) { return Q == 27 ? G : (G == 1 ? 0 : 1); }
 
-// store group G of this lane's populations (its c_z = -1, 0, +1 members)
-template <int Q, int G>
-__device__ __forceinline__ void ex_write(const float* f, float4* e4, int NW, int warp, int lane)
+// Exchange buffers hold NW + 2 rows of EX_COLS slots per group; a thread's
+// own slot is row warp + 1, column lane + 1, and the slot it reads a group
+// from (row warp - c_y, lane - c_x) is a compile-time offset from it, so no
+// index arithmetic runs per access.  The halo rows and lanes read the padding
+// rows and columns (their results are never stored).
+constexpr int EX_COLS = 34;
+
+template <int Q, int NW>
+struct Exchange {
+    static constexpr int NPACK = ex_npack(Q);        // float4 groups
+    static constexpr int NSCAL = Q == 19 ? 4 : 0;    // scalar slots
+    static constexpr int plane = (NW + 2) * EX_COLS;  // slots of one group
+    static constexpr int buf4 = NPACK * plane;       // float4 per buffer
+    static constexpr int buf1 = NSCAL * plane;       // floats per buffer
+    static constexpr size_t bytes_per_buffer = (size_t)plane * (NPACK * 16 + NSCAL * 4);
+    __device__ __forceinline__ static int thread_slot(int warp, int lane) { return (warp + 1) * EX_COLS + lane + 1; }
+};
+
+// store group G of this lane's populations (its c_z = -1, 0, +1 members);
+// e4t is this thread's slot of group 0 in the buffer being written
+template <int Q, int G, int NW>
+__device__ __forceinline__ void ex_write(const float* f, float4* e4t)
 {
     if constexpr (ex_group_used<Q, G>()) {
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -456,19 +476,17 @@ __device__ __forceinline__ void ex_write(const float* f, float4* e4, int NW, int
                 else v.z = f[i];
             }
         });
-        e4[(ex_slot4(Q, G) * NW + warp) * 32 + lane] = v;
+        e4t[ex_slot4(Q, G) * Exchange<Q, NW>::plane] = v;
     }
 }
 
 // fetch group G arriving from row warp - c_y, lane - c_x
-template <int Q, int G>
-__device__ __forceinline__ void ex_read(float* g, const float4* e4, int NW, int warp, int lane)
+template <int Q, int G, int NW>
+__device__ __forceinline__ void ex_read(float* g, const float4* e4t)
 {
     if constexpr (ex_group_used<Q, G>()) {
         constexpr int cx = (G % 3) - 1, cy = G >= 3 ? 1 : -1;
-        const int w = min(max(warp - cy, 0), NW - 1);
-        const int l = (lane - cx) & 31;
-        const float4 v = e4[(ex_slot4(Q, G) * NW + w) * 32 + l];
+        const float4 v = e4t[ex_slot4(Q, G) * Exchange<Q, NW>::plane - cy * EX_COLS - cx];
         static_for<1, Q>([&](auto I) {
             constexpr int i = I;
             if constexpr (lat_cy(i) != 0 && ex_group(i) == G && ex_packed(Q, i))
@@ -477,43 +495,38 @@ __device__ __forceinline__ void ex_read(float* g, const float4* e4, int NW, int 
     }
 }
 
-template <int Q, int NW>
-struct Exchange {
-    static constexpr int NPACK = ex_npack(Q);        // float4 groups
-    static constexpr int NSCAL = Q == 19 ? 4 : 0;    // scalar slots
-    static constexpr size_t bytes_per_buffer = (size_t)NW * 32 * (NPACK * 16 + NSCAL * 4);
-};
-
 // Production of plane k (first half of a pipeline step): the plane's moments
 // come from TMA stage `stage`, its post-collision populations are
 // reconstructed, the c_y != 0 ones are written to exchange buffer k&1 and the
 // c_y = 0 ones are exchanged along x with shuffles into gsh (kept in
 // registers until the plane is consumed, one step later).
+// sp: this thread's element of moment 0 in the plane's TMA stage (moment m
+// is BOX_X elements further); e4t / e1t: this thread's exchange slots in the
+// buffer this production writes.
 template <int Q, int NM, typename T, int TYI>
-__device__ __forceinline__ void prod_a(const StepArgs& a, const T* stage, int k, float4* ex4, float* ex1, int lane,
-                                       int warp, int col, float (&gsh)[Q], float& om_node)
+__device__ __forceinline__ void prod_a(const StepArgs& a, const T* sp, float4* e4t, float* e1t, float (&gsh)[Q],
+                                       float& om_node)
 {
     constexpr int NW = TYI + 2;
     float mc[NM];
 #pragma unroll
     for (int m = 0; m < NM; m++) {
-        const float v = Stor<T>::lds(stage + (warp * NM + m) * BOX_X + col);
+        const float v = Stor<T>::lds(sp + m * BOX_X);
         mc[m] = is_f32<T>() ? v : v * a.iscale[m];
     }
     float f[Q];
     reconstruct<Q>(mc, a.rho0, f);
-    float4* e4 = ex4 + (k & 1) * (ex_npack(Q) * NW * 32);
-    float* e1 = ex1 + (k & 1) * (4 * NW * 32);
-    ex_write<Q, 0>(f, e4, NW, warp, lane);
-    ex_write<Q, 1>(f, e4, NW, warp, lane);
-    ex_write<Q, 2>(f, e4, NW, warp, lane);
-    ex_write<Q, 3>(f, e4, NW, warp, lane);
-    ex_write<Q, 4>(f, e4, NW, warp, lane);
-    ex_write<Q, 5>(f, e4, NW, warp, lane);
+    ex_write<Q, 0, NW>(f, e4t);
+    ex_write<Q, 1, NW>(f, e4t);
+    ex_write<Q, 2, NW>(f, e4t);
+    ex_write<Q, 3, NW>(f, e4t);
+    ex_write<Q, 4, NW>(f, e4t);
+    ex_write<Q, 5, NW>(f, e4t);
     if constexpr (Q == 19) {
         static_for<1, Q>([&](auto I) {
             constexpr int i = I;
-            if constexpr (lat_cy(i) != 0 && !ex_packed(Q, i)) e1[(ex_scalar_slot(i) * NW + warp) * 32 + lane] = f[i];
+            if constexpr (lat_cy(i) != 0 && !ex_packed(Q, i))
+                e1t[ex_scalar_slot(i) * Exchange<Q, NW>::plane] = f[i];
         });
     }
     static_for<0, Q>([&](auto I) {
@@ -525,6 +538,16 @@ __device__ __forceinline__ void prod_a(const StepArgs& a, const T* stage, int k,
         }
     });
     om_node = mc[NM - 1];
+}
+
+// store of the node at padded offset idx (< 2^32: a domain's moment field is
+// limited to that at creation) through the per-moment base pointers: one
+// wide multiply-add per store
+template <typename T, int NM>
+__device__ __forceinline__ void store_node32(const StepArgs& a, unsigned idx, const float* o)
+{
+#pragma unroll
+    for (int m = 0; m < NM; m++) Stor<T>::st(reinterpret_cast<T*>(a.out_m[m]) + idx, o[m]);
 }
 
 template <typename T, int NM>
@@ -543,28 +566,23 @@ __device__ __forceinline__ void store_node(const StepArgs& a, long long idx, con
 // over the warp (so it interleaves with the next production); only the BC
 // solve and the stores are predicated.
 template <int Q, int NM, int NUP, int NMID, typename T, int FLAGS, int TYI, typename BCP>
-__device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const float4* ex4, const float* ex1,
-                                       int lane, int warp, bool interior, int x, int y, const float (&gsh)[Q],
-                                       float (&up_old)[NUP], float (&mid)[NMID], float om_out)
+__device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const float4* e4t, const float* e1t,
+                                       bool interior, int x, int y, const float (&gsh)[Q], float (&up_old)[NUP],
+                                       float (&mid)[NMID], float om_out)
 {
     constexpr int NW = TYI + 2;
-    const float4* e4 = ex4 + (k & 1) * (ex_npack(Q) * NW * 32);
-    const float* e1 = ex1 + (k & 1) * (4 * NW * 32);
     float g[Q];
-    ex_read<Q, 0>(g, e4, NW, warp, lane);
-    ex_read<Q, 1>(g, e4, NW, warp, lane);
-    ex_read<Q, 2>(g, e4, NW, warp, lane);
-    ex_read<Q, 3>(g, e4, NW, warp, lane);
-    ex_read<Q, 4>(g, e4, NW, warp, lane);
-    ex_read<Q, 5>(g, e4, NW, warp, lane);
+    ex_read<Q, 0, NW>(g, e4t);
+    ex_read<Q, 1, NW>(g, e4t);
+    ex_read<Q, 2, NW>(g, e4t);
+    ex_read<Q, 3, NW>(g, e4t);
+    ex_read<Q, 4, NW>(g, e4t);
+    ex_read<Q, 5, NW>(g, e4t);
     if constexpr (Q == 19) {
         static_for<1, Q>([&](auto I) {
             constexpr int i = I;
-            if constexpr (lat_cy(i) != 0 && !ex_packed(Q, i)) {
-                const int w = min(max(warp - lat_cy(i), 0), NW - 1);
-                const int l = (lane - lat_cx(i)) & 31;
-                g[i] = e1[(ex_scalar_slot(i) * NW + w) * 32 + l];
-            }
+            if constexpr (lat_cy(i) != 0 && !ex_packed(Q, i))
+                g[i] = e1t[ex_scalar_slot(i) * Exchange<Q, NW>::plane - lat_cy(i) * EX_COLS - lat_cx(i)];
         });
     }
     static_for<0, Q>([&](auto I) {
@@ -588,7 +606,7 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
         });
         constexpr bool OMF = (FLAGS & (F_POWERLAW | F_BINGHAM)) != 0;
         const float omega = OMF ? om_out : a.omega0;
-        const long long oidx = pidx(x, y, zd, a.pitch, a.plane);
+        const unsigned oidx = (unsigned)(zd + 1) * (unsigned)a.plane + (unsigned)((y + 1) * a.pitch + x + XOFF);
         uint8_t cls = CLS_BULK;
         if constexpr ((FLAGS & F_BC) != 0) cls = live ? __ldg(a.cls + oidx) : CLS_SOLID;
         float mac[10];
@@ -615,7 +633,7 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
             for (int m = 0; m < NM; m++) o[m] = o[m] * a.scale[m];
         }
         if (live && cls != CLS_SOLID) {
-            store_node<T, NM>(a, oidx, o);
+            store_node32<T, NM>(a, oidx, o);
             // periodic axes: keep the ghost shell equal to the wrapped interior
             const bool gx = (a.periodic & 1) && (x == 0 || x == a.nx - 1);
             const bool gy = (a.periodic & 2) && (y == 0 || y == a.ny - 1);
@@ -672,54 +690,66 @@ struct ZMarch {
     static constexpr int NM = OMF ? 11 : 10;
     static constexpr size_t stage_bytes = (size_t)NW * NM * BOX_X * sizeof(T);
     static constexpr size_t stage_al = (stage_bytes + 127) / 128 * 128;
+    using EX = Exchange<Q, NW>;
 
     const StepArgs& a;
     const CUtensorMap* map;
     uint64_t* bars;
     unsigned char* stages;
-    float4* ex4;
-    float* ex1;
+    float4* e4t[2];   // this thread's exchange slots, buffer 0 and 1
+    float* e1t[2];
     unsigned g0;
-    int lane, warp, col, x, y, z0, Y0, p0, nprod;
+    int toff;         // this thread's element offset in a stage
+    int x, y, z0, Y0, p0, nprod;
     bool interior;
+    int cs;           // ring slot of the next production to wait for
+    unsigned cph;     // its mbarrier phase parity
 
     __device__ __forceinline__ int slot(int k) const { return (int)((g0 + (unsigned)k) % NSTAGE); }
     __device__ __forceinline__ unsigned phase(int k) const { return ((g0 + (unsigned)k) / NSTAGE) & 1u; }
     // ring stride: the flag-independent maximum (11 moments), see ZSmem
     static constexpr size_t ring_stride = ((size_t)NW * 11 * BOX_X * sizeof(T) + 127) / 128 * 128;
-    __device__ __forceinline__ const T* stage_of(int k) const
+    __device__ __forceinline__ const T* stage_ptr() const
     {
-        return reinterpret_cast<const T*>(stages + slot(k) * ring_stride);
+        return reinterpret_cast<const T*>(stages + cs * ring_stride) + toff;
     }
-    __device__ __forceinline__ void load(int k) const
+    __device__ __forceinline__ void load_slot(int s, int k) const
     {
-        const int s = slot(k);
         mbar_expect_tx(&bars[s], (unsigned)stage_bytes);
         tma_load_4d(stages + s * ring_stride, map, p0, 0, Y0, z0 + k, &bars[s]);
     }
-    __device__ __forceinline__ void refill(int k) const
+    __device__ __forceinline__ void load(int k) const { load_slot(slot(k), k); }
+    // after production k: reload its slot with production k + NSTAGE, then
+    // move to the next slot
+    __device__ __forceinline__ void advance(int k)
     {
         if (threadIdx.x == 0 && k + NSTAGE < nprod) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            load(k + NSTAGE);
+            load_slot(cs, k + NSTAGE);
+        }
+        if (++cs == NSTAGE) {
+            cs = 0;
+            cph ^= 1u;
         }
     }
 
-    // pipeline step j: production j and consumption j-1, one barrier.  The
+    // pipeline step j (parity PAR = j & 1): production j into exchange
+    // buffer PAR and consumption j-1 from buffer PAR ^ 1, one barrier.  The
     // node output by consumption j-1 lies in the plane of production j-2,
     // whose stored omega is in om_par (same parity as j) until production j
     // overwrites it.  Returns false when a bounded wait timed out somewhere
     // in the CTA.
+    template <int PAR>
     __device__ __forceinline__ bool iter(int j, float (&gsh_new)[Q], const float (&gsh_old)[Q], float (&up)[NUP],
-                                         float (&mid)[NMID], float& om_par) const
+                                         float (&mid)[NMID], float& om_par)
     {
-        const bool ok = mbar_wait(&bars[slot(j)], phase(j));
+        const bool ok = mbar_wait(&bars[cs], cph);
         const float om_out = om_par;
-        prod_a<Q, NM, T, TYI>(a, stage_of(j), j, ex4, ex1, lane, warp, col, gsh_new, om_par);
-        prod_b<Q, NM, NUP, NMID, T, FLAGS, TYI, BCP>(a, j - 1, z0 - 2 + j, ex4, ex1, lane, warp, interior, x, y, gsh_old,
-                                                up, mid, om_out);
+        prod_a<Q, NM, T, TYI>(a, stage_ptr(), e4t[PAR], e1t[PAR], gsh_new, om_par);
+        prod_b<Q, NM, NUP, NMID, T, FLAGS, TYI, BCP>(a, j - 1, z0 - 2 + j, e4t[PAR ^ 1], e1t[PAR ^ 1], interior, x, y,
+                                                gsh_old, up, mid, om_out);
         if (__syncthreads_or(!ok)) return false;
-        refill(j);
+        advance(j);
         return true;
     }
 };
@@ -747,7 +777,7 @@ struct ZSmem {
         bars = reinterpret_cast<uint64_t*>(smem);
         stages = smem + 128;
         ex4 = reinterpret_cast<float4*>(stages + NSTAGE * stage_max);
-        ex1 = reinterpret_cast<float*>(ex4 + 2 * ex_npack(Q) * NW * 32);
+        ex1 = reinterpret_cast<float*>(ex4 + 2 * Exchange<Q, NW>::buf4);
     }
 };
 
@@ -766,9 +796,16 @@ __device__ __forceinline__ bool zmarch_column(const StepArgs& a, const CUtensorM
     const int p0 = (X0 - 1 + XOFF) & ~(ALIGN - 1);  // aligned box start (padded column)
     // the ring stride is the flag-independent maximum; ZM's stage_al only
     // sizes the copies
-    ZM zm{a, map, sm.bars, sm.stages, sm.ex4, sm.ex1, g0, lane, warp, (x + XOFF) - p0, x, y, z0, Y0, p0,
+    const int ts = ZM::EX::thread_slot(warp, lane);
+    ZM zm{a, map, sm.bars, sm.stages,
+          {sm.ex4 + ts, sm.ex4 + ZM::EX::buf4 + ts},
+          {sm.ex1 + ts, sm.ex1 + ZM::EX::buf1 + ts},
+          g0, warp * ZM::NM * BOX_X + (x + XOFF) - p0, x, y, z0, Y0, p0,
           zend - z0 + 2 /* planes z0-1 .. zend */,
-          lane >= 1 && lane <= TILE_X && x < a.nx && warp >= 1 && warp <= TYI && y < a.ny};
+          lane >= 1 && lane <= TILE_X && x < a.nx && warp >= 1 && warp <= TYI && y < a.ny,
+          0, 0u};
+    zm.cs = zm.slot(0);
+    zm.cph = zm.phase(0);
 
     if (threadIdx.x == 0) {
         // the ring was last read through the generic proxy (previous column)
@@ -785,30 +822,31 @@ __device__ __forceinline__ bool zmarch_column(const StepArgs& a, const CUtensorM
 
     int kfail = -1;
     {
-        // prologue: production 0 only
-        const bool ok = mbar_wait(&sm.bars[zm.slot(0)], zm.phase(0));
-        prod_a<Q, ZM::NM, T, TYI>(a, zm.stage_of(0), 0, sm.ex4, sm.ex1, lane, warp, zm.col, gA, omA);
+        // prologue: production 0 only (exchange buffer 0)
+        const bool ok = mbar_wait(&sm.bars[zm.cs], zm.cph);
+        prod_a<Q, ZM::NM, T, TYI>(a, zm.stage_ptr(), zm.e4t[0], zm.e1t[0], gA, omA);
         if (__syncthreads_or(!ok)) kfail = 0;
-        else zm.refill(0);
+        else zm.advance(0);
     }
-    // even productions use gA / upA, odd ones gB / upB: no register copies
+    // even productions use gA / upA and exchange buffer 0, odd ones gB / upB
+    // and buffer 1: no register copies, no buffer selection at run time
     int j = 1;
     while (kfail < 0) {
         // epilogues consume the last production j-1; its output plane is that
         // of production j-2, whose omega has the parity of j
         if (j >= zm.nprod) {  // j odd: last production even
-            prod_b<Q, ZM::NM, NUP, NMID, T, FLAGS, TYI, BCP>(a, j - 1, z0 - 2 + j, sm.ex4, sm.ex1, lane, warp, zm.interior, x,
+            prod_b<Q, ZM::NM, NUP, NMID, T, FLAGS, TYI, BCP>(a, j - 1, z0 - 2 + j, zm.e4t[0], zm.e1t[0], zm.interior, x,
                                                         y, gA, upA, mid, omB);
             break;
         }
-        if (!zm.iter(j, gB, gA, upA, mid, omB)) { kfail = j; break; }
+        if (!zm.template iter<1>(j, gB, gA, upA, mid, omB)) { kfail = j; break; }
         j++;
         if (j >= zm.nprod) {  // j even: last production odd
-            prod_b<Q, ZM::NM, NUP, NMID, T, FLAGS, TYI, BCP>(a, j - 1, z0 - 2 + j, sm.ex4, sm.ex1, lane, warp, zm.interior, x,
+            prod_b<Q, ZM::NM, NUP, NMID, T, FLAGS, TYI, BCP>(a, j - 1, z0 - 2 + j, zm.e4t[1], zm.e1t[1], zm.interior, x,
                                                         y, gB, upB, mid, omA);
             break;
         }
-        if (!zm.iter(j, gA, gB, upB, mid, omA)) { kfail = j; break; }
+        if (!zm.template iter<0>(j, gA, gB, upB, mid, omA)) { kfail = j; break; }
         j++;
     }
     if (kfail >= 0) {

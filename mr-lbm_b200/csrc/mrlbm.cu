@@ -237,6 +237,11 @@ mrlbm_status mrlbm::domain_alloc(mrlbm_domain* dom)
     dom->pitch = (d.nx + XOFF + 1 + 7) / 8 * 8;
     dom->plane = (long long)dom->pitch * (d.ny + 2);
     dom->field = dom->plane * (d.nz + 2);
+    // the step kernel addresses a node within one moment's plane stack with
+    // 32-bit offsets
+    if (dom->field >= (1LL << 32))
+        return fail(MRLBM_EINVAL, "domain %d x %d x %d: %lld padded nodes per moment, the limit is 2^32", d.nx, d.ny,
+                    d.nz, dom->field);
     dom->omega0 = 1.0 / d.tau;
     storage_scales(d.storage, dom->scale, dom->iscale);
     const size_t mbytes = (size_t)dom->field * dom->nm * dom->esize;
@@ -514,6 +519,8 @@ void mrlbm::fill_step_args(const mrlbm_domain* dom, StepArgs& a, int parity, int
 {
     const mrlbm_desc& d = dom->d;
     a.m_out = dom->m[parity ^ 1];
+    for (int m = 0; m < 11; m++)
+        a.out_m[m] = m < dom->nm ? static_cast<char*>(dom->m[parity ^ 1]) + (size_t)m * dom->field * dom->esize : nullptr;
     a.err = dom->err;
     a.cls = dom->cls;
     a.bc = dom->bc;
