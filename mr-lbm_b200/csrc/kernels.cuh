@@ -16,7 +16,7 @@
 //   * A CTA owns a column of 30 x TYI interior nodes in (x, y) and a chunk of
 //     LZ planes in z.  Warp w holds row y = Y0 - 1 + w, lane l holds
 //     x = X0 - 1 + l: the outer lanes / warps are the one-node halo.
-//   * One elected thread streams the planes of the column into a 3-stage
+//   * One elected thread streams the planes of the column into a 4-stage
 //     shared-memory ring with cp.async.bulk.tensor (TMA) and mbarrier
 //     transaction counts; the waits are bounded and a timeout makes every
 //     thread leave together with an error flag set.
@@ -50,7 +50,7 @@ enum : int {
 constexpr int TILE_X = 30;   // interior nodes per warp row
 constexpr int XOFF = 4;      // padded column of x = 0 (x = -1 is the ghost column)
 constexpr int BOX_X = 40;    // TMA box width (elements) covering the 32 lanes
-constexpr int NSTAGE = 3;    // TMA ring depth
+constexpr int NSTAGE = 4;    // TMA ring depth (4 measured 1-3 % faster than 3)
 // interior rows per CTA (warps = rows + 2 halo rows): 16 warps at 128
 // registers fill the register file.  (18 rows at 96 registers measured
 // slower: the compiler's schedule needs the registers more than the SM needs
