@@ -194,6 +194,10 @@ mrlbm_status mrlbm_save_checkpoint(mrlbm_domain* dom, const char* path_files, co
 mrlbm_status mrlbm_load_checkpoint(mrlbm_domain* dom, const char* path_files, const char* id_sim, int* step);
 /* <path>/<id>/<id>_{rho,ux,uy,uz[,omega]}NNNNNN.bin (src/saveData.cu:62-260, 439-467). */
 mrlbm_status mrlbm_save_macr_bin(mrlbm_domain* dom, const char* path_files, const char* id_sim, int step);
+/* Legacy VTK structured points, binary big-endian, as saveVarVTK writes it
+ * (src/saveData.cu:303-400): rho, velocity (physical u), omega when present;
+ * <path>/<id>/<id>_vtk<step>.vtk (src/saveData.cu:153). */
+mrlbm_status mrlbm_save_vtk(mrlbm_domain* dom, const char* path_files, const char* id_sim, int step);
 /* <path>/<id>/<id>_info.txt (src/saveData.cu:469-613); case_name = BC type. */
 mrlbm_status mrlbm_save_info(mrlbm_domain* dom, const char* path_files, const char* id_sim,
                              const char* case_name, int nsteps, double mlups);

@@ -203,6 +203,62 @@ extern "C" mrlbm_status mrlbm_save_macr_bin(mrlbm_domain* dom, const char* path_
     return MRLBM_OK;
 }
 
+// Legacy VTK structured-points file, binary (big-endian floats), as
+// saveVarVTK writes it (src/saveData.cu:303-400): SCALARS rho (rho0 + m0),
+// VECTORS velocity (physical u, the stored 3u divided by 3), and SCALARS omega
+// when the domain carries an omega field.  File <path>/<id>/<id>_vtk<step>.vtk
+// (src/saveData.cu:153).  The reference's optional node-type and BC-force
+// sections (NODE_TYPE_SAVE, SAVE_BC_FORCES) are not written.
+static void put_be(std::string& out, const float* v, size_t n)
+{
+    const size_t at = out.size();
+    out.resize(at + 4 * n);
+    for (size_t i = 0; i < n; i++) {
+        uint32_t w;
+        memcpy(&w, &v[i], 4);
+        w = __builtin_bswap32(w);
+        memcpy(&out[at + 4 * i], &w, 4);
+    }
+}
+
+extern "C" mrlbm_status mrlbm_save_vtk(mrlbm_domain* dom, const char* path_files, const char* id_sim, int step)
+{
+    if (!dom || !path_files || !id_sim) return fail(MRLBM_EINVAL, "null argument");
+    const mrlbm_desc& d = dom->d;
+    const size_t n = (size_t)d.nx * d.ny * d.nz;
+    mrlbm_status st = mkdirs(std::string(path_files) + "/" + id_sim);
+    if (st) return st;
+    std::vector<float> rho(n), ux(n), uy(n), uz(n), om;
+    if (dom->nm > 10) om.resize(n);
+    if ((st = mrlbm_get_macr(dom, rho.data(), ux.data(), uy.data(), uz.data(), dom->nm > 10 ? om.data() : nullptr)))
+        return st;
+    std::string out;
+    out.reserve(n * 16 + 512);
+    char head[512];
+    snprintf(head, sizeof(head),
+             "# vtk DataFile Version 3.0\nLBM output (binary)\nBINARY\nDATASET STRUCTURED_POINTS\n"
+             "DIMENSIONS %d %d %d\nORIGIN 0 0 0\nSPACING 1 1 1\nPOINT_DATA %zu\n",
+             d.nx, d.ny, d.nz, n);
+    out += head;
+    out += "SCALARS rho float 1\nLOOKUP_TABLE default\n";
+    put_be(out, rho.data(), n);
+    out += "VECTORS velocity float\n";
+    {
+        std::vector<float> v(3 * n);
+        for (size_t i = 0; i < n; i++) {
+            v[3 * i] = ux[i] / 3.0f;
+            v[3 * i + 1] = uy[i] / 3.0f;
+            v[3 * i + 2] = uz[i] / 3.0f;
+        }
+        put_be(out, v.data(), 3 * n);
+    }
+    if (dom->nm > 10) {
+        out += "SCALARS omega float 1\nLOOKUP_TABLE default\n";
+        put_be(out, om.data(), n);
+    }
+    return write_file(var_filename(path_files, id_sim, "vtk", (unsigned)step, ".vtk"), out.data(), out.size());
+}
+
 // Same keys and number formatting as getSimInfoString (src/saveData.cu:469-613),
 // which the reference's reader parses (post/fileTreat.py:61-150).
 extern "C" mrlbm_status mrlbm_save_info(mrlbm_domain* dom, const char* path_files, const char* id_sim,

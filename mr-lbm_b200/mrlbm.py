@@ -128,6 +128,7 @@ def lib():
             "mrlbm_save_checkpoint": [VP, C.c_char_p, C.c_char_p, C.c_int],
             "mrlbm_load_checkpoint": [VP, C.c_char_p, C.c_char_p, C.POINTER(C.c_int)],
             "mrlbm_save_macr_bin": [VP, C.c_char_p, C.c_char_p, C.c_int],
+            "mrlbm_save_vtk": [VP, C.c_char_p, C.c_char_p, C.c_int],
             "mrlbm_save_info": [VP, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, C.c_double],
             "mrlbm_voxel_node_types": [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint8), C.POINTER(C.c_int),
                                        C.POINTER(C.c_uint32)],
@@ -345,6 +346,9 @@ class Domain:
 
     def save_macr_bin(self, path, sim_id, step):
         check(self.L.mrlbm_save_macr_bin(self.h, path.encode(), sim_id.encode(), int(step)))
+
+    def save_vtk(self, path, sim_id, step):
+        check(self.L.mrlbm_save_vtk(self.h, path.encode(), sim_id.encode(), int(step)))
 
     def save_info(self, path, sim_id, case_name, nsteps, mlups):
         check(self.L.mrlbm_save_info(self.h, path.encode(), sim_id.encode(), case_name.encode(), int(nsteps),

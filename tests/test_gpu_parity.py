@@ -241,3 +241,49 @@ def test_kinetic_energy_decay_matches_oracle():
         dom.step(25)
         orc.step(25)
         np.testing.assert_allclose(dom.sums()["kinetic_energy"], orc.sums()[4], rtol=1e-5)
+
+
+def read_vtk(path):
+    """Legacy binary VTK structured points: header lines, then big-endian
+    float sections (the reference's saveVarVTK layout)."""
+    raw = open(path, "rb").read()
+    out, pos, n = {}, 0, None
+    header = {}
+    while pos < len(raw):
+        end = raw.index(b"\n", pos)
+        line = raw[pos:end].decode()
+        pos = end + 1
+        parts = line.split()
+        if not parts:
+            continue
+        if parts[0] in ("DIMENSIONS", "ORIGIN", "SPACING", "DATASET"):
+            header[parts[0]] = parts[1:]
+        elif parts[0] == "POINT_DATA":
+            n = int(parts[1])
+        elif parts[0] == "SCALARS":
+            end = raw.index(b"\n", pos)  # LOOKUP_TABLE default
+            pos = end + 1
+            out[parts[1]] = np.frombuffer(raw, dtype=">f4", count=n, offset=pos)
+            pos += 4 * n
+        elif parts[0] == "VECTORS":
+            out[parts[1]] = np.frombuffer(raw, dtype=">f4", count=3 * n, offset=pos).reshape(n, 3)
+            pos += 12 * n
+    return header, out
+
+
+def test_vtk_writer(tmp_path):
+    nx, ny, nz = 24, 16, 8
+    d = mrlbm.make_desc(nx, ny, nz, lattice=19, tau=0.7, rheology=mrlbm.BINGHAM, nnf_yield=1e-6,
+                        periodic=(1, 0, 1), force=(1e-5, 0, 0))
+    dom = mrlbm.Domain(d)
+    dom.set_node_types(mrlbm.voxel_node_types(np.zeros((nz, ny, nx), np.uint8), (1, 0, 1)))
+    dom.init_uniform()
+    dom.step(20)
+    dom.save_vtk(str(tmp_path), "000", 20)
+    m = dom.moments()
+    dom.close()
+    header, f = read_vtk(tmp_path / "000" / "000_vtk000020.vtk")
+    assert header["DIMENSIONS"] == [str(nx), str(ny), str(nz)] and header["DATASET"] == ["STRUCTURED_POINTS"]
+    np.testing.assert_array_equal(f["rho"], (np.float32(1.0) + m[0]).reshape(-1))
+    np.testing.assert_allclose(f["velocity"], (m[1:4] / np.float32(3.0)).reshape(3, -1).T, rtol=1e-6)
+    np.testing.assert_array_equal(f["omega"], m[10].reshape(-1))
