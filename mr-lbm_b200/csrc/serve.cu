@@ -271,8 +271,19 @@ extern "C" mrlbm_status mrlbm_server_tick(mrlbm_server* s, int* active_out)
             continue;
         }
     }
-    if (!s->active.empty()) {
+    if (s->active.size() == 1) {
+        // a lone solve runs on the single-domain step kernel: same arithmetic
+        // (bit-identical results), no work queue, a grid sized for its grid
+        mrlbm_domain* dom = nullptr;
+        if ((st = mrlbm_batch_domain(s->batch, s->reqs[s->active[0]].member, &dom))) return st;
+        // the single-domain grid's own z chunking (the batch sets its own
+        // chunk again before its next step)
+        dom->lz = mrlbm::choose_lz(dom);
+        if ((st = mrlbm_step(dom, s->steps_per_tick))) return st;
+    } else if (!s->active.empty()) {
         if ((st = mrlbm_batch_step(s->batch, s->steps_per_tick))) return st;
+    }
+    if (!s->active.empty()) {
         for (int rid : s->active) {
             Request& q = s->reqs[rid];
             q.steps += s->steps_per_tick;
