@@ -80,8 +80,8 @@ __global__ void init_kernel(const InitArgs a)
         T* p1 = reinterpret_cast<T*>(a.m1);
         for (int k = 0; k < a.nm; k++) {
             const float v = is_f32<T>() ? m[k] : m[k] * a.scale[k];
-            Stor<T>::st(p0 + k * a.field + idx, v);
-            Stor<T>::st(p1 + k * a.field + idx, v);
+            Stor<T>::st(p0 + mphys(k, idx, a.field), v);
+            Stor<T>::st(p1 + mphys(k, idx, a.field), v);
         }
     }
 }
@@ -111,7 +111,7 @@ __global__ void convert_kernel(const ConvArgs a)
         const int x = (int)(node % a.nx);
         const int y = (int)((node / a.nx) % a.ny);
         const int z = (int)(node / ((long long)a.nx * a.ny));
-        const long long idx = k * a.field + pidx(x, y, z, a.pitch, a.plane);
+        const long long idx = mphys(k, pidx(x, y, z, a.pitch, a.plane), a.field);
         long long fi;
         if (a.mode < 2) {
             fi = g;
@@ -167,14 +167,14 @@ __global__ void ghost_fill_kernel(const GhostArgs a)
         if (wall) {
             for (int k = 0; k < a.nm; k++) {
                 const float v = is_f32<T>() ? a.ext[k] : a.ext[k] * a.scale[k];
-                Stor<T>::st(p0 + k * a.field + di, v);
-                Stor<T>::st(p1 + k * a.field + di, v);
+                Stor<T>::st(p0 + mphys(k, di, a.field), v);
+                Stor<T>::st(p1 + mphys(k, di, a.field), v);
             }
         } else {
             const long long si = pidx(sx, sy, sz, a.pitch, a.plane);
             for (int k = 0; k < a.nm; k++) {
-                p0[k * a.field + di] = p0[k * a.field + si];
-                p1[k * a.field + di] = p0[k * a.field + si];
+                p0[mphys(k, di, a.field)] = p0[mphys(k, si, a.field)];
+                p1[mphys(k, di, a.field)] = p0[mphys(k, si, a.field)];
             }
         }
     }
@@ -220,7 +220,7 @@ __global__ void __launch_bounds__(RED_THREADS) reduce_kernel(const RedArgs a)
         float v[4];
         bool finite = true;
         for (int k = 0; k < 4; k++) {
-            const float s = Stor<T>::ld(mp + k * a.field + idx);
+            const float s = Stor<T>::ld(mp + mphys(k, idx, a.field));
             v[k] = is_f32<T>() ? s : s * a.iscale[k];
             finite = finite && isfinite(v[k]);
         }

@@ -45,7 +45,7 @@ namespace {
 template <int Q, typename T>
 mrlbm_status set_attr(size_t& smem)
 {
-    smem = ZSmem<Q, T, batch_tyi(Q)>::bytes;
+    smem = ZSmem<Q, T, batch_tyi(Q), 6>::bytes;
     cudaError_t e = cudaFuncSetAttribute(batch_step<Q, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return fail(MRLBM_ECUDA, "batch attribute: %s", cudaGetErrorString(e));
     return MRLBM_OK;

@@ -38,7 +38,7 @@ struct BatchCtl {
 
 template <int Q, typename T, int FLAGS>
 __device__ __forceinline__ bool batch_column(const StepArgs& a, const CUtensorMap* map, const BatchItem& it,
-                                             const ZSmem<Q, T, batch_tyi(Q)>& sm, unsigned& g0)
+                                             const ZSmem<Q, T, batch_tyi(Q), 6>& sm, unsigned& g0)
 {
     return zmarch_column<Q, T, FLAGS, batch_tyi(Q)>(a, map, it.X0, it.Y0, it.z0, min(it.z0 + a.lz, a.nz), sm, g0);
 }
@@ -50,8 +50,8 @@ __global__ void __launch_bounds__(32 * (batch_tyi(Q) + 2), 1)
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ int s_item;
     __shared__ __align__(16) StepArgs s_args;
-    const ZSmem<Q, T, batch_tyi(Q)> sm(smem);
-    zmarch_init_barriers<Q, T, batch_tyi(Q)>(sm);
+    const ZSmem<Q, T, batch_tyi(Q), 6> sm(smem);  // ring slots for the largest flag set
+    zmarch_init_barriers(sm);
     const int step = *((volatile int*)&ctl->step);
     const int nitems = *((volatile int*)&ctl->nitems);
     unsigned g0 = 0;

@@ -14,12 +14,14 @@ constexpr int GRAPH_STEPS = 16;  // launches per captured graph (even: parities 
 
 }  // namespace mrlbm
 
-// HBM layout: each of the nm moments is a plane stack [z+1][y+1][x+XOFF]
-// with a one-node ghost shell (z = -1..nz, y = -1..ny, x = -1..nx; pitch =
-// nx + XOFF + 1 rounded up to 8 elements, so rows are 16-byte aligned for
-// TMA), stored in the domain's storage type, twice (ping-pong: step n reads
+// HBM layout: the nm moments are stored in pairs (moments 2p, 2p + 1); each
+// pair is a plane stack [z+1][y+1][x+XOFF][2] with a one-node ghost shell
+// (z = -1..nz, y = -1..ny, x = -1..nx; pitch = nx + XOFF + 1 rounded up to 8
+// nodes, so rows are 16-byte aligned for TMA), in the domain's storage type;
+// an odd moment count is padded to a full pair (mphys() gives the element of
+// moment m at node offset pidx()).  Two such buffers ping-pong (step n reads
 // m[cur] and writes m[cur^1]).  Node classes are one byte per node in the
-// same padded layout.
+// padded node layout.
 struct mrlbm_domain {
     mrlbm_desc d{};
     int q = 19, nm = 10;

@@ -8,8 +8,11 @@
 // them in moment space.  Only the 10 (11) moments live in HBM.
 //
 // B200 design (z-marching, ping-pong moments, TMA-fed):
-//   * Moments are stored per moment as padded plane stacks with a one-node
-//     ghost shell (x = -1..nx, y = -1..ny, z = -1..nz).  Periodic axes keep
+//   * Moments are stored in pairs (moments 2p and 2p + 1 side by side per
+//     node, so a node's pair is one 8-byte word in FP32) as padded plane
+//     stacks with a one-node ghost shell (x = -1..nx, y = -1..ny,
+//     z = -1..nz): half the load and store instructions of one plane stack
+//     per moment.  Periodic axes keep
 //     the shell equal to the wrapped interior: the kernel writes the extra
 //     copies of boundary nodes.  Wall axes keep the shell at the exterior rest
 //     state.  So every halo read is an in-bounds tile read with no wrap logic.
@@ -50,7 +53,9 @@ enum : int {
 constexpr int TILE_X = 30;   // interior nodes per warp row
 constexpr int XOFF = 4;      // padded column of x = 0 (x = -1 is the ghost column)
 constexpr int BOX_X = 40;    // TMA box width (elements) covering the 32 lanes
-constexpr int NSTAGE = 4;    // TMA ring depth (4 measured 1-3 % faster than 3)
+// TMA ring depth: 4 stages where the ring and the row exchange fit in shared
+// memory (4 measured 1-3 % faster than 3), else 3
+constexpr int NSTAGE_MAX = 4;
 // interior rows per CTA (warps = rows + 2 halo rows): 16 warps at 128
 // registers fill the register file.  (18 rows at 96 registers measured
 // slower: the compiler's schedule needs the registers more than the SM needs
@@ -82,7 +87,7 @@ struct BcClass {
 
 struct StepArgs {
     void* __restrict__ m_out;         // padded planes [nm][nz+2][ny+2][pitch]
-    void* out_m[11];                  // m_out + m * field: each moment's plane stack
+    void* out_p[6];                   // plane stack of moment pair p (moments 2p, 2p+1)
     const uint8_t* __restrict__ cls;  // padded [nz+2][ny+2][pitch]
     const BcClass* __restrict__ bc;
     int* err;                         // bit 0: a bounded wait timed out
@@ -101,6 +106,13 @@ struct StepArgs {
 __host__ __device__ __forceinline__ long long pidx(int x, int y, int z, int pitch, long long plane)
 {
     return (long long)(z + 1) * plane + (long long)(y + 1) * pitch + (x + XOFF);
+}
+
+// Element of moment m at padded node offset idx (pidx): moment pairs are
+// stacked 2 * field elements apart, the pair's two moments side by side.
+__host__ __device__ __forceinline__ long long mphys(int m, long long idx, long long field)
+{
+    return (long long)(m >> 1) * 2 * field + 2 * idx + (m & 1);
 }
 
 // ------------------------------------------------------------------ storage
@@ -131,6 +143,37 @@ constexpr bool is_f32()
 {
     return sizeof(T) == 4;
 }
+
+// a moment pair of one node: 8 bytes (FP32) or 4 bytes (FP16 / BF16)
+template <typename T>
+struct Stor2;
+template <>
+struct Stor2<float> {
+    static __device__ __forceinline__ float2 lds(const float* p) { return *reinterpret_cast<const float2*>(p); }
+    static __device__ __forceinline__ void st(float* p, float a, float b) { *reinterpret_cast<float2*>(p) = make_float2(a, b); }
+};
+template <>
+struct Stor2<__half> {
+    static __device__ __forceinline__ float2 lds(const __half* p)
+    {
+        return __half22float2(*reinterpret_cast<const __half2*>(p));
+    }
+    static __device__ __forceinline__ void st(__half* p, float a, float b)
+    {
+        *reinterpret_cast<__half2*>(p) = __floats2half2_rn(a, b);
+    }
+};
+template <>
+struct Stor2<__nv_bfloat16> {
+    static __device__ __forceinline__ float2 lds(const __nv_bfloat16* p)
+    {
+        return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
+    }
+    static __device__ __forceinline__ void st(__nv_bfloat16* p, float a, float b)
+    {
+        *reinterpret_cast<__nv_bfloat162*>(p) = __floats2bfloat162_rn(a, b);
+    }
+};
 
 // ------------------------------------------------------------ per-node math
 
@@ -500,9 +543,9 @@ __device__ __forceinline__ void ex_read(float* g, const float4* e4t)
 // reconstructed, the c_y != 0 ones are written to exchange buffer k&1 and the
 // c_y = 0 ones are exchanged along x with shuffles into gsh (kept in
 // registers until the plane is consumed, one step later).
-// sp: this thread's element of moment 0 in the plane's TMA stage (moment m
-// is BOX_X elements further); e4t / e1t: this thread's exchange slots in the
-// buffer this production writes.
+// sp: this thread's element pair of moments 0, 1 in the plane's TMA stage
+// (pair p is 2 BOX_X elements further); e4t / e1t: this thread's exchange
+// slots in the buffer this production writes.
 template <int Q, int NM, typename T, int TYI>
 __device__ __forceinline__ void prod_a(const StepArgs& a, const T* sp, float4* e4t, float* e1t, float (&gsh)[Q],
                                        float& om_node)
@@ -510,9 +553,10 @@ __device__ __forceinline__ void prod_a(const StepArgs& a, const T* sp, float4* e
     constexpr int NW = TYI + 2;
     float mc[NM];
 #pragma unroll
-    for (int m = 0; m < NM; m++) {
-        const float v = Stor<T>::lds(sp + m * BOX_X);
-        mc[m] = is_f32<T>() ? v : v * a.iscale[m];
+    for (int p = 0; p < (NM + 1) / 2; p++) {
+        const float2 v = Stor2<T>::lds(sp + p * 2 * BOX_X);
+        mc[2 * p] = is_f32<T>() ? v.x : v.x * a.iscale[2 * p];
+        if (2 * p + 1 < NM) mc[2 * p + 1] = is_f32<T>() ? v.y : v.y * a.iscale[2 * p + 1];
     }
     float f[Q];
     reconstruct<Q>(mc, a.rho0, f);
@@ -541,13 +585,14 @@ __device__ __forceinline__ void prod_a(const StepArgs& a, const T* sp, float4* e
 }
 
 // store of the node at padded offset idx (< 2^32: a domain's moment field is
-// limited to that at creation) through the per-moment base pointers: one
-// wide multiply-add per store
+// limited to that at creation) through the per-pair base pointers: one
+// 8-byte (FP32) or 4-byte (16-bit) store per moment pair
 template <typename T, int NM>
 __device__ __forceinline__ void store_node32(const StepArgs& a, unsigned idx, const float* o)
 {
 #pragma unroll
-    for (int m = 0; m < NM; m++) Stor<T>::st(reinterpret_cast<T*>(a.out_m[m]) + idx, o[m]);
+    for (int p = 0; p < NM / 2; p++) Stor2<T>::st(reinterpret_cast<T*>(a.out_p[p]) + 2 * (size_t)idx, o[2 * p], o[2 * p + 1]);
+    if constexpr (NM % 2 != 0) Stor<T>::st(reinterpret_cast<T*>(a.out_p[NM / 2]) + 2 * (size_t)idx, o[NM - 1]);
 }
 
 template <typename T, int NM>
@@ -555,7 +600,7 @@ __device__ __forceinline__ void store_node(const StepArgs& a, long long idx, con
 {
     T* outp = reinterpret_cast<T*>(a.m_out);
 #pragma unroll
-    for (int m = 0; m < NM; m++) Stor<T>::st(outp + m * a.field + idx, o[m]);
+    for (int m = 0; m < NM; m++) Stor<T>::st(outp + mphys(m, idx, a.field), o[m]);
 }
 
 // Consumption of plane k (second half): the c_y != 0 populations arriving from
@@ -678,19 +723,51 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
     });
 }
 
+// Shared-memory carve-up used by every z-march kernel: barriers, TMA ring,
+// double-buffered exchange.  Ring slots hold NPM moment pairs (kernels that
+// switch between flag sets at run time size them for the largest set), and
+// the ring has NSTAGE_MAX stages when they fit next to the exchange buffers,
+// else one fewer.
+template <int Q, typename T, int TYI, int NPM>
+struct ZSmem {
+    static constexpr int NW = TYI + 2;
+    static constexpr size_t stage_max = ((size_t)NW * NPM * 2 * BOX_X * sizeof(T) + 127) / 128 * 128;
+    static constexpr size_t ex_bytes = 2 * Exchange<Q, NW>::bytes_per_buffer;
+    static constexpr int NS = 128 + NSTAGE_MAX * stage_max + ex_bytes <= 232448 ? NSTAGE_MAX : NSTAGE_MAX - 1;
+    static constexpr size_t bytes = 128 + NS * stage_max + ex_bytes;
+    uint64_t* bars;
+    unsigned char* stages;
+    float4* ex4;
+    float* ex1;
+    __device__ __forceinline__ explicit ZSmem(unsigned char* smem)
+    {
+        bars = reinterpret_cast<uint64_t*>(smem);
+        stages = smem + 128;
+        ex4 = reinterpret_cast<float4*>(stages + NS * stage_max);
+        ex1 = reinterpret_cast<float*>(ex4 + 2 * Exchange<Q, NW>::buf4);
+    }
+};
+
+// moment pairs of a flag set
+__host__ __device__ constexpr int npairs_of(int flags) { return (flags & (F_POWERLAW | F_BINGHAM)) ? 6 : 5; }
+
 // Per-CTA pipeline state and the loop of the z-march over one column.  The
 // TMA ring is indexed by a running production count `g0 + k` so a persistent
 // CTA can chain columns without re-initialising its mbarriers.
-template <int Q, typename T, int FLAGS, int TYI, typename BCP>
+template <int Q, typename T, int FLAGS, int TYI, typename BCP, int NPM>
 struct ZMarch {
     static constexpr int NW = TYI + 2;
     static constexpr int NUP = lat_num_cz(Q, 1);
     static constexpr int NMID = lat_num_cz(Q, 0);
     static constexpr bool OMF = (FLAGS & (F_POWERLAW | F_BINGHAM)) != 0;
     static constexpr int NM = OMF ? 11 : 10;
-    static constexpr size_t stage_bytes = (size_t)NW * NM * BOX_X * sizeof(T);
+    static constexpr int NP = (NM + 1) / 2;  // moment pairs in a stage row
+    static constexpr size_t stage_bytes = (size_t)NW * NP * 2 * BOX_X * sizeof(T);
     static constexpr size_t stage_al = (stage_bytes + 127) / 128 * 128;
     using EX = Exchange<Q, NW>;
+    using SM = ZSmem<Q, T, TYI, NPM>;
+    static constexpr int NS = SM::NS;
+    static_assert(NP <= NPM, "ring slots sized for fewer moment pairs");
 
     const StepArgs& a;
     const CUtensorMap* map;
@@ -705,10 +782,9 @@ struct ZMarch {
     int cs;           // ring slot of the next production to wait for
     unsigned cph;     // its mbarrier phase parity
 
-    __device__ __forceinline__ int slot(int k) const { return (int)((g0 + (unsigned)k) % NSTAGE); }
-    __device__ __forceinline__ unsigned phase(int k) const { return ((g0 + (unsigned)k) / NSTAGE) & 1u; }
-    // ring stride: the flag-independent maximum (11 moments), see ZSmem
-    static constexpr size_t ring_stride = ((size_t)NW * 11 * BOX_X * sizeof(T) + 127) / 128 * 128;
+    __device__ __forceinline__ int slot(int k) const { return (int)((g0 + (unsigned)k) % NS); }
+    __device__ __forceinline__ unsigned phase(int k) const { return ((g0 + (unsigned)k) / NS) & 1u; }
+    static constexpr size_t ring_stride = SM::stage_max;
     __device__ __forceinline__ const T* stage_ptr() const
     {
         return reinterpret_cast<const T*>(stages + cs * ring_stride) + toff;
@@ -716,18 +792,19 @@ struct ZMarch {
     __device__ __forceinline__ void load_slot(int s, int k) const
     {
         mbar_expect_tx(&bars[s], (unsigned)stage_bytes);
-        tma_load_4d(stages + s * ring_stride, map, p0, 0, Y0, z0 + k, &bars[s]);
+        // x runs over the interleaved pair elements: 2 per node
+        tma_load_4d(stages + s * ring_stride, map, 2 * p0, 0, Y0, z0 + k, &bars[s]);
     }
     __device__ __forceinline__ void load(int k) const { load_slot(slot(k), k); }
-    // after production k: reload its slot with production k + NSTAGE, then
-    // move to the next slot
+    // after production k: reload its slot with production k + NS, then move
+    // to the next slot
     __device__ __forceinline__ void advance(int k)
     {
-        if (threadIdx.x == 0 && k + NSTAGE < nprod) {
+        if (threadIdx.x == 0 && k + NS < nprod) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            load_slot(cs, k + NSTAGE);
+            load_slot(cs, k + NS);
         }
-        if (++cs == NSTAGE) {
+        if (++cs == NS) {
             cs = 0;
             cph ^= 1u;
         }
@@ -754,53 +831,26 @@ struct ZMarch {
     }
 };
 
-template <int Q, typename T, int FLAGS, int TYI>
-constexpr size_t zmarch_stage_al()
-{
-    return ZMarch<Q, T, FLAGS, TYI, TableBC>::stage_al;
-}
-
-// Shared-memory carve-up used by every z-march kernel: barriers, TMA ring,
-// double-buffered exchange.  The ring is sized for 11 moments so kernels that
-// switch between flag sets at run time share one layout.
-template <int Q, typename T, int TYI>
-struct ZSmem {
-    static constexpr int NW = TYI + 2;
-    static constexpr size_t stage_max = ((size_t)NW * 11 * BOX_X * sizeof(T) + 127) / 128 * 128;
-    static constexpr size_t bytes = 128 + NSTAGE * stage_max + 2 * Exchange<Q, NW>::bytes_per_buffer;
-    uint64_t* bars;
-    unsigned char* stages;
-    float4* ex4;
-    float* ex1;
-    __device__ __forceinline__ explicit ZSmem(unsigned char* smem)
-    {
-        bars = reinterpret_cast<uint64_t*>(smem);
-        stages = smem + 128;
-        ex4 = reinterpret_cast<float4*>(stages + NSTAGE * stage_max);
-        ex1 = reinterpret_cast<float*>(ex4 + 2 * Exchange<Q, NW>::buf4);
-    }
-};
-
 // One column (X0, Y0) x planes [z0, zend) of one domain.  g0 is the CTA's
 // running production count (advanced by the column's productions).  Returns
 // false when a bounded wait timed out (the CTA must stop).
-template <int Q, typename T, int FLAGS, int TYI, typename BCP = TableBC>
+template <int Q, typename T, int FLAGS, int TYI, typename BCP = TableBC, int NPM>
 __device__ __forceinline__ bool zmarch_column(const StepArgs& a, const CUtensorMap* map, int X0, int Y0, int z0,
-                                              int zend, const ZSmem<Q, T, TYI>& sm, unsigned& g0)
+                                              int zend, const ZSmem<Q, T, TYI, NPM>& sm, unsigned& g0)
 {
-    using ZM = ZMarch<Q, T, FLAGS, TYI, BCP>;
+    using ZM = ZMarch<Q, T, FLAGS, TYI, BCP, NPM>;
     constexpr int NUP = ZM::NUP, NMID = ZM::NMID;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int x = X0 - 1 + lane, y = Y0 - 1 + warp;
     constexpr int ALIGN = 16 / (int)sizeof(T);      // elements per 16 bytes (TMA x alignment)
     const int p0 = (X0 - 1 + XOFF) & ~(ALIGN - 1);  // aligned box start (padded column)
-    // the ring stride is the flag-independent maximum; ZM's stage_al only
-    // sizes the copies
+    // stage rows are [row][pair][2 * BOX_X]: this thread's pair of moments
+    // 0, 1 is at element 2 * col of its row
     const int ts = ZM::EX::thread_slot(warp, lane);
     ZM zm{a, map, sm.bars, sm.stages,
           {sm.ex4 + ts, sm.ex4 + ZM::EX::buf4 + ts},
           {sm.ex1 + ts, sm.ex1 + ZM::EX::buf1 + ts},
-          g0, warp * ZM::NM * BOX_X + (x + XOFF) - p0, x, y, z0, Y0, p0,
+          g0, warp * ZM::NP * 2 * BOX_X + 2 * ((x + XOFF) - p0), x, y, z0, Y0, p0,
           zend - z0 + 2 /* planes z0-1 .. zend */,
           lane >= 1 && lane <= TILE_X && x < a.nx && warp >= 1 && warp <= TYI && y < a.ny,
           0, 0u};
@@ -810,7 +860,7 @@ __device__ __forceinline__ bool zmarch_column(const StepArgs& a, const CUtensorM
     if (threadIdx.x == 0) {
         // the ring was last read through the generic proxy (previous column)
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        for (int s = 0; s < NSTAGE && s < zm.nprod; s++) zm.load(s);
+        for (int s = 0; s < ZM::NS && s < zm.nprod; s++) zm.load(s);
     }
 
     float upA[NUP], upB[NUP], mid[NMID], gA[Q], gB[Q];
@@ -854,7 +904,7 @@ __device__ __forceinline__ bool zmarch_column(const StepArgs& a, const CUtensorM
         // bounded time to land, and leave together
         if (threadIdx.x == 0) {
             atomicOr(a.err, 1);
-            for (int q = kfail; q < zm.nprod && q < kfail + NSTAGE; q++) (void)mbar_wait(&sm.bars[zm.slot(q)], zm.phase(q));
+            for (int q = kfail; q < zm.nprod && q < kfail + ZM::NS; q++) (void)mbar_wait(&sm.bars[zm.slot(q)], zm.phase(q));
         }
         __syncthreads();
         return false;
@@ -865,11 +915,11 @@ __device__ __forceinline__ bool zmarch_column(const StepArgs& a, const CUtensorM
     return true;
 }
 
-template <int Q, typename T, int TYI>
-__device__ __forceinline__ void zmarch_init_barriers(const ZSmem<Q, T, TYI>& sm)
+template <int Q, typename T, int TYI, int NPM>
+__device__ __forceinline__ void zmarch_init_barriers(const ZSmem<Q, T, TYI, NPM>& sm)
 {
     if (threadIdx.x == 0) {
-        for (int s = 0; s < NSTAGE; s++) mbar_init(&sm.bars[s], 1);
+        for (int s = 0; s < ZSmem<Q, T, TYI, NPM>::NS; s++) mbar_init(&sm.bars[s], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -883,8 +933,8 @@ __global__ void __launch_bounds__(32 * (TYI + 2), 1)
     zmarch_step(const __grid_constant__ CUtensorMap map_in, const StepArgs a)
 {
     extern __shared__ __align__(128) unsigned char smem[];
-    const ZSmem<Q, T, TYI> sm(smem);
-    zmarch_init_barriers<Q, T, TYI>(sm);
+    const ZSmem<Q, T, TYI, npairs_of(FLAGS)> sm(smem);
+    zmarch_init_barriers(sm);
     unsigned g0 = 0;
     const int z0 = blockIdx.z * a.lz;
     (void)zmarch_column<Q, T, FLAGS, TYI, BCP>(a, &map_in, blockIdx.x * TILE_X, blockIdx.y * TYI, z0,
@@ -900,7 +950,7 @@ __host__ __device__ inline dim3 zmarch_grid(int nx, int ny, int nz, int tyi, int
 template <int Q, typename T, int FLAGS, int TYI>
 constexpr size_t step_smem_bytes()
 {
-    return ZSmem<Q, T, TYI>::bytes;
+    return ZSmem<Q, T, TYI, npairs_of(FLAGS)>::bytes;
 }
 
 }  // namespace mrlbm

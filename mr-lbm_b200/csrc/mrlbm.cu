@@ -224,7 +224,8 @@ extern "C" mrlbm_status mrlbm_domain_bytes(const mrlbm_desc* d, size_t* bytes)
     if (st) return st;
     const size_t pitch = (size_t)((d->nx + XOFF + 1 + 7) / 8 * 8);
     const size_t field = pitch * (d->ny + 2) * (d->nz + 2);
-    *bytes = 2 * field * moments_of(*d) * elem_size(d->storage) + field;
+    // two buffers of moment pairs (an odd count is padded to the next pair), node classes
+    *bytes = 2 * field * (2 * ((moments_of(*d) + 1) / 2)) * elem_size(d->storage) + field;
     return MRLBM_OK;
 }
 
@@ -244,7 +245,8 @@ mrlbm_status mrlbm::domain_alloc(mrlbm_domain* dom)
                     d.nz, dom->field);
     dom->omega0 = 1.0 / d.tau;
     storage_scales(d.storage, dom->scale, dom->iscale);
-    const size_t mbytes = (size_t)dom->field * dom->nm * dom->esize;
+    // moment pairs: moments 2p and 2p + 1 interleaved per node (an odd count is padded)
+    const size_t mbytes = (size_t)dom->field * (2 * ((dom->nm + 1) / 2)) * dom->esize;
     CK(cudaMalloc(&dom->m[0], mbytes));
     CK(cudaMalloc(&dom->m[1], mbytes));
     CK(cudaMemset(dom->m[0], 0, mbytes));
@@ -519,8 +521,9 @@ void mrlbm::fill_step_args(const mrlbm_domain* dom, StepArgs& a, int parity, int
 {
     const mrlbm_desc& d = dom->d;
     a.m_out = dom->m[parity ^ 1];
-    for (int m = 0; m < 11; m++)
-        a.out_m[m] = m < dom->nm ? static_cast<char*>(dom->m[parity ^ 1]) + (size_t)m * dom->field * dom->esize : nullptr;
+    for (int p = 0; p < 6; p++)
+        a.out_p[p] = 2 * p < dom->nm ? static_cast<char*>(dom->m[parity ^ 1]) + (size_t)p * 2 * dom->field * dom->esize
+                                     : nullptr;
     a.err = dom->err;
     a.cls = dom->cls;
     a.bc = dom->bc;
@@ -760,9 +763,10 @@ static EncodeTiledFn encode_fn()
     return fn;
 }
 
-// 4-D map over one padded moment buffer with dimension order (x, moment, y, z)
-// so that a box of (40, nm, tile_y(q) + 2, 1) lands in shared memory as
-// [row][moment][x]: one plane of a CTA column per copy.
+// 4-D map over one padded moment buffer with dimension order (x and pair
+// element, moment pair, y, z) so that a box of (2 * 40, pairs, tile_y(q) + 2,
+// 1) lands in shared memory as [row][pair][x][2]: one plane of a CTA column
+// per copy.
 mrlbm_status mrlbm::make_tensor_maps(mrlbm_domain* dom)
 {
     EncodeTiledFn enc = encode_fn();
@@ -772,11 +776,13 @@ mrlbm_status mrlbm::make_tensor_maps(mrlbm_domain* dom)
                                    : d.storage == MRLBM_F16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
                                                             : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
     const cuuint64_t es = dom->esize;
-    const cuuint64_t dims[4] = {(cuuint64_t)dom->pitch, (cuuint64_t)dom->nm, (cuuint64_t)(d.ny + 2),
-                                (cuuint64_t)(d.nz + 2)};
-    const cuuint64_t strides[3] = {(cuuint64_t)dom->field * es, (cuuint64_t)dom->pitch * es,
-                                   (cuuint64_t)dom->plane * es};
-    const cuuint32_t box[4] = {(cuuint32_t)BOX_X, (cuuint32_t)dom->nm, (cuuint32_t)(tile_y(dom->q) + 2), 1};
+    // x runs over the interleaved pair elements (2 per node), the second
+    // dimension over moment pairs
+    const cuuint32_t npairs = (cuuint32_t)((dom->nm + 1) / 2);
+    const cuuint64_t dims[4] = {(cuuint64_t)(2 * dom->pitch), npairs, (cuuint64_t)(d.ny + 2), (cuuint64_t)(d.nz + 2)};
+    const cuuint64_t strides[3] = {(cuuint64_t)(2 * dom->field) * es, (cuuint64_t)(2 * dom->pitch) * es,
+                                   (cuuint64_t)(2 * dom->plane) * es};
+    const cuuint32_t box[4] = {(cuuint32_t)(2 * BOX_X), npairs, (cuuint32_t)(tile_y(dom->q) + 2), 1};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     for (int b = 0; b < 2; b++) {
         CUresult r = enc(&dom->tmap[b], dt, 4, dom->m[b], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
