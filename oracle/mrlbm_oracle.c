@@ -39,6 +39,7 @@
 #endif
 
 #define ORC_MAXQ 27
+#define ORC_SLAB 16   /* z planes per slab of the step (bounds the population scratch) */
 
 /* Arithmetic type of the step.  FP64 by default (liboracle.so, the oracle);
  * `-DORC_REAL=float -fsingle-precision-constant` builds liboracle_f32.so, the
@@ -87,8 +88,8 @@ typedef struct {
     size_t n;
     real *m, *m2;        /* [node][nm], node = x + nx*(y + ny*z) */
     uint32_t *type;        /* reference nodeTypeMap words, same node order */
-    real *pop;           /* [3][plane][q] post-collision populations of a 3-plane window */
-    int win[3];            /* z plane held by each window slot, -1 = none */
+    real *pop;           /* [slab + 2][plane][q] post-collision populations of a slab of planes */
+    int slab;              /* output planes per slab */
 } orc_domain;
 
 /* ----------------------------------------------------------------- per node */
@@ -314,7 +315,8 @@ void *orc_create(const orc_desc *d)
     o->m = (real *)calloc(o->n * o->nm, sizeof(real));
     o->m2 = (real *)calloc(o->n * o->nm, sizeof(real));
     o->type = (uint32_t *)calloc(o->n, sizeof(uint32_t));
-    o->pop = (real *)malloc(3 * (size_t)d->nx * d->ny * d->q * sizeof(real));
+    o->slab = d->nz < ORC_SLAB ? d->nz : ORC_SLAB;
+    o->pop = (real *)malloc((size_t)(o->slab + 2) * d->nx * d->ny * d->q * sizeof(real));
     if (!o->m || !o->m2 || !o->type || !o->pop) {
         free(o->m); free(o->m2); free(o->type); free(o->pop); free(o);
         return NULL;
@@ -395,87 +397,66 @@ static inline int resolve(int v, int n, int periodic, int *outside)
     return 0;
 }
 
-/* The window slot holding the populations of plane z, or NULL. */
-static real *window_plane(orc_domain *o, int z)
-{
-    const int q = o->d.q;
-    const size_t pl = (size_t)o->d.nx * o->d.ny;
-    for (int s = 0; s < 3; s++)
-        if (o->win[s] == z) return o->pop + (size_t)s * pl * q;
-    return NULL;
-}
-
-/* Post-collision populations of plane z into a slot that is empty or holds a
- * plane outside the current window keep[]. */
-static void window_fill(orc_domain *o, int z, const int keep[3])
-{
-    const int q = o->d.q, nm = o->nm;
-    const size_t pl = (size_t)o->d.nx * o->d.ny;
-    if (window_plane(o, z)) return;
-    int s = 0;
-    while (s < 3 && o->win[s] >= 0 && (o->win[s] == keep[0] || o->win[s] == keep[1] || o->win[s] == keep[2])) s++;
-    real *dst = o->pop + (size_t)s * pl * q;
-    const real *src = o->m + (size_t)z * pl * nm;
-#pragma omp parallel for schedule(static)
-    for (long k = 0; k < (long)pl; k++) orc_reconstruct(q, o->d.rho0, src + k * nm, dst + k * q);
-    o->win[s] = z;
-}
-
 void orc_step(void *h, int nsteps)
 {
     orc_domain *o = (orc_domain *)h;
     const orc_desc *d = &o->d;
     const int q = d->q, nm = o->nm, nx = d->nx, ny = d->ny, nz = d->nz;
+    const size_t pl = (size_t)nx * ny;
     const real omega0 = 1.0 / d->tau;
     real fext[ORC_MAXQ];
     real ext[10];
     for (int k = 0; k < 10; k++) ext[k] = (real)d->exterior[k];
     orc_reconstruct(q, d->rho0, ext, fext);
     for (int s = 0; s < nsteps; s++) {
-        /* output plane z pulls from planes z-1, z, z+1: their post-collision
-         * populations (from the stored moments) are kept in a 3-plane window,
-         * so the scratch is 3 planes, not the whole domain */
-        o->win[0] = o->win[1] = o->win[2] = -1;
-        for (int z = 0; z < nz; z++) {
-            int src[3];
-            for (int dz = -1; dz <= 1; dz++) {
+        /* output planes [z0, z1) pull from planes z0-1 .. z1: their
+         * post-collision populations (from the stored moments) are built
+         * for one slab at a time, so the scratch is slab + 2 planes */
+        for (int z0 = 0; z0 < nz; z0 += o->slab) {
+            const int z1 = (z0 + o->slab < nz) ? z0 + o->slab : nz;
+            const int nsl = z1 - z0 + 2;
+            int src[ORC_SLAB + 2];
+            for (int k = 0; k < nsl; k++) {
                 int out = 0;
-                int sz = resolve(z + dz, nz, d->periodic[2], &out);
-                src[dz + 1] = out ? -1 : sz;
+                const int sz = resolve(z0 - 1 + k, nz, d->periodic[2], &out);
+                src[k] = out ? -1 : sz;
             }
-            for (int k = 0; k < 3; k++)
-                if (src[k] >= 0) window_fill(o, src[k], src);
-            const real *wp[3];
-            for (int k = 0; k < 3; k++) wp[k] = src[k] >= 0 ? window_plane(o, src[k]) : NULL;
-#pragma omp parallel for schedule(static)
-            for (int y = 0; y < ny; y++)
-                for (int x = 0; x < nx; x++) {
-                    size_t k = (size_t)x + (size_t)nx * (y + (size_t)ny * z);
-                    uint32_t t = o->type[k];
-                    real *mo = o->m2 + k * nm;
-                    const real *mi = o->m + k * nm;
-                    if ((t & 0xFFu) == 0xFFu) { memcpy(mo, mi, nm * sizeof(real)); continue; }
-                    real f[ORC_MAXQ];
-                    for (int i = 0; i < q; i++) {
-                        int out = 0;
-                        int sx = resolve(x - CX[i], nx, d->periodic[0], &out);
-                        int sy = resolve(y - CY[i], ny, d->periodic[1], &out);
-                        const real *pl = wp[1 - CZ[i]];
-                        f[i] = (out || !pl) ? fext[i] : pl[((size_t)sx + (size_t)nx * sy) * q + i];
+#pragma omp parallel for collapse(2) schedule(static)
+            for (int k = 0; k < nsl; k++)
+                for (long c = 0; c < (long)pl; c++)
+                    if (src[k] >= 0)
+                        orc_reconstruct(q, d->rho0, o->m + ((size_t)src[k] * pl + c) * nm, o->pop + ((size_t)k * pl + c) * q);
+#pragma omp parallel for collapse(2) schedule(static)
+            for (int z = z0; z < z1; z++)
+                for (int y = 0; y < ny; y++)
+                    for (int x = 0; x < nx; x++) {
+                        size_t k = (size_t)x + (size_t)nx * (y + (size_t)ny * z);
+                        uint32_t t = o->type[k];
+                        real *mo = o->m2 + k * nm;
+                        const real *mi = o->m + k * nm;
+                        if ((t & 0xFFu) == 0xFFu) { memcpy(mo, mi, nm * sizeof(real)); continue; }
+                        real f[ORC_MAXQ];
+                        for (int i = 0; i < q; i++) {
+                            int out = 0;
+                            int sx = resolve(x - CX[i], nx, d->periodic[0], &out);
+                            int sy = resolve(y - CY[i], ny, d->periodic[1], &out);
+                            const int ks = z - CZ[i] - (z0 - 1);
+                            f[i] = (out || src[ks] < 0) ? fext[i]
+                                                        : o->pop[((size_t)ks * pl + (size_t)sx + (size_t)nx * sy) * q + i];
+                        }
+                        real omega = (nm > 10) ? mi[10] : omega0;
+                        real mac[10];
+                        if ((t & 0xFFu) == 0) {
+                            orc_bulk_moments(q, f, mac);
+                        } else {
+                            int vidx = (t >> 11) & 3u;
+                            int kind = (t >> 8) & 7u;
+                            real u[3] = {0, 0, 0};
+                            if (kind == 1) { u[0] = d->bc_velocity[vidx][0]; u[1] = d->bc_velocity[vidx][1]; u[2] = d->bc_velocity[vidx][2]; }
+                            orc_bc_solve(q, d->bc_matrix_q ? d->bc_matrix_q : q, orc_known_mask(q, t & 0xFFu), u, omega, f, mac);
+                        }
+                        collide_store(d, nm, mac, omega, mo);
                     }
-                    real omega = (nm > 10) ? mi[10] : omega0;
-                    real mac[10];
-                    if ((t & 0xFFu) == 0) {
-                        orc_bulk_moments(q, f, mac);
-                    } else {
-                        int vidx = (t >> 11) & 3u;
-                        int kind = (t >> 8) & 7u;
-                        real u[3] = {0, 0, 0};
-                        if (kind == 1) { u[0] = d->bc_velocity[vidx][0]; u[1] = d->bc_velocity[vidx][1]; u[2] = d->bc_velocity[vidx][2]; }
-                        orc_bc_solve(q, d->bc_matrix_q ? d->bc_matrix_q : q, orc_known_mask(q, t & 0xFFu), u, omega, f, mac);
-                    }
-                    collide_store(d, nm, mac, omega, mo);
-                }
         }
         real *tmp = o->m; o->m = o->m2; o->m2 = tmp;
     }
