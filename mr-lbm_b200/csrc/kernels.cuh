@@ -404,17 +404,51 @@ __device__ __forceinline__ float nnf_powerlaw(float omega_old, float smag, float
 
 // Scale to the stored form, update omega (non-Newtonian), collide
 // (src/colrec/MR_LBM/collision.inc:2-14), write the 10/11 stored moments.
+// The collision on the stored (scaled) moments: 3u, 4.5 Pi_ii, 9 Pi_ij
+// (src/colrec/MR_LBM/collision.inc:2-14); writes the 10/11 stored moments.
+template <int FLAGS>
+__device__ __forceinline__ void collide_scaled(const StepArgs& a, float rho, float ux, float uy, float uz, float mxx,
+                                               float mxy, float mxz, float myy, float myz, float mzz, float omega,
+                                               float* out)
+{
+    const float t_om = 1.0f - omega, om_d2 = 0.5f * omega;
+    if constexpr ((FLAGS & F_FORCE) != 0) {
+        const float Fx = a.fx, Fy = a.fy, Fz = a.fz;
+        const float ir = 1.0f / rho;
+        const float tt_om = 1.0f - 0.5f * omega;
+        ux += 3.0f * ir * Fx;
+        uy += 3.0f * ir * Fy;
+        uz += 3.0f * ir * Fz;
+        const float c15 = 1.5f * ir * tt_om, c3 = 3.0f * tt_om * ir;
+        mxx = t_om * mxx + om_d2 * ux * ux + c15 * (2.0f * Fx * ux);
+        myy = t_om * myy + om_d2 * uy * uy + c15 * (2.0f * Fy * uy);
+        mzz = t_om * mzz + om_d2 * uz * uz + c15 * (2.0f * Fz * uz);
+        mxy = t_om * mxy + omega * ux * uy + c3 * (Fx * uy + Fy * ux);
+        mxz = t_om * mxz + omega * ux * uz + c3 * (Fx * uz + Fz * ux);
+        myz = t_om * myz + omega * uy * uz + c3 * (Fy * uz + Fz * uy);
+    } else {
+        mxx = t_om * mxx + om_d2 * ux * ux;
+        myy = t_om * myy + om_d2 * uy * uy;
+        mzz = t_om * mzz + om_d2 * uz * uz;
+        mxy = t_om * mxy + omega * ux * uy;
+        mxz = t_om * mxz + omega * ux * uz;
+        myz = t_om * myz + omega * uy * uz;
+    }
+    out[0] = rho - a.rho0;
+    out[1] = ux; out[2] = uy; out[3] = uz;
+    out[4] = mxx; out[5] = mxy; out[6] = mxz; out[7] = myy; out[8] = myz; out[9] = mzz;
+    out[10] = omega;
+}
+
+// Scale to the stored form, update omega (non-Newtonian), collide.
 template <int FLAGS>
 __device__ __forceinline__ void collide(const StepArgs& a, const float* mac, float omega, float* out)
 {
     const float rho = mac[0];
-    float ux = 3.0f * mac[1], uy = 3.0f * mac[2], uz = 3.0f * mac[3];
-    float mxx = 4.5f * mac[4], mxy = 9.0f * mac[5], mxz = 9.0f * mac[6];
-    float myy = 4.5f * mac[7], myz = 9.0f * mac[8], mzz = 4.5f * mac[9];
-    const float Fx = (FLAGS & F_FORCE) ? a.fx : 0.f;
-    const float Fy = (FLAGS & F_FORCE) ? a.fy : 0.f;
-    const float Fz = (FLAGS & F_FORCE) ? a.fz : 0.f;
     if constexpr ((FLAGS & (F_POWERLAW | F_BINGHAM)) != 0) {
+        const float Fx = (FLAGS & F_FORCE) ? a.fx : 0.f;
+        const float Fy = (FLAGS & F_FORCE) ? a.fy : 0.f;
+        const float Fz = (FLAGS & F_FORCE) ? a.fz : 0.f;
         // shear magnitude from the non-equilibrium second moments, src/mlbm.cu:526-546
         const float sxx = rho * (mac[4] - mac[1] * mac[1]), syy = rho * (mac[7] - mac[2] * mac[2]);
         const float szz = rho * (mac[9] - mac[3] * mac[3]), sxy = rho * (mac[5] - mac[1] * mac[2]);
@@ -429,33 +463,8 @@ __device__ __forceinline__ void collide(const StepArgs& a, const float* mac, flo
         else
             omega = a.nnf_omega_p * fmaxf(0.f, 1.0f - a.nnf_yield / smag);
     }
-    const float ir = 1.0f / rho;
-    const float t_om = 1.0f - omega, tt_om = 1.0f - 0.5f * omega, om_d2 = 0.5f * omega;
-    if constexpr ((FLAGS & F_FORCE) != 0) {
-        ux += 3.0f * ir * Fx;
-        uy += 3.0f * ir * Fy;
-        uz += 3.0f * ir * Fz;
-        const float c15 = 1.5f * ir * tt_om, c3 = 3.0f * tt_om * ir;
-        mxx = t_om * mxx + om_d2 * ux * ux + c15 * (2.0f * Fx * ux);
-        myy = t_om * myy + om_d2 * uy * uy + c15 * (2.0f * Fy * uy);
-        mzz = t_om * mzz + om_d2 * uz * uz + c15 * (2.0f * Fz * uz);
-        mxy = t_om * mxy + omega * ux * uy + c3 * (Fx * uy + Fy * ux);
-        mxz = t_om * mxz + omega * ux * uz + c3 * (Fx * uz + Fz * ux);
-        myz = t_om * myz + omega * uy * uz + c3 * (Fy * uz + Fz * uy);
-    } else {
-        (void)ir;
-        (void)tt_om;
-        mxx = t_om * mxx + om_d2 * ux * ux;
-        myy = t_om * myy + om_d2 * uy * uy;
-        mzz = t_om * mzz + om_d2 * uz * uz;
-        mxy = t_om * mxy + omega * ux * uy;
-        mxz = t_om * mxz + omega * ux * uz;
-        myz = t_om * myz + omega * uy * uz;
-    }
-    out[0] = rho - a.rho0;
-    out[1] = ux; out[2] = uy; out[3] = uz;
-    out[4] = mxx; out[5] = mxy; out[6] = mxz; out[7] = myy; out[8] = myz; out[9] = mzz;
-    out[10] = omega;
+    collide_scaled<FLAGS>(a, rho, 3.0f * mac[1], 3.0f * mac[2], 3.0f * mac[3], 4.5f * mac[4], 9.0f * mac[5],
+                          9.0f * mac[6], 4.5f * mac[7], 9.0f * mac[8], 4.5f * mac[9], omega, out);
 }
 
 // ---------------------------------------------------- TMA / mbarrier helpers
@@ -698,10 +707,18 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
         const unsigned oidx = (unsigned)(zd + 1) * (unsigned)a.plane + (unsigned)((y + 1) * a.pitch + x + XOFF);
         uint8_t cls = CLS_BULK;
         if constexpr ((FLAGS & F_BC) != 0) cls = live ? __ldg(a.cls + oidx) : CLS_SOLID;
-        float mac[10];
-        {
-            float r, j[3], P[6];
-            lattice_sums<Q>(p, r, j, P);
+        float o[11];
+        float r, j[3], P[6];
+        lattice_sums<Q>(p, r, j, P);
+        if constexpr ((FLAGS & (F_BC | F_POWERLAW | F_BINGHAM)) == 0) {
+            // bulk-only domains: the moments straight in the stored scaling
+            // (3u = 3 j / rho, 4.5 Pi_ii = 4.5 P_ii / rho - 1.5, 9 Pi_ij)
+            const float ir = 1.0f / r;
+            const float i3 = 3.0f * ir, i45 = 4.5f * ir, i9 = 9.0f * ir;
+            collide_scaled<FLAGS>(a, r, j[0] * i3, j[1] * i3, j[2] * i3, fmaf(P[0], i45, -1.5f), P[1] * i9, P[2] * i9,
+                                  fmaf(P[3], i45, -1.5f), P[4] * i9, fmaf(P[5], i45, -1.5f), omega, o);
+        } else {
+            float mac[10];
             const float ir = 1.0f / r;
             mac[0] = r;
             mac[1] = j[0] * ir; mac[2] = j[1] * ir; mac[3] = j[2] * ir;
@@ -711,12 +728,11 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
             mac[7] = P[3] * ir - (1.0f / 3.0f);
             mac[8] = P[4] * ir;
             mac[9] = P[5] * ir - (1.0f / 3.0f);
+            if constexpr ((FLAGS & F_BC) != 0) {
+                if (cls != CLS_BULK && cls != CLS_SOLID) BCP::template apply<Q>(a, cls, p, omega, x, y, zd, mac);
+            }
+            collide<FLAGS>(a, mac, omega, o);
         }
-        if constexpr ((FLAGS & F_BC) != 0) {
-            if (cls != CLS_BULK && cls != CLS_SOLID) BCP::template apply<Q>(a, cls, p, omega, x, y, zd, mac);
-        }
-        float o[11];
-        collide<FLAGS>(a, mac, omega, o);
         if constexpr (!is_f32<T>()) {
 #pragma unroll
             for (int m = 0; m < NM; m++) o[m] = o[m] * a.scale[m];
