@@ -42,7 +42,7 @@ METRIC = "MLUPS (fused MR-LBM step)"
 
 
 def workload_config():
-    return {"workload": "taylor_green_256^3_d3q27_fp32", "grid": [N, N, N], "lattice": "D3Q27",
+    return {"workload": "taylor_green_256^3_d3q%d_fp32" % LATTICE, "grid": [N, N, N], "lattice": "D3Q%d" % LATTICE,
             "storage": "fp32", "re": RE, "u0": U0, "tau": round(TAU, 8), "steps_per_e2e_run": E2E_STEPS,
             "l2": "inputs larger than L2 (2 x 671 MB ping-pong moment buffers)", "parallelism": "replicas"}
 
@@ -58,7 +58,7 @@ def measured_peaks():
 
 def profiled_traffic():
     """DRAM bytes per launch of the step kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "zmarch_step_d3q27_f32_tgv.md")
+    path = os.path.join(ROOT, "profiles", "zmarch_step_d3q%d_f32_tgv.md" % LATTICE)
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch_256:"):
@@ -176,7 +176,7 @@ def cpu_oracle_mlups(budget_s, n=96, steps_max=40):
         steps += 1
     dt = time.perf_counter() - t0
     threads = oracle_ffi.lib().orc_threads()
-    return steps * n ** 3 / dt / 1e6, threads, "%d^3 D3Q27 Taylor-Green, %d steps, FP64" % (n, steps)
+    return steps * n ** 3 / dt / 1e6, threads, "%d^3 D3Q%d Taylor-Green, %d steps, FP64" % (n, LATTICE, steps)
 
 
 def run_reference_arm(args):
@@ -200,7 +200,7 @@ def run_reference_arm(args):
     dt = time.perf_counter() - t0
     mlups = args.steps * n ** 3 / dt / 1e6
     threads = oracle_ffi.lib().orc_threads()
-    sample = "%d^3 D3Q27 Taylor-Green per step (bounded sample of the 256^3 workload), FP64 OpenMP" % n
+    sample = "%d^3 D3Q%d Taylor-Green per step (bounded sample of the 256^3 workload), FP64 OpenMP" % (n, LATTICE)
     line = {"impl": "reference", "metric": METRIC, "value": round(mlups, 3), "unit": "MLUPS", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * dt / args.steps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -542,6 +542,8 @@ def main():
     ap.add_argument("--workload", default="tgv", choices=["tgv", "batch", "serve", "precision"],
                     help="tgv: the headline step benchmark (default); batch / serve / precision: the "
                          "batched-cavity, serving and storage-precision workloads (longer, run on their own)")
+    ap.add_argument("--lattice", type=int, default=27, choices=[19, 27],
+                    help="tgv workload: velocity set (D3Q27 is the benchmark's; D3Q19 for comparison)")
     ap.add_argument("--n", type=int, default=512, help="precision workload: grid edge")
     ap.add_argument("--precision-steps", type=int, default=1000)
     ap.add_argument("--reference", default=None, help="precision workload: FP64 planes from oracle/tgv_reference.py")
@@ -553,6 +555,8 @@ def main():
     ap.add_argument("--max-active", type=int, default=512)
     ap.add_argument("--max-steps", type=int, default=20000)
     args = ap.parse_args()
+    global LATTICE
+    LATTICE = args.lattice
     if args.impl == "reference":
         return run_reference_arm(args)
     if args.workload == "batch":
