@@ -882,9 +882,19 @@ struct ZMarch {
     {
         const bool ok = mbar_wait(&bars[cs], cph);
         const float om_out = om_par;
-        prod_a<Q, NM, T, TYI>(a, stage_ptr(), e4t[PAR], e1t[PAR], gsh_new, om_par);
-        prod_b<Q, NM, NUP, NMID, T, FLAGS, TYI, BCP>(a, j - 1, z0 - 2 + j, e4t[PAR ^ 1], e1t[PAR ^ 1], interior, x, y,
-                                                gsh_old, up, mid, om_out);
+        // the two halves are independent; which comes first in the source
+        // only steers the compiler's schedule (results are bit-identical):
+        // consumption first measured 4 % faster on bulk and D3Q27 domains,
+        // production first 4 % faster on D3Q19 domains with walls
+        if constexpr (Q == 27 || (FLAGS & F_BC) == 0) {
+            prod_b<Q, NM, NUP, NMID, T, FLAGS, TYI, BCP>(a, j - 1, z0 - 2 + j, e4t[PAR ^ 1], e1t[PAR ^ 1], interior, x,
+                                                    y, gsh_old, up, mid, om_out);
+            prod_a<Q, NM, T, TYI>(a, stage_ptr(), e4t[PAR], e1t[PAR], gsh_new, om_par);
+        } else {
+            prod_a<Q, NM, T, TYI>(a, stage_ptr(), e4t[PAR], e1t[PAR], gsh_new, om_par);
+            prod_b<Q, NM, NUP, NMID, T, FLAGS, TYI, BCP>(a, j - 1, z0 - 2 + j, e4t[PAR ^ 1], e1t[PAR ^ 1], interior, x,
+                                                    y, gsh_old, up, mid, om_out);
+        }
         if (__syncthreads_or(!ok)) return false;
         advance(j);
         return true;
