@@ -25,6 +25,13 @@
  *      POWERLAW/POWER_LAW guard, the undeclared `omega`, POW_FUNCTION = pow)
  *   - initial moments                 src/lbmInitialization.cu:28-131
  *   - kinetic energy                  src/reduction.cu:128-155, src/treatData.cu:105-165
+ *   - thermal scalar (D3G19)          src/mlbm.cu:157-191 (pull + sums), 515-522 (Boussinesq
+ *                                     force), 603-616 (stored C, q); G_SCALAR reconstruction
+ *                                     src/colrec/G_SCALAR/reconstruction.inc:1-25; weights
+ *                                     src/includeFiles/velocitySets/D3G19.inc:1-19; diffusivity
+ *                                     coefficient src/cases/rayleighBenard_Periodic/constants.inc:54-65;
+ *                                     wall kinds as in src/cases/thermal_2D/g_bc_definition.inc,
+ *                                     src/cases/rayleighBenard_Closed/g_bc_definition.inc
  *
  * Parity pins: per-node functions are checked against the reference's own
  * snippets compiled on the host (oracle/ref_kat.cpp -> oracle/_ref); full runs
@@ -80,15 +87,26 @@ typedef struct {
     double n_index, k_consistency, yield_stress, omega_p;
     double exterior[10];   /* stored-moment state used for sources outside wall axes */
     int bc_matrix_q;       /* lattice of the BC system matrix (19 or q) */
+    /* thermal scalar C on D3G19 (THERMAL_MODEL): 4 more stored moments
+     * C, 3 sum g c_x, 3 sum g c_y, 3 sum g c_z after the flow's */
+    int thermal;
+    double t_alpha;        /* T_DIFFUSIVITY */
+    double t_reference;    /* T_REFERENCE: buoyancy reference, exterior C */
+    double t_gbeta[3];     /* gravity_vector * T_gravity_t_beta */
+    double t_source;       /* T_Q_INTERNAL_D_Cp, added at bulk nodes */
+    double t_wall[4];      /* wall values by thermal value index */
 } orc_desc;
 
 typedef struct {
     orc_desc d;
-    int nm;                /* 10, or 11 with an omega field */
+    int nm;                /* 10, or 11 with an omega field, or 14 with the thermal scalar */
+    int nmf;               /* flow moments (10 or 11) */
+    real tcoef;            /* G_DIFF_FLUC_COEF */
     size_t n;
     real *m, *m2;        /* [node][nm], node = x + nx*(y + ny*z) */
     uint32_t *type;        /* reference nodeTypeMap words, same node order */
     real *pop;           /* [slab + 2][plane][q] post-collision populations of a slab of planes */
+    real *gpop;          /* [slab + 2][plane][19] thermal populations (thermal only) */
     int slab;              /* output planes per slab */
 } orc_domain;
 
@@ -260,13 +278,13 @@ real orc_nnf_bingham(real smag, real omega_p, real yield_stress)
 
 /* Scale, (shear, nnf), collide.  mac = rho,u,Pi unscaled in/out; m = stored
  * scaled moments out (nm entries).  Follows mlbm.cu:500-591 + collision.inc. */
-static void collide_store(const orc_desc *d, int nm, const real *mac, real omega_in, real *m)
+static void collide_store(const orc_desc *d, int nm, const real *mac, real omega_in, real *m, const real *F)
 {
     real rho = mac[0];
     real ux = 3.0 * mac[1], uy = 3.0 * mac[2], uz = 3.0 * mac[3];
     real mxx = 4.5 * mac[4], mxy = 9.0 * mac[5], mxz = 9.0 * mac[6];
     real myy = 4.5 * mac[7], myz = 9.0 * mac[8], mzz = 4.5 * mac[9];
-    real Fx = d->force[0], Fy = d->force[1], Fz = d->force[2];
+    real Fx = F[0], Fy = F[1], Fz = F[2];
     real omega = omega_in;
     if (d->rheology != ORC_NEWTONIAN) {
         real sxx = rho * (mxx / 4.5 - ux * ux / 9.0), syy = rho * (myy / 4.5 - uy * uy / 9.0);
@@ -300,7 +318,59 @@ static void collide_store(const orc_desc *d, int nm, const real *mac, real omega
 /* exposed for KATs: unscaled macroscopics + omega -> stored post-collision moments */
 void orc_collide(const orc_desc *d, const real *mac, real omega, real *m_out, int nm)
 {
-    collide_store(d, nm, mac, omega, m_out);
+    real F[3] = {d->force[0], d->force[1], d->force[2]};
+    collide_store(d, nm, mac, omega, m_out, F);
+}
+
+/* --------------------------------------------------------- thermal scalar */
+
+/* G_DIFF_FLUC_COEF from the thermal diffusivity, with the reference's fixed
+ * T_DIFF_REF = 1/6 and G_TAU = 3 T_DIFF_REF + 1/2
+ * (src/cases/rayleighBenard_Periodic/constants.inc:58-65). */
+double orc_thermal_coef(double alpha)
+{
+    double diff_ref = 1.0 / 6.0, g_tau = diff_ref * 3.0 + 0.5, g_omega = 1.0 / g_tau;
+    double aaa = 3.0 * (alpha - diff_ref) * g_omega;
+    return aaa / (1.0 + aaa);
+}
+
+/* g_i = C w_i (1 + c_i . (u3 + ud3)), ud3 = coef (q3 / C - u3), on the first
+ * 19 directions with the D3Q19 weights (G_SCALAR/reconstruction.inc:1-25,
+ * mlbm.cu:159-167). u3, q3: stored 3u and 3 sum g c. */
+void orc_reconstruct_g(real coef, real c, const real *u3, const real *q3, real *g)
+{
+    real ic = 1.0 / c, v[3];
+    for (int a = 0; a < 3; a++) v[a] = u3[a] + coef * (q3[a] * ic - u3[a]);
+    for (int i = 0; i < 19; i++)
+        g[i] = c * weight(19, i) * (1.0 + CX[i] * v[0] + CY[i] * v[1] + CZ[i] * v[2]);
+}
+
+/* C = sum g + source, q3 = 3 sum g c (mlbm.cu:180-188). */
+void orc_sums_g(const real *g, real source, real *cq)
+{
+    real c = 0, qx = 0, qy = 0, qz = 0;
+    for (int i = 0; i < 19; i++) {
+        c += g[i];
+        qx += g[i] * CX[i]; qy += g[i] * CY[i]; qz += g[i] * CZ[i];
+    }
+    cq[0] = c + source;
+    cq[1] = 3.0 * qx; cq[2] = 3.0 * qy; cq[3] = 3.0 * qz;
+}
+
+/* The wall of a face class: the axis whose whole + or - half of the octant
+ * mask is solid, when exactly one such (axis, side) exists.  Returns the axis
+ * (0..2) and *side (+1: solid on the + side), or -1. */
+int orc_face_normal(uint32_t octants, int *side)
+{
+    int found = -1, n = 0;
+    for (int a = 0; a < 3; a++)
+        for (int sd = 0; sd < 2; sd++) {
+            int all = 1;
+            for (int o = 0; o < 8; o++)
+                if ((((o >> a) & 1) == sd) && !((octants >> o) & 1u)) all = 0;
+            if (all) { found = a; *side = sd ? 1 : -1; n++; }
+        }
+    return n == 1 ? found : -1;
 }
 
 /* ------------------------------------------------------------------ domain */
@@ -310,15 +380,18 @@ void *orc_create(const orc_desc *d)
     orc_domain *o = (orc_domain *)calloc(1, sizeof(orc_domain));
     if (!o) return NULL;
     o->d = *d;
-    o->nm = (d->rheology != ORC_NEWTONIAN) ? 11 : 10;
+    o->nmf = (d->rheology != ORC_NEWTONIAN) ? 11 : 10;
+    o->nm = o->nmf + (d->thermal ? 4 : 0);
+    o->tcoef = (real)orc_thermal_coef(d->t_alpha);
     o->n = (size_t)d->nx * d->ny * d->nz;
     o->m = (real *)calloc(o->n * o->nm, sizeof(real));
     o->m2 = (real *)calloc(o->n * o->nm, sizeof(real));
     o->type = (uint32_t *)calloc(o->n, sizeof(uint32_t));
     o->slab = d->nz < ORC_SLAB ? d->nz : ORC_SLAB;
     o->pop = (real *)malloc((size_t)(o->slab + 2) * d->nx * d->ny * d->q * sizeof(real));
-    if (!o->m || !o->m2 || !o->type || !o->pop) {
-        free(o->m); free(o->m2); free(o->type); free(o->pop); free(o);
+    o->gpop = d->thermal ? (real *)malloc((size_t)(o->slab + 2) * d->nx * d->ny * 19 * sizeof(real)) : NULL;
+    if (!o->m || !o->m2 || !o->type || !o->pop || (d->thermal && !o->gpop)) {
+        free(o->m); free(o->m2); free(o->type); free(o->pop); free(o->gpop); free(o);
         return NULL;
     }
     return o;
@@ -328,7 +401,7 @@ void orc_destroy(void *h)
 {
     orc_domain *o = (orc_domain *)h;
     if (!o) return;
-    free(o->m); free(o->m2); free(o->type); free(o->pop); free(o);
+    free(o->m); free(o->m2); free(o->type); free(o->pop); free(o->gpop); free(o);
 }
 
 int orc_num_moments(void *h) { return ((orc_domain *)h)->nm; }
@@ -384,7 +457,11 @@ void orc_init_from_macro(void *h, const double *rho, const double *ux, const dou
         m[7] = 4.5 * (p[3] * ir - 1.0 / 3.0);
         m[8] = 9.0 * (p[4] * ir);
         m[9] = 4.5 * (p[5] * ir - 1.0 / 3.0);
-        if (o->nm > 10) m[10] = omega;
+        if (o->nmf > 10) m[10] = omega;
+        if (o->d.thermal) {
+            m[o->nmf] = o->d.t_reference;
+            m[o->nmf + 1] = m[o->nmf + 2] = m[o->nmf + 3] = 0.0;
+        }
     }
     memcpy(o->m2, o->m, o->n * o->nm * sizeof(real));
 }
@@ -401,13 +478,18 @@ void orc_step(void *h, int nsteps)
 {
     orc_domain *o = (orc_domain *)h;
     const orc_desc *d = &o->d;
-    const int q = d->q, nm = o->nm, nx = d->nx, ny = d->ny, nz = d->nz;
+    const int q = d->q, nm = o->nm, nmf = o->nmf, nx = d->nx, ny = d->ny, nz = d->nz;
+    const int th = d->thermal;
     const size_t pl = (size_t)nx * ny;
     const real omega0 = 1.0 / d->tau;
-    real fext[ORC_MAXQ];
+    real fext[ORC_MAXQ], gext[19];
     real ext[10];
     for (int k = 0; k < 10; k++) ext[k] = (real)d->exterior[k];
     orc_reconstruct(q, d->rho0, ext, fext);
+    if (th) {
+        const real q0[3] = {0, 0, 0};
+        orc_reconstruct_g(o->tcoef, (real)d->t_reference, ext + 1, q0, gext);
+    }
     for (int s = 0; s < nsteps; s++) {
         /* output planes [z0, z1) pull from planes z0-1 .. z1: their
          * post-collision populations (from the stored moments) are built
@@ -424,8 +506,12 @@ void orc_step(void *h, int nsteps)
 #pragma omp parallel for collapse(2) schedule(static)
             for (int k = 0; k < nsl; k++)
                 for (long c = 0; c < (long)pl; c++)
-                    if (src[k] >= 0)
-                        orc_reconstruct(q, d->rho0, o->m + ((size_t)src[k] * pl + c) * nm, o->pop + ((size_t)k * pl + c) * q);
+                    if (src[k] >= 0) {
+                        const real *ms = o->m + ((size_t)src[k] * pl + c) * nm;
+                        orc_reconstruct(q, d->rho0, ms, o->pop + ((size_t)k * pl + c) * q);
+                        if (th)
+                            orc_reconstruct_g(o->tcoef, ms[nmf], ms + 1, ms + nmf + 1, o->gpop + ((size_t)k * pl + c) * 19);
+                    }
 #pragma omp parallel for collapse(2) schedule(static)
             for (int z = z0; z < z1; z++)
                 for (int y = 0; y < ny; y++)
@@ -435,16 +521,65 @@ void orc_step(void *h, int nsteps)
                         real *mo = o->m2 + k * nm;
                         const real *mi = o->m + k * nm;
                         if ((t & 0xFFu) == 0xFFu) { memcpy(mo, mi, nm * sizeof(real)); continue; }
-                        real f[ORC_MAXQ];
+                        real f[ORC_MAXQ], g[19];
                         for (int i = 0; i < q; i++) {
                             int out = 0;
                             int sx = resolve(x - CX[i], nx, d->periodic[0], &out);
                             int sy = resolve(y - CY[i], ny, d->periodic[1], &out);
                             const int ks = z - CZ[i] - (z0 - 1);
-                            f[i] = (out || src[ks] < 0) ? fext[i]
-                                                        : o->pop[((size_t)ks * pl + (size_t)sx + (size_t)nx * sy) * q + i];
+                            const int ext_src = out || src[ks] < 0;
+                            const size_t ps = (size_t)ks * pl + (size_t)sx + (size_t)nx * sy;
+                            f[i] = ext_src ? fext[i] : o->pop[ps * q + i];
+                            if (th && i < 19) g[i] = ext_src ? gext[i] : o->gpop[ps * 19 + i];
                         }
-                        real omega = (nm > 10) ? mi[10] : omega0;
+                        real omega = (nmf > 10) ? mi[10] : omega0;
+                        real F[3] = {d->force[0], d->force[1], d->force[2]};
+                        real cq[4];
+                        if (th) {
+                            const int tkind = (t >> 13) & 3u;
+                            if ((t & 0xFFu) == 0) {
+                                orc_sums_g(g, (real)d->t_source, cq);
+                                /* Boussinesq force at bulk nodes (mlbm.cu:515-522) */
+                                for (int a = 0; a < 3; a++) F[a] += (real)d->t_gbeta[a] * d->rho0 * (cq[0] - d->t_reference);
+                            } else if (tkind == 0) {
+                                /* no thermal rule for this node type: C, q keep the stored values */
+                                for (int c = 0; c < 4; c++) cq[c] = mi[nmf + c];
+                            } else {
+                                const real tw = (real)d->t_wall[(t >> 15) & 3u];
+                                int side = 0;
+                                const int ax = orc_face_normal(t & 0xFFu, &side);
+                                if (tkind == 1 || ax < 0) {
+                                    cq[0] = tw; cq[1] = cq[2] = cq[3] = 0.0;
+                                } else if (tkind == 2) {
+                                    /* normal flux of the inward neighbour, previous step */
+                                    int nb[3] = {x, y, z};
+                                    const int dim[3] = {nx, ny, nz};
+                                    nb[ax] -= side;
+                                    cq[0] = tw; cq[1] = cq[2] = cq[3] = 0.0;
+                                    if (nb[ax] >= 0 && nb[ax] < dim[ax]) {
+                                        const size_t kn = (size_t)nb[0] + (size_t)nx * (nb[1] + (size_t)ny * nb[2]);
+                                        cq[1 + ax] = o->m[kn * nm + nmf + 1 + ax];
+                                    }
+                                } else {
+                                    /* adiabatic: populations arriving from the solid side
+                                     * mirrored across the wall plane */
+                                    real gm[19];
+                                    for (int i = 0; i < 19; i++) {
+                                        const int c[3] = {CX[i], CY[i], CZ[i]};
+                                        if (c[ax] == -side) {
+                                            int mc[3] = {c[0], c[1], c[2]};
+                                            mc[ax] = -mc[ax];
+                                            int j = 0;
+                                            while (CX[j] != mc[0] || CY[j] != mc[1] || CZ[j] != mc[2]) j++;
+                                            gm[i] = g[j];
+                                        } else {
+                                            gm[i] = g[i];
+                                        }
+                                    }
+                                    orc_sums_g(gm, 0.0, cq);
+                                }
+                            }
+                        }
                         real mac[10];
                         if ((t & 0xFFu) == 0) {
                             orc_bulk_moments(q, f, mac);
@@ -455,7 +590,9 @@ void orc_step(void *h, int nsteps)
                             if (kind == 1) { u[0] = d->bc_velocity[vidx][0]; u[1] = d->bc_velocity[vidx][1]; u[2] = d->bc_velocity[vidx][2]; }
                             orc_bc_solve(q, d->bc_matrix_q ? d->bc_matrix_q : q, orc_known_mask(q, t & 0xFFu), u, omega, f, mac);
                         }
-                        collide_store(d, nm, mac, omega, mo);
+                        collide_store(d, nmf, mac, omega, mo, F);
+                        if (th)
+                            for (int c = 0; c < 4; c++) mo[nmf + c] = cq[c];
                     }
         }
         real *tmp = o->m; o->m = o->m2; o->m2 = tmp;

@@ -12,6 +12,9 @@
 //   src/cases/lidDrivenCavity_3D/bc_definition.inc         26 wall cases + moving lid
 //   src/cases/voxel/bc_definition.inc                      254 octant masks
 //   src/cases/parallelPlates_D3Q27/bc_definition.inc       D3Q27 plate walls
+//   src/includeFiles/velocitySets/D3G19.inc                thermal lattice weights
+//   src/colrec/G_SCALAR/reconstruction.inc                 thermal population reconstruction
+//   src/cases/rayleighBenard_Periodic/constants.inc        thermal case constants
 #include <cmath>
 #include <cstdint>
 
@@ -51,6 +54,39 @@ void ref_reconstruct_q27(const double* m, double rho0, double* pop)
 #include "colrec/MR_LBM/reconstruction.inc"
 }
 #undef D3Q27
+
+namespace g19 {
+#include "includeFiles/velocitySets/D3G19.inc"
+}
+
+// thermal populations from C, the stored flow velocity 3u and the diffusive
+// correction ud (src/mlbm.cu:165-169 computes ud = G_DIFF_FLUC_COEF (q/C - u))
+void ref_reconstruct_g19(double cVar, const double* u3, const double* ud3, double* gNode)
+{
+    using namespace g19;
+    dfloat ux_t30 = u3[0], uy_t30 = u3[1], uz_t30 = u3[2];
+    dfloat udx_t30 = ud3[0], udy_t30 = ud3[1], udz_t30 = ud3[2];
+    dfloat multiplyTerm, pics2;
+#include "colrec/G_SCALAR/reconstruction.inc"
+}
+
+namespace rbp {
+#include "cases/rayleighBenard_Periodic/constants.inc"
+}
+
+// [0] G_DIFF_FLUC_COEF, [1] T_DIFFUSIVITY, [2] T_gravity_t_beta, [3] VISC,
+// [4] T_REFERENCE, [5] T_HOT, [6] T_COLD, [7..9] gravity_vector
+void ref_rb_periodic_constants(double* out)
+{
+    out[0] = rbp::G_DIFF_FLUC_COEF;
+    out[1] = rbp::T_DIFFUSIVITY;
+    out[2] = rbp::T_gravity_t_beta;
+    out[3] = rbp::VISC;
+    out[4] = rbp::T_REFERENCE;
+    out[5] = rbp::T_HOT;
+    out[6] = rbp::T_COLD;
+    for (int a = 0; a < 3; a++) out[7 + a] = rbp::gravity_vector[a];
+}
 
 // scaled pre-collision moments m[1..9], rho, force, omega -> post-collision m[1..9]
 void ref_collide(double* m, double rho, const double* F, double omegaVar)

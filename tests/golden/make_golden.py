@@ -15,6 +15,11 @@ Contents (all float64):
       src/cases/voxel/bc_definition.inc (all 254 octant masks)
   pl27_type, pl27_pops (.,27), pl27_omega, pl27_out
       src/cases/parallelPlates_D3Q27/bc_definition.inc
+  g19_in (N,7) / g19_out (N,19)            src/colrec/G_SCALAR/reconstruction.inc (D3G19)
+      g19_in = [C, 3ux, 3uy, 3uz, udx, udy, udz]
+  rbp_const (10,)                          src/cases/rayleighBenard_Periodic/constants.inc:
+      G_DIFF_FLUC_COEF, T_DIFFUSIVITY, T_gravity_t_beta, VISC, T_REFERENCE, T_HOT,
+      T_COLD, gravity_vector[3]
 BC outputs are [rho, ux, uy, uz, Pi_xx, Pi_xy, Pi_xz, Pi_yy, Pi_yz, Pi_zz] (unscaled).
 """
 import ctypes as C
@@ -98,6 +103,19 @@ def main():
             types.append(t); pops.append(f); oms.append(om); res.append(r)
     out["pl27_type"] = np.array(types, dtype=np.uint32)
     out["pl27_pops"], out["pl27_omega"], out["pl27_out"] = map(np.array, (pops, oms, res))
+
+    gin = np.zeros((64, 7))
+    gout = np.zeros((64, 19))
+    for k in range(64):
+        gin[k, 0] = rng.uniform(0.5, 1.5)
+        gin[k, 1:4] = rng.normal(0.0, 0.1, 3)
+        gin[k, 4:7] = rng.normal(0.0, 0.05, 3)
+        R.ref_reconstruct_g19(gin[k, 0], P(np.ascontiguousarray(gin[k, 1:4])), P(np.ascontiguousarray(gin[k, 4:7])),
+                              P(gout[k]))
+    out["g19_in"], out["g19_out"] = gin, gout
+    rc = np.zeros(10)
+    R.ref_rb_periodic_constants(P(rc))
+    out["rbp_const"] = rc
 
     path = os.path.join(HERE, "ref_kat.npz")
     np.savez_compressed(path, **out)

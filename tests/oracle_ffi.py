@@ -33,6 +33,12 @@ class OrcDesc(C.Structure):
         ("yield_stress", C.c_double), ("omega_p", C.c_double),
         ("exterior", C.c_double * 10),
         ("bc_matrix_q", C.c_int),
+        ("thermal", C.c_int),
+        ("t_alpha", C.c_double),
+        ("t_reference", C.c_double),
+        ("t_gbeta", C.c_double * 3),
+        ("t_source", C.c_double),
+        ("t_wall", C.c_double * 4),
     ]
 
 
@@ -75,6 +81,12 @@ def lib(fp32=False):
         L.orc_nnf_bingham.argtypes = [C.c_double] * 3
         L.orc_nnf_bingham.restype = C.c_double
         L.orc_collide.argtypes = [C.POINTER(OrcDesc), D, C.c_double, D, C.c_int]
+        L.orc_thermal_coef.argtypes = [C.c_double]
+        L.orc_thermal_coef.restype = C.c_double
+        L.orc_reconstruct_g.argtypes = [C.c_double, C.c_double, D, D, D]
+        L.orc_sums_g.argtypes = [D, C.c_double, D]
+        L.orc_face_normal.argtypes = [C.c_uint32, C.POINTER(C.c_int)]
+        L.orc_face_normal.restype = C.c_int
     return _libs[so]
 
 
@@ -91,6 +103,8 @@ def ref_kat():
     L.ref_bc_voxel_q19.argtypes = [C.c_uint, D, C.c_double, C.c_double, D]
     L.ref_bc_plates_q27.argtypes = [C.c_uint, D, C.c_double, D]
     L.ref_bc_plates_q19.argtypes = [C.c_uint, D, C.c_double, D]
+    L.ref_reconstruct_g19.argtypes = [C.c_double, D, D, D]
+    L.ref_rb_periodic_constants.argtypes = [D]
     for f in ("ref_bc_lid_q19", "ref_bc_voxel_q19", "ref_bc_plates_q27", "ref_bc_plates_q19"):
         getattr(L, f).restype = C.c_int
     return L
@@ -98,7 +112,8 @@ def ref_kat():
 
 def make_desc(nx, ny, nz, q=19, periodic=(1, 1, 1), tau=0.8, rho0=1.0, force=(0, 0, 0),
               bc_velocity=None, rheology=NEWTONIAN, n_index=1.0, k_consistency=0.0,
-              yield_stress=0.0, omega_p=0.0, exterior=None, bc_matrix_q=None):
+              yield_stress=0.0, omega_p=0.0, exterior=None, bc_matrix_q=None, thermal=None):
+    """thermal: None, or a dict with alpha, reference, gbeta (3), source, wall (4)."""
     d = OrcDesc()
     d.nx, d.ny, d.nz, d.q = nx, ny, nz, q
     for a in range(3):
@@ -115,6 +130,15 @@ def make_desc(nx, ny, nz, q=19, periodic=(1, 1, 1), tau=0.8, rho0=1.0, force=(0,
         for k in range(10):
             d.exterior[k] = float(exterior[k])
     d.bc_matrix_q = int(bc_matrix_q if bc_matrix_q is not None else (19 if q == 27 else q))
+    if thermal is not None:
+        d.thermal = 1
+        d.t_alpha = float(thermal["alpha"])
+        d.t_reference = float(thermal.get("reference", 1.0))
+        for a, v in enumerate(thermal.get("gbeta", (0, 0, 0))):
+            d.t_gbeta[a] = float(v)
+        d.t_source = float(thermal.get("source", 0.0))
+        for k, v in enumerate(thermal.get("wall", (1, 1, 1, 1))):
+            d.t_wall[k] = float(v)
     return d
 
 

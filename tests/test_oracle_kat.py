@@ -134,3 +134,49 @@ def test_fp32_build_is_the_same_algorithm_in_fp32():
     err = np.linalg.norm(mb[..., 1:4] - ma[..., 1:4]) / np.linalg.norm(ma[..., 1:4])
     assert 1e-9 < err < 1e-4, err
     assert np.array_equal(mb, mb.astype(np.float32).astype(np.float64))
+
+
+def test_thermal_reconstruction_golden():
+    """D3G19 populations of the thermal scalar against G_SCALAR/reconstruction.inc.
+    The snippet takes the diffusive correction ud directly; the oracle forms it
+    as coef (q3 / C - u3), so q3 is chosen to give the same ud."""
+    coef = 0.37
+    for row, ref in zip(GOLD["g19_in"], GOLD["g19_out"]):
+        c, u3, ud3 = row[0], np.ascontiguousarray(row[1:4]), row[4:7]
+        q3 = np.ascontiguousarray(c * (u3 + ud3 / coef))
+        g = np.zeros(19)
+        L.orc_reconstruct_g(coef, float(c), P(u3), P(q3), P(g))
+        np.testing.assert_allclose(g, ref, rtol=1e-12, atol=1e-15)
+
+
+def test_thermal_coefficient_golden():
+    """G_DIFF_FLUC_COEF from T_DIFFUSIVITY as the Rayleigh-Benard case computes it."""
+    rc = GOLD["rbp_const"]
+    assert abs(L.orc_thermal_coef(rc[1]) - rc[0]) < 1e-15
+    # T_gravity_t_beta = Ra alpha nu / (dT L^3) with Ra = 1e5, dT = 1, L = N = 64
+    assert abs(rc[2] - 1e5 * rc[1] * rc[3] / 64 ** 3) < 1e-18
+
+
+def test_thermal_sums_recover_moments():
+    """Sum g = C and 3 sum g c = C (u3 + coef (q3 / C - u3)): the scalar is
+    conserved by the reconstruction and its flux relaxes towards C u."""
+    rng = np.random.default_rng(11)
+    for _ in range(32):
+        c = rng.uniform(0.5, 1.5)
+        u3, q3 = rng.normal(0, 0.1, 3), rng.normal(0, 0.1, 3)
+        coef = rng.uniform(-0.99, 0.9)
+        g, cq = np.zeros(19), np.zeros(4)
+        L.orc_reconstruct_g(coef, c, P(u3), P(q3), P(g))
+        L.orc_sums_g(P(g), 0.0, P(cq))
+        np.testing.assert_allclose(cq[0], c, rtol=1e-14)
+        np.testing.assert_allclose(cq[1:], c * (u3 + coef * (q3 / c - u3)), rtol=1e-12, atol=1e-15)
+
+
+def test_thermal_face_normals():
+    side = C.c_int(0)
+    for name, axis, sd in (("WEST", 0, -1), ("EAST", 0, 1), ("SOUTH", 1, -1), ("NORTH", 1, 1), ("BACK", 2, -1),
+                           ("FRONT", 2, 1)):
+        assert L.orc_face_normal(lattice_np.FACES[name], C.byref(side)) == axis
+        assert side.value == sd
+    # an edge has two solid halves: no single normal
+    assert L.orc_face_normal(lattice_np.FACES["WEST"] | lattice_np.FACES["SOUTH"], C.byref(side)) == -1
