@@ -20,7 +20,9 @@
  *     and nz to be multiples of 8, like the reference.
  *   - Stored moments use the reference's scaled form (src/arrayIndex.h:8-17,
  *     186-187): rho-rho0, 3u, 4.5*Pi_xx, 9*Pi_xy, 9*Pi_xz, 4.5*Pi_yy, 9*Pi_yz,
- *     4.5*Pi_zz (+ omega as moment 10 when the viscosity is non-Newtonian).
+ *     4.5*Pi_zz (+ omega as moment 10 when the viscosity is non-Newtonian;
+ *     + C, 3 sum g c_x, 3 sum g c_y, 3 sum g c_z as moments 10-13 with the
+ *     thermal scalar).
  */
 #ifndef MRLBM_H
 #define MRLBM_H
@@ -56,6 +58,25 @@ typedef enum { MRLBM_NEWTONIAN = 0, MRLBM_POWERLAW = 1, MRLBM_BINGHAM = 2 } mrlb
 #define MRLBM_NODE_SOLID 0xFFu
 #define MRLBM_BC_VELOCITY_WALL (1u << 8)
 #define MRLBM_BC_VELOCITY_INDEX(k) (((uint32_t)(k) & 3u) << 11)
+/* Thermal rule of a boundary node (bits 13-14) and its wall value index into
+ * mrlbm_desc.t_wall (bits 15-16): the per-case g_bc_definition.inc switch of
+ * the reference, as run-time data.  Bulk nodes always take C = sum g + source.
+ *   0  C and its flux keep their stored values (node types the case's
+ *      g_bc_definition.inc does not list)
+ *   1  C = t_wall, flux 0 (src/cases/thermal_2D/g_bc_definition.inc)
+ *   2  C = t_wall, flux along the wall normal copied from the inward
+ *      neighbour's previous-step value, tangential flux 0
+ *      (src/cases/rayleighBenard_Periodic/g_bc_definition.inc EAST/WEST)
+ *   3  adiabatic: populations arriving from the solid side mirrored across the
+ *      wall plane, C and flux from the sums
+ *      (src/cases/rayleighBenard_Closed/g_bc_definition.inc NORTH/SOUTH)
+ * Rules 2 and 3 need a face node (one solid half of the octant mask). */
+#define MRLBM_THERMAL_KEEP 0u
+#define MRLBM_THERMAL_DIRICHLET 1u
+#define MRLBM_THERMAL_DIRICHLET_FLUX 2u
+#define MRLBM_THERMAL_ADIABATIC 3u
+#define MRLBM_THERMAL_RULE(r) (((uint32_t)(r) & 3u) << 13)
+#define MRLBM_THERMAL_INDEX(k) (((uint32_t)(k) & 3u) << 15)
 
 /* Run-time description of one domain: the physics that a reference case fixes
  * at compile time in constants.inc / model.inc (src/cases/<case>/). */
@@ -75,7 +96,20 @@ typedef struct {
     double nnf_omega_p;     /* Bingham plastic omega OMEGA_P (0: 1/tau) */
     int bc_matrix_q;        /* 0: reference behaviour (19 on D3Q27, i.e. the
                                D3Q19 wall closed forms), or 19 / 27 explicitly */
-    int reserved[7];
+    /* Thermal scalar C transported on D3G19 (constants.inc THERMAL_MODEL:
+     * SECOND_DIST + CONVECTION_DIFFUSION_TRANSPORT, src/mlbm.cu:157-191,
+     * 515-522, 603-616).  Four more stored moments follow the flow's: C and
+     * 3 sum g c (M2_C_INDEX, M2_CX..CZ_INDEX, src/arrayIndex.h:42-50).
+     * Supported on D3Q19, FP32 storage, Newtonian flow. */
+    int thermal;            /* 1: transport C */
+    double t_diffusivity;   /* T_DIFFUSIVITY (alpha); the relaxation uses the reference's
+                               G_DIFF_FLUC_COEF with T_DIFF_REF = 1/6 */
+    double t_reference;     /* T_REFERENCE: Boussinesq reference, initial and exterior C */
+    double t_gravity_beta[3]; /* gravity_vector * T_gravity_t_beta: bulk nodes get the force
+                               t_gravity_beta * rho0 * (C - t_reference) */
+    double t_source;        /* T_Q_INTERNAL_D_Cp, added to C at bulk nodes every step */
+    double t_wall[4];       /* wall temperatures by thermal value index (T_HOT, T_COLD, ...) */
+    int reserved[8];
 } mrlbm_desc;
 
 typedef struct mrlbm_domain mrlbm_domain;

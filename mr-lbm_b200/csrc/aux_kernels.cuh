@@ -46,7 +46,9 @@ struct InitArgs {
     const float *rho, *ux, *uy, *uz;  // device copies of x-fastest fields (kind 0)
     float u0[3];
     float tg_u0, tg_L;
-    float scale[11];
+    int thermal;  // moments 10..13 are C and its flux: C = c0, no flux
+    float c0;     // (the thermal cases' flow_initialization.inc: cVar = T_REFERENCE, q = 0)
+    float scale[NM_MAX];
 };
 
 template <int Q, typename T>
@@ -72,9 +74,14 @@ __global__ void init_kernel(const InitArgs a)
             uy = -U * cosf(x / L) * sinf(y / L) * cosf(z / L);
             uz = 0.0f;
         }
-        float m[11];
+        float m[NM_MAX];
         init_moments<Q>(rho, ux, uy, uz, a.rho0, a.qs, m);
-        m[10] = a.omega0;
+        if (a.thermal) {
+            m[10] = a.c0;
+            m[11] = m[12] = m[13] = 0.f;
+        } else {
+            m[10] = a.omega0;
+        }
         const long long idx = pidx(x, y, z, a.pitch, a.plane);
         T* p0 = reinterpret_cast<T*>(a.m0);
         T* p1 = reinterpret_cast<T*>(a.m1);
@@ -96,7 +103,7 @@ struct ConvArgs {
     int nx, ny, nz, pitch;
     long long plane, field;
     int nm, mode;
-    float scale[11], iscale[11];
+    float scale[NM_MAX], iscale[NM_MAX];
 };
 
 template <typename T>
@@ -141,8 +148,8 @@ struct GhostArgs {
     int nx, ny, nz, pitch;
     long long plane, field;
     int nm, periodic;
-    float ext[11];
-    float scale[11];
+    float ext[NM_MAX];
+    float scale[NM_MAX];
 };
 
 template <typename T>
@@ -195,7 +202,7 @@ struct RedArgs {
     long long plane, field;
     int nm;
     float rho0;
-    float iscale[11];
+    float iscale[NM_MAX];
     double* partial;
     double* out;
     int nblocks;

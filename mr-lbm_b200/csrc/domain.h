@@ -38,8 +38,8 @@ struct mrlbm_domain {
     mrlbm::BcClass* bc = nullptr;
     int nclasses = 0;
     bool has_bc = false;
-    float ext[11] = {};
-    float scale[11] = {}, iscale[11] = {};
+    float ext[mrlbm::NM_MAX] = {};
+    float scale[mrlbm::NM_MAX] = {}, iscale[mrlbm::NM_MAX] = {};
     int lz = 16;                     // z planes per CTA (batch members: per work item)
     int nsm = 148;                   // SMs of the device the domain lives on
     cudaStream_t stream = nullptr;
@@ -60,7 +60,7 @@ uint32_t known_mask(int q, uint32_t octants);
 mrlbm_status build_bc_class(int q, int mq, uint32_t word, const double uvel[4][3], double omega0, BcClass* out);
 mrlbm_status classify_nodes(int q, int mq, const uint32_t* nt, long long n, const double uvel[4][3], double omega0,
                             std::vector<uint8_t>& cls, std::vector<BcClass>& table, bool& any_bc,
-                            bool case_mode = false);
+                            bool case_mode = false, const double* t_wall = nullptr);
 void storage_scales(int storage, float* scale, float* iscale);
 mrlbm_status domain_alloc(mrlbm_domain* dom);
 int choose_lz(const mrlbm_domain* dom);

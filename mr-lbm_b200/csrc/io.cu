@@ -68,58 +68,82 @@ static void host_reconstruct(int q, float rho0, const float* m, float* f)
     }
 }
 
+// Host reconstruction of the thermal populations (same formula as the
+// device's): g_i = C w_i (1 + c_i . (u3 + coef (q3 / C - u3))), D3G19.
+static void host_reconstruct_g(float coef, const float* m, float* g)
+{
+    const float C = m[10], iC = 1.0f / C;
+    float v[3];
+    for (int a = 0; a < 3; a++) v[a] = m[1 + a] + coef * (m[11 + a] * iC - m[1 + a]);
+    for (int i = 0; i < 19; i++)
+        g[i] = C * (float)lat_w(19, i) * (1.0f + lat_cx(i) * v[0] + lat_cy(i) * v[1] + lat_cz(i) * v[2]);
+}
+
 // Ghost-face files of the reference (fGhost.{X,Y,Z}_{0,1}, layout idxPopX/Y/Z,
 // src/globalFunctions.h:45-124): the populations leaving each 8^3 block through
 // each face, face pops in increasing velocity index.  On a wall axis the faces
 // on the domain boundary hold the initial rest state, as in the reference
-// (they are never rewritten there, src/includeFiles/interface.h:6-19).
+// (they are never rewritten there, src/includeFiles/interface.h:6-19).  With
+// the thermal scalar the D3G19 populations go to g_fGhost.* the same way
+// (src/checkpoint.cu:188-194, GF = 5 per face).
 static mrlbm_status write_ghosts(mrlbm_domain* dom, const std::vector<float>& m, const std::string& base)
 {
     const mrlbm_desc& d = dom->d;
-    const int q = dom->q, qf = q == 19 ? 5 : 9;
     const int nbx = d.nx / 8, nby = d.ny / 8, nbz = d.nz / 8;
     const size_t n = (size_t)d.nx * d.ny * d.nz;
-    float fext[27];
-    host_reconstruct(q, (float)d.rho0, dom->ext, fext);
+    const int nm = dom->nm;
     static const char* names[6] = {"X_0", "X_1", "Y_0", "Y_1", "Z_0", "Z_1"};
-    for (int face = 0; face < 6; face++) {
-        const int axis = face / 2, side = face % 2;  // side 0: the -face (pops with c_axis = -1)
-        const int sgn = side ? 1 : -1;
-        std::vector<int> pops;
-        for (int i = 0; i < q; i++) {
-            const int c = axis == 0 ? lat_cx(i) : axis == 1 ? lat_cy(i) : lat_cz(i);
-            if (c == sgn) pops.push_back(i);
-        }
-        std::vector<float> buf((size_t)64 * qf * nbx * nby * nbz);
-        for (int bz = 0; bz < nbz; bz++)
-            for (int by = 0; by < nby; by++)
-                for (int bx = 0; bx < nbx; bx++)
-                    for (int b = 0; b < 8; b++)
-                        for (int a = 0; a < 8; a++) {
-                            int tx, ty, tz;
-                            const int t = side ? 7 : 0;
-                            if (axis == 0) { tx = t; ty = a; tz = b; }
-                            else if (axis == 1) { tx = a; ty = t; tz = b; }
-                            else { tx = a; ty = b; tz = t; }
-                            const int x = bx * 8 + tx, y = by * 8 + ty, z = bz * 8 + tz;
-                            const int coord = axis == 0 ? x : axis == 1 ? y : z;
-                            const int ncoord = axis == 0 ? d.nx : axis == 1 ? d.ny : d.nz;
-                            const bool wall_face = !d.periodic[axis] && coord == (side ? ncoord - 1 : 0);
-                            float f[27];
-                            if (wall_face) {
-                                memcpy(f, fext, sizeof(f));
-                            } else {
-                                float mm[10];
-                                const size_t node = (size_t)x + (size_t)d.nx * (y + (size_t)d.ny * z);
-                                for (int k = 0; k < 10; k++) mm[k] = m[k * n + node];
-                                host_reconstruct(q, (float)d.rho0, mm, f);
+    float coef = 0.f;
+    if (d.thermal) {
+        const double diff_ref = 1.0 / 6.0, aaa = 3.0 * (d.t_diffusivity - diff_ref) / (diff_ref * 3.0 + 0.5);
+        coef = (float)(aaa / (1.0 + aaa));
+    }
+    for (int dist = 0; dist < (d.thermal ? 2 : 1); dist++) {
+        const int q = dist ? 19 : dom->q, qf = q == 19 ? 5 : 9;
+        float mext[NM_MAX];
+        memcpy(mext, dom->ext, sizeof(mext));
+        float fext[27];
+        if (dist) host_reconstruct_g(coef, mext, fext); else host_reconstruct(q, (float)d.rho0, mext, fext);
+        for (int face = 0; face < 6; face++) {
+            const int axis = face / 2, side = face % 2;  // side 0: the -face (pops with c_axis = -1)
+            const int sgn = side ? 1 : -1;
+            std::vector<int> pops;
+            for (int i = 0; i < q; i++) {
+                const int c = axis == 0 ? lat_cx(i) : axis == 1 ? lat_cy(i) : lat_cz(i);
+                if (c == sgn) pops.push_back(i);
+            }
+            std::vector<float> buf((size_t)64 * qf * nbx * nby * nbz);
+            for (int bz = 0; bz < nbz; bz++)
+                for (int by = 0; by < nby; by++)
+                    for (int bx = 0; bx < nbx; bx++)
+                        for (int b = 0; b < 8; b++)
+                            for (int a = 0; a < 8; a++) {
+                                int tx, ty, tz;
+                                const int t = side ? 7 : 0;
+                                if (axis == 0) { tx = t; ty = a; tz = b; }
+                                else if (axis == 1) { tx = a; ty = t; tz = b; }
+                                else { tx = a; ty = b; tz = t; }
+                                const int x = bx * 8 + tx, y = by * 8 + ty, z = bz * 8 + tz;
+                                const int coord = axis == 0 ? x : axis == 1 ? y : z;
+                                const int ncoord = axis == 0 ? d.nx : axis == 1 ? d.ny : d.nz;
+                                const bool wall_face = !d.periodic[axis] && coord == (side ? ncoord - 1 : 0);
+                                float f[27];
+                                if (wall_face) {
+                                    memcpy(f, fext, sizeof(f));
+                                } else {
+                                    float mm[NM_MAX];
+                                    const size_t node = (size_t)x + (size_t)d.nx * (y + (size_t)d.ny * z);
+                                    for (int k = 0; k < nm; k++) mm[k] = m[k * n + node];
+                                    if (dist) host_reconstruct_g(coef, mm, f); else host_reconstruct(q, (float)d.rho0, mm, f);
+                                }
+                                const size_t blk = bx + (size_t)nbx * (by + (size_t)nby * bz);
+                                for (int p = 0; p < qf; p++)
+                                    buf[a + 8 * (b + 8 * (p + (size_t)qf * blk))] = f[pops[p]];
                             }
-                            const size_t blk = bx + (size_t)nbx * (by + (size_t)nby * bz);
-                            for (int p = 0; p < qf; p++)
-                                buf[a + 8 * (b + 8 * (p + (size_t)qf * blk))] = f[pops[p]];
-                        }
-        mrlbm_status st = write_file(base + "fGhost." + names[face] + ".bin", buf.data(), buf.size() * sizeof(float));
-        if (st) return st;
+            mrlbm_status st = write_file(base + (dist ? "g_fGhost." : "fGhost.") + names[face] + ".bin", buf.data(),
+                                         buf.size() * sizeof(float));
+            if (st) return st;
+        }
     }
     return MRLBM_OK;
 }
@@ -157,11 +181,12 @@ extern "C" mrlbm_status mrlbm_load_checkpoint(mrlbm_domain* dom, const char* pat
     // the ghost files hold populations this solver reconstructs from the
     // moments; their presence is checked for format compatibility only
     static const char* names[6] = {"X_0", "X_1", "Y_0", "Y_1", "Z_0", "Z_1"};
-    for (int f = 0; f < 6; f++) {
-        const std::string g = base + "fGhost." + names[f] + ".bin";
-        struct stat sb;
-        if (stat(g.c_str(), &sb) != 0) return fail(MRLBM_EIO, "missing ghost file '%s'", g.c_str());
-    }
+    for (int dist = 0; dist < (d.thermal ? 2 : 1); dist++)
+        for (int f = 0; f < 6; f++) {
+            const std::string g = base + (dist ? "g_fGhost." : "fGhost.") + names[f] + ".bin";
+            struct stat sb;
+            if (stat(g.c_str(), &sb) != 0) return fail(MRLBM_EIO, "missing ghost file '%s'", g.c_str());
+        }
     *step = s32 + 1;
     dom->step = s32 + 1;
     return MRLBM_OK;
@@ -182,6 +207,17 @@ static std::string var_filename(const char* path, const char* id, const char* va
     return s + std::to_string(step) + ext;
 }
 
+// the thermal scalar C (moment 10 of a thermal domain), x-fastest
+static mrlbm_status thermal_scalar(mrlbm_domain* dom, std::vector<float>& c)
+{
+    const size_t n = (size_t)dom->d.nx * dom->d.ny * dom->d.nz;
+    std::vector<float> all(n * dom->nm);
+    mrlbm_status st = mrlbm_get_moments(dom, all.data());
+    if (st) return st;
+    c.assign(all.begin() + 10 * n, all.begin() + 11 * n);
+    return MRLBM_OK;
+}
+
 extern "C" mrlbm_status mrlbm_save_macr_bin(mrlbm_domain* dom, const char* path_files, const char* id_sim, int step)
 {
     if (!dom || !path_files || !id_sim) return fail(MRLBM_EINVAL, "null argument");
@@ -189,24 +225,29 @@ extern "C" mrlbm_status mrlbm_save_macr_bin(mrlbm_domain* dom, const char* path_
     const size_t n = (size_t)d.nx * d.ny * d.nz;
     mrlbm_status st = mkdirs(std::string(path_files) + "/" + id_sim);
     if (st) return st;
-    std::vector<float> rho(n), ux(n), uy(n), uz(n), om;
-    if (dom->nm > 10) om.resize(n);
-    if ((st = mrlbm_get_macr(dom, rho.data(), ux.data(), uy.data(), uz.data(), dom->nm > 10 ? om.data() : nullptr)))
+    const bool has_om = d.rheology != MRLBM_NEWTONIAN;
+    std::vector<float> rho(n), ux(n), uy(n), uz(n), om, cv;
+    if (has_om) om.resize(n);
+    if ((st = mrlbm_get_macr(dom, rho.data(), ux.data(), uy.data(), uz.data(), has_om ? om.data() : nullptr)))
         return st;
+    if (d.thermal && (st = thermal_scalar(dom, cv))) return st;
     const unsigned s = (unsigned)step;
     if ((st = write_file(var_filename(path_files, id_sim, "rho", s, ".bin"), rho.data(), n * 4))) return st;
     if ((st = write_file(var_filename(path_files, id_sim, "ux", s, ".bin"), ux.data(), n * 4))) return st;
     if ((st = write_file(var_filename(path_files, id_sim, "uy", s, ".bin"), uy.data(), n * 4))) return st;
     if ((st = write_file(var_filename(path_files, id_sim, "uz", s, ".bin"), uz.data(), n * 4))) return st;
-    if (dom->nm > 10)
+    if (has_om)
         if ((st = write_file(var_filename(path_files, id_sim, "omega", s, ".bin"), om.data(), n * 4))) return st;
+    // SECOND_DIST: <id>_C<step>.bin (src/saveData.cu:192-193, 229-230)
+    if (d.thermal)
+        if ((st = write_file(var_filename(path_files, id_sim, "C", s, ".bin"), cv.data(), n * 4))) return st;
     return MRLBM_OK;
 }
 
 // Legacy VTK structured-points file, binary (big-endian floats), as
 // saveVarVTK writes it (src/saveData.cu:303-400): SCALARS rho (rho0 + m0),
-// VECTORS velocity (physical u, the stored 3u divided by 3), and SCALARS omega
-// when the domain carries an omega field.  File <path>/<id>/<id>_vtk<step>.vtk
+// VECTORS velocity (physical u, the stored 3u divided by 3), SCALARS omega
+// when the domain carries an omega field and SCALARS C with the thermal scalar.  File <path>/<id>/<id>_vtk<step>.vtk
 // (src/saveData.cu:153).  The reference's optional node-type and BC-force
 // sections (NODE_TYPE_SAVE, SAVE_BC_FORCES) are not written.
 static void put_be(std::string& out, const float* v, size_t n)
@@ -228,10 +269,12 @@ extern "C" mrlbm_status mrlbm_save_vtk(mrlbm_domain* dom, const char* path_files
     const size_t n = (size_t)d.nx * d.ny * d.nz;
     mrlbm_status st = mkdirs(std::string(path_files) + "/" + id_sim);
     if (st) return st;
-    std::vector<float> rho(n), ux(n), uy(n), uz(n), om;
-    if (dom->nm > 10) om.resize(n);
-    if ((st = mrlbm_get_macr(dom, rho.data(), ux.data(), uy.data(), uz.data(), dom->nm > 10 ? om.data() : nullptr)))
+    const bool has_om = d.rheology != MRLBM_NEWTONIAN;
+    std::vector<float> rho(n), ux(n), uy(n), uz(n), om, cv;
+    if (has_om) om.resize(n);
+    if ((st = mrlbm_get_macr(dom, rho.data(), ux.data(), uy.data(), uz.data(), has_om ? om.data() : nullptr)))
         return st;
+    if (d.thermal && (st = thermal_scalar(dom, cv))) return st;
     std::string out;
     out.reserve(n * 16 + 512);
     char head[512];
@@ -252,9 +295,13 @@ extern "C" mrlbm_status mrlbm_save_vtk(mrlbm_domain* dom, const char* path_files
         }
         put_be(out, v.data(), 3 * n);
     }
-    if (dom->nm > 10) {
+    if (has_om) {
         out += "SCALARS omega float 1\nLOOKUP_TABLE default\n";
         put_be(out, om.data(), n);
+    }
+    if (d.thermal) {  // src/saveData.cu:371-376
+        out += "SCALARS C float 1\nLOOKUP_TABLE default\n";
+        put_be(out, cv.data(), n);
     }
     return write_file(var_filename(path_files, id_sim, "vtk", (unsigned)step, ".vtk"), out.data(), out.size());
 }

@@ -48,7 +48,11 @@ enum : int {
     F_FORCE = 2,     // non-zero body force
     F_POWERLAW = 4,  // omega field, power-law viscosity
     F_BINGHAM = 8,   // omega field, Bingham viscosity
+    F_THERMAL = 16,  // thermal scalar C on D3G19 (4 more stored moments, Boussinesq force)
 };
+
+// most stored moments per node: 10 flow moments + omega, or + C and its flux
+constexpr int NM_MAX = 14;
 
 constexpr int TILE_X = 30;   // interior nodes per warp row
 constexpr int XOFF = 4;      // padded column of x = 0 (x = -1 is the ghost column)
@@ -83,13 +87,16 @@ struct alignas(16) BcClass {
     uint32_t known;    // bit i: population i is known (incoming from fluid)
     uint32_t valid;
     uint32_t word;     // the node-type word of the class (nodeTypeMap encoding)
-    uint32_t pad[2];
+    uint32_t trule;    // thermal rule (bits 0-1), wall normal axis (bits 2-3, 3 = none),
+                       // solid side of the normal (bit 4: + side)
+    float twall;       // thermal wall value
 };
 static_assert(sizeof(BcClass) == 288, "BcClass is read as float4 words");
 
 struct StepArgs {
     void* __restrict__ m_out;         // padded planes [nm][nz+2][ny+2][pitch]
-    void* out_p[6];                   // plane stack of moment pair p (moments 2p, 2p+1)
+    void* out_p[(NM_MAX + 1) / 2];    // plane stack of moment pair p (moments 2p, 2p+1)
+    const float* __restrict__ m_in;   // the buffer being read (thermal wall rules read it)
     const uint8_t* __restrict__ cls;  // padded [nz+2][ny+2][pitch]
     const BcClass* __restrict__ bc;
     int* err;                         // bit 0: a bounded wait timed out
@@ -101,8 +108,12 @@ struct StepArgs {
     float rho0, omega0;
     float fx, fy, fz;
     float nnf_n, nnf_k, nnf_yield, nnf_omega_p;
-    float scale[11];   // storage scale per moment (1 for fp32)
-    float iscale[11];
+    float t_coef;      // thermal: G_DIFF_FLUC_COEF
+    float t_ref;       // thermal: T_REFERENCE
+    float t_gb[3];     // thermal: t_gravity_beta * rho0
+    float t_src;       // thermal: source added to C at bulk nodes
+    float scale[NM_MAX];   // storage scale per moment (1 for fp32)
+    float iscale[NM_MAX];
 };
 
 __host__ __device__ __forceinline__ long long pidx(int x, int y, int z, int pitch, long long plane)
@@ -409,11 +420,10 @@ __device__ __forceinline__ float nnf_powerlaw(float omega_old, float smag, float
 template <int FLAGS>
 __device__ __forceinline__ void collide_scaled(const StepArgs& a, float rho, float ux, float uy, float uz, float mxx,
                                                float mxy, float mxz, float myy, float myz, float mzz, float omega,
-                                               float* out)
+                                               float* out, float Fx, float Fy, float Fz)
 {
     const float t_om = 1.0f - omega, om_d2 = 0.5f * omega;
     if constexpr ((FLAGS & F_FORCE) != 0) {
-        const float Fx = a.fx, Fy = a.fy, Fz = a.fz;
         const float ir = 1.0f / rho;
         const float tt_om = 1.0f - 0.5f * omega;
         ux += 3.0f * ir * Fx;
@@ -442,13 +452,11 @@ __device__ __forceinline__ void collide_scaled(const StepArgs& a, float rho, flo
 
 // Scale to the stored form, update omega (non-Newtonian), collide.
 template <int FLAGS>
-__device__ __forceinline__ void collide(const StepArgs& a, const float* mac, float omega, float* out)
+__device__ __forceinline__ void collide(const StepArgs& a, const float* mac, float omega, float* out, float Fx, float Fy,
+                                        float Fz)
 {
     const float rho = mac[0];
     if constexpr ((FLAGS & (F_POWERLAW | F_BINGHAM)) != 0) {
-        const float Fx = (FLAGS & F_FORCE) ? a.fx : 0.f;
-        const float Fy = (FLAGS & F_FORCE) ? a.fy : 0.f;
-        const float Fz = (FLAGS & F_FORCE) ? a.fz : 0.f;
         // shear magnitude from the non-equilibrium second moments, src/mlbm.cu:526-546
         const float sxx = rho * (mac[4] - mac[1] * mac[1]), syy = rho * (mac[7] - mac[2] * mac[2]);
         const float szz = rho * (mac[9] - mac[3] * mac[3]), sxy = rho * (mac[5] - mac[1] * mac[2]);
@@ -464,7 +472,7 @@ __device__ __forceinline__ void collide(const StepArgs& a, const float* mac, flo
             omega = a.nnf_omega_p * fmaxf(0.f, 1.0f - a.nnf_yield / smag);
     }
     collide_scaled<FLAGS>(a, rho, 3.0f * mac[1], 3.0f * mac[2], 3.0f * mac[3], 4.5f * mac[4], 9.0f * mac[5],
-                          9.0f * mac[6], 4.5f * mac[7], 9.0f * mac[8], 4.5f * mac[9], omega, out);
+                          9.0f * mac[6], 4.5f * mac[7], 9.0f * mac[8], 4.5f * mac[9], omega, out, Fx, Fy, Fz);
 }
 
 // ---------------------------------------------------- TMA / mbarrier helpers
@@ -599,9 +607,10 @@ __device__ __forceinline__ void ex_read(float* g, const float4* e4t)
 // sp: this thread's element pair of moments 0, 1 in the plane's TMA stage
 // (pair p is 2 BOX_X elements further); e4t / e1t: this thread's exchange
 // slots in the buffer this production writes.
-template <int Q, int NM, typename T, int TYI>
+template <int Q, int NM, typename T, int TYI, bool TH = false>
 __device__ __forceinline__ void prod_a(const StepArgs& a, const T* sp, float4* e4t, float* e1t, float (&gsh)[Q],
-                                       float& om_node)
+                                       float& om_node, float4* e4g = nullptr, float* e1g = nullptr,
+                                       float* gshg = nullptr)
 {
     constexpr int NW = TYI + 2;
     float mc[NM];
@@ -635,6 +644,98 @@ __device__ __forceinline__ void prod_a(const StepArgs& a, const T* sp, float4* e
         }
     });
     om_node = mc[NM - 1];
+    if constexpr (TH) {
+        // thermal populations on D3G19 (the D3Q19 directions and weights):
+        // g_i = C w_i (1 + c_i . (u3 + ud3)), ud3 = coef (q3 / C - u3) with the
+        // node's stored flow velocity u3 = 3u and flux q3 = 3 sum g c
+        // (src/colrec/G_SCALAR/reconstruction.inc:1-25, src/mlbm.cu:159-169)
+        const float C = mc[10], iC = 1.0f / C;
+        const float vx = fmaf(a.t_coef, fmaf(mc[11], iC, -mc[1]), mc[1]);
+        const float vy = fmaf(a.t_coef, fmaf(mc[12], iC, -mc[2]), mc[2]);
+        const float vz = fmaf(a.t_coef, fmaf(mc[13], iC, -mc[3]), mc[3]);
+        float g[19];
+        static_for<0, 19>([&](auto I) {
+            constexpr int i = I;
+            float t = 1.0f;
+            if constexpr (lat_cx(i) > 0) t += vx; else if constexpr (lat_cx(i) < 0) t -= vx;
+            if constexpr (lat_cy(i) > 0) t += vy; else if constexpr (lat_cy(i) < 0) t -= vy;
+            if constexpr (lat_cz(i) > 0) t += vz; else if constexpr (lat_cz(i) < 0) t -= vz;
+            g[i] = (C * (float)lat_w(19, i)) * t;
+        });
+        ex_write<19, 0, NW>(g, e4g);
+        ex_write<19, 1, NW>(g, e4g);
+        ex_write<19, 2, NW>(g, e4g);
+        ex_write<19, 3, NW>(g, e4g);
+        ex_write<19, 4, NW>(g, e4g);
+        ex_write<19, 5, NW>(g, e4g);
+        static_for<1, 19>([&](auto I) {
+            constexpr int i = I;
+            if constexpr (lat_cy(i) != 0 && !ex_packed(19, i)) e1g[ex_scalar_slot(i) * Exchange<19, NW>::plane] = g[i];
+        });
+        static_for<0, 19>([&](auto I) {
+            constexpr int i = I;
+            if constexpr (lat_cy(i) == 0) {
+                if constexpr (lat_cx(i) > 0) gshg[i] = __shfl_up_sync(0xffffffffu, g[i], 1);
+                else if constexpr (lat_cx(i) < 0) gshg[i] = __shfl_down_sync(0xffffffffu, g[i], 1);
+                else gshg[i] = g[i];
+            }
+        });
+    }
+}
+
+// D3Q19 direction with component `axis` of direction i negated
+__host__ __device__ constexpr int lat_mirror19(int i, int axis)
+{
+    const int cx = axis == 0 ? -lat_cx(i) : lat_cx(i);
+    const int cy = axis == 1 ? -lat_cy(i) : lat_cy(i);
+    const int cz = axis == 2 ? -lat_cz(i) : lat_cz(i);
+    return lat_find(19, cx, cy, cz);
+}
+
+// C and 3 sum g c at a boundary node of a thermal domain, by the class's rule
+// (include/mrlbm.h MRLBM_THERMAL_*; the reference's per-case
+// g_bc_definition.inc, e.g. src/cases/rayleighBenard_Periodic/g_bc_definition.inc,
+// src/cases/rayleighBenard_Closed/g_bc_definition.inc).  pg: the streamed
+// populations; values "from the previous step" come from the buffer this step
+// reads (the reference reads its in-place buffer, whose neighbour entries may
+// or may not have been updated already).
+__device__ __forceinline__ void thermal_wall(const StepArgs& a, const BcClass* __restrict__ c, const float* pg,
+                                             unsigned oidx, float& C, float* q)
+{
+    const uint32_t tr = c->trule;
+    const int rule = (int)(tr & 3u), axis = (int)((tr >> 2) & 3u);
+    const int side = (tr >> 4) & 1u ? 1 : -1;
+    if (rule == 0) {
+        // the stored values stand (node types without a thermal rule)
+        C = a.m_in[mphys(10, oidx, a.field)];
+        for (int k = 0; k < 3; k++) q[k] = a.m_in[mphys(11 + k, oidx, a.field)];
+    } else if (rule == 1 || axis == 3) {
+        C = c->twall;
+        q[0] = q[1] = q[2] = 0.f;
+    } else if (rule == 2) {
+        // normal flux of the inward neighbour
+        C = c->twall;
+        q[0] = q[1] = q[2] = 0.f;
+        const long long stride = axis == 0 ? 1LL : (axis == 1 ? (long long)a.pitch : a.plane);
+        const long long nb = (long long)oidx - side * stride;
+        q[axis] = a.m_in[mphys(11 + axis, nb, a.field)];
+    } else {
+        // adiabatic: what arrives from the solid side is the mirror image of
+        // what leaves towards it
+        float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+        static_for<0, 19>([&](auto I) {
+            constexpr int i = I;
+            const int ca = axis == 0 ? lat_cx(i) : (axis == 1 ? lat_cy(i) : lat_cz(i));
+            const float mv = axis == 0 ? pg[lat_mirror19(i, 0)] : (axis == 1 ? pg[lat_mirror19(i, 1)] : pg[lat_mirror19(i, 2)]);
+            const float v = ca == -side ? mv : pg[i];
+            s0 += v;
+            if constexpr (lat_cx(i) > 0) s1 += v; else if constexpr (lat_cx(i) < 0) s1 -= v;
+            if constexpr (lat_cy(i) > 0) s2 += v; else if constexpr (lat_cy(i) < 0) s2 -= v;
+            if constexpr (lat_cz(i) > 0) s3 += v; else if constexpr (lat_cz(i) < 0) s3 -= v;
+        });
+        C = s0;
+        q[0] = 3.0f * s1; q[1] = 3.0f * s2; q[2] = 3.0f * s3;
+    }
 }
 
 // store of the node at padded offset idx (< 2^32: a domain's moment field is
@@ -666,9 +767,35 @@ __device__ __forceinline__ void store_node(const StepArgs& a, long long idx, con
 template <int Q, int NM, int NUP, int NMID, typename T, int FLAGS, int TYI, typename BCP>
 __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const float4* e4t, const float* e1t,
                                        bool interior, int x, int y, const float (&gsh)[Q], float (&up_old)[NUP],
-                                       float (&mid)[NMID], float om_out)
+                                       float (&mid)[NMID], float om_out, const float4* e4g = nullptr,
+                                       const float* e1g = nullptr, const float* gshg = nullptr,
+                                       float* upg_old = nullptr, float* midg = nullptr)
 {
     constexpr int NW = TYI + 2;
+    constexpr bool TH = (FLAGS & F_THERMAL) != 0;
+    // thermal populations arriving at the node (same three sources as the flow's)
+    float gg[19], pg[19];
+    if constexpr (TH) {
+        ex_read<19, 0, NW>(gg, e4g);
+        ex_read<19, 1, NW>(gg, e4g);
+        ex_read<19, 2, NW>(gg, e4g);
+        ex_read<19, 3, NW>(gg, e4g);
+        ex_read<19, 4, NW>(gg, e4g);
+        ex_read<19, 5, NW>(gg, e4g);
+        static_for<1, 19>([&](auto I) {
+            constexpr int i = I;
+            if constexpr (lat_cy(i) != 0 && !ex_packed(19, i))
+                gg[i] = e1g[ex_scalar_slot(i) * Exchange<19, NW>::plane - lat_cy(i) * EX_COLS - lat_cx(i)];
+        });
+        static_for<0, 19>([&](auto I) {
+            constexpr int i = I;
+            if constexpr (lat_cy(i) == 0) gg[i] = gshg[i];
+            constexpr int slot = lat_cz_slot(19, i);
+            if constexpr (lat_cz(i) > 0) pg[i] = upg_old[slot];
+            else if constexpr (lat_cz(i) == 0) pg[i] = midg[slot];
+            else pg[i] = gg[i];
+        });
+    }
     float g[Q];
     ex_read<Q, 0, NW>(g, e4t);
     ex_read<Q, 1, NW>(g, e4t);
@@ -707,16 +834,41 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
         const unsigned oidx = (unsigned)(zd + 1) * (unsigned)a.plane + (unsigned)((y + 1) * a.pitch + x + XOFF);
         uint8_t cls = CLS_BULK;
         if constexpr ((FLAGS & F_BC) != 0) cls = live ? __ldg(a.cls + oidx) : CLS_SOLID;
-        float o[11];
+        float o[NM_MAX];
         float r, j[3], P[6];
         lattice_sums<Q>(p, r, j, P);
+        float Fx = 0.f, Fy = 0.f, Fz = 0.f;
+        if constexpr ((FLAGS & F_FORCE) != 0) { Fx = a.fx; Fy = a.fy; Fz = a.fz; }
+        float tC = 0.f, tq[3] = {0.f, 0.f, 0.f};
+        if constexpr (TH) {
+            // C = sum g + source, q3 = 3 sum g c at bulk nodes (src/mlbm.cu:180-188) and
+            // the Boussinesq force there (src/mlbm.cu:515-522); walls by their rule
+            if (cls == CLS_BULK) {
+                float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+                static_for<0, 19>([&](auto I) {
+                    constexpr int i = I;
+                    s0 += pg[i];
+                    if constexpr (lat_cx(i) > 0) s1 += pg[i]; else if constexpr (lat_cx(i) < 0) s1 -= pg[i];
+                    if constexpr (lat_cy(i) > 0) s2 += pg[i]; else if constexpr (lat_cy(i) < 0) s2 -= pg[i];
+                    if constexpr (lat_cz(i) > 0) s3 += pg[i]; else if constexpr (lat_cz(i) < 0) s3 -= pg[i];
+                });
+                tC = s0 + a.t_src;
+                tq[0] = 3.0f * s1; tq[1] = 3.0f * s2; tq[2] = 3.0f * s3;
+                const float dC = tC - a.t_ref;
+                Fx = fmaf(a.t_gb[0], dC, Fx);
+                Fy = fmaf(a.t_gb[1], dC, Fy);
+                Fz = fmaf(a.t_gb[2], dC, Fz);
+            } else if (cls != CLS_SOLID) {
+                thermal_wall(a, a.bc + cls, pg, oidx, tC, tq);
+            }
+        }
         if constexpr ((FLAGS & (F_BC | F_POWERLAW | F_BINGHAM)) == 0) {
             // bulk-only domains: the moments straight in the stored scaling
             // (3u = 3 j / rho, 4.5 Pi_ii = 4.5 P_ii / rho - 1.5, 9 Pi_ij)
             const float ir = 1.0f / r;
             const float i3 = 3.0f * ir, i45 = 4.5f * ir, i9 = 9.0f * ir;
             collide_scaled<FLAGS>(a, r, j[0] * i3, j[1] * i3, j[2] * i3, fmaf(P[0], i45, -1.5f), P[1] * i9, P[2] * i9,
-                                  fmaf(P[3], i45, -1.5f), P[4] * i9, fmaf(P[5], i45, -1.5f), omega, o);
+                                  fmaf(P[3], i45, -1.5f), P[4] * i9, fmaf(P[5], i45, -1.5f), omega, o, Fx, Fy, Fz);
         } else {
             float mac[10];
             const float ir = 1.0f / r;
@@ -731,7 +883,11 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
             if constexpr ((FLAGS & F_BC) != 0) {
                 if (cls != CLS_BULK && cls != CLS_SOLID) BCP::template apply<Q>(a, cls, p, omega, x, y, zd, mac);
             }
-            collide<FLAGS>(a, mac, omega, o);
+            collide<FLAGS>(a, mac, omega, o, Fx, Fy, Fz);
+        }
+        if constexpr (TH) {
+            o[10] = tC;
+            o[11] = tq[0]; o[12] = tq[1]; o[13] = tq[2];
         }
         if constexpr (!is_f32<T>()) {
 #pragma unroll
@@ -781,6 +937,14 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
         if constexpr (lat_cz(i) > 0) up_old[slot] = g[i];
         else if constexpr (lat_cz(i) == 0) mid[slot] = g[i];
     });
+    if constexpr (TH) {
+        static_for<0, 19>([&](auto I) {
+            constexpr int i = I;
+            constexpr int slot = lat_cz_slot(19, i);
+            if constexpr (lat_cz(i) > 0) upg_old[slot] = gg[i];
+            else if constexpr (lat_cz(i) == 0) midg[slot] = gg[i];
+        });
+    }
 }
 
 // Shared-memory carve-up used by every z-march kernel: barriers, TMA ring,
@@ -788,28 +952,38 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
 // switch between flag sets at run time size them for the largest set), and
 // the ring has NSTAGE_MAX stages when they fit next to the exchange buffers,
 // else one fewer.
-template <int Q, typename T, int TYI, int NPM>
+template <int Q, typename T, int TYI, int NPM, bool TH = false>
 struct ZSmem {
     static constexpr int NW = TYI + 2;
     static constexpr size_t stage_max = ((size_t)NW * NPM * 2 * BOX_X * sizeof(T) + 127) / 128 * 128;
-    static constexpr size_t ex_bytes = 2 * Exchange<Q, NW>::bytes_per_buffer;
+    // the thermal populations have a row exchange of their own (D3Q19 layout)
+    static constexpr size_t ex_bytes =
+        2 * Exchange<Q, NW>::bytes_per_buffer + (TH ? 2 * Exchange<19, NW>::bytes_per_buffer : 0);
     static constexpr int NS = 128 + NSTAGE_MAX * stage_max + ex_bytes <= 232448 ? NSTAGE_MAX : NSTAGE_MAX - 1;
     static constexpr size_t bytes = 128 + NS * stage_max + ex_bytes;
     uint64_t* bars;
     unsigned char* stages;
     float4* ex4;
     float* ex1;
+    float4* exg4;   // thermal exchange (TH only)
+    float* exg1;
     __device__ __forceinline__ explicit ZSmem(unsigned char* smem)
     {
         bars = reinterpret_cast<uint64_t*>(smem);
         stages = smem + 128;
         ex4 = reinterpret_cast<float4*>(stages + NS * stage_max);
         ex1 = reinterpret_cast<float*>(ex4 + 2 * Exchange<Q, NW>::buf4);
+        exg4 = reinterpret_cast<float4*>(ex1 + 2 * Exchange<Q, NW>::buf1);
+        exg1 = reinterpret_cast<float*>(exg4 + 2 * Exchange<19, NW>::buf4);
     }
 };
 
-// moment pairs of a flag set
-__host__ __device__ constexpr int npairs_of(int flags) { return (flags & (F_POWERLAW | F_BINGHAM)) ? 6 : 5; }
+// stored moments and moment pairs of a flag set
+__host__ __device__ constexpr int nmoments_of(int flags)
+{
+    return ((flags & (F_POWERLAW | F_BINGHAM)) ? 11 : 10) + ((flags & F_THERMAL) ? 4 : 0);
+}
+__host__ __device__ constexpr int npairs_of(int flags) { return (nmoments_of(flags) + 1) / 2; }
 
 // Per-CTA pipeline state and the loop of the z-march over one column.  The
 // TMA ring is indexed by a running production count `g0 + k` so a persistent
@@ -820,12 +994,13 @@ struct ZMarch {
     static constexpr int NUP = lat_num_cz(Q, 1);
     static constexpr int NMID = lat_num_cz(Q, 0);
     static constexpr bool OMF = (FLAGS & (F_POWERLAW | F_BINGHAM)) != 0;
-    static constexpr int NM = OMF ? 11 : 10;
+    static constexpr bool TH = (FLAGS & F_THERMAL) != 0;
+    static constexpr int NM = nmoments_of(FLAGS);
     static constexpr int NP = (NM + 1) / 2;  // moment pairs in a stage row
     static constexpr size_t stage_bytes = (size_t)NW * NP * 2 * BOX_X * sizeof(T);
     static constexpr size_t stage_al = (stage_bytes + 127) / 128 * 128;
     using EX = Exchange<Q, NW>;
-    using SM = ZSmem<Q, T, TYI, NPM>;
+    using SM = ZSmem<Q, T, TYI, NPM, TH>;
     static constexpr int NS = SM::NS;
     static_assert(NP <= NPM, "ring slots sized for fewer moment pairs");
 
@@ -841,6 +1016,8 @@ struct ZMarch {
     bool interior;
     int cs;           // ring slot of the next production to wait for
     unsigned cph;     // its mbarrier phase parity
+    float4* e4g[2];   // thermal: this thread's exchange slots, buffer 0 and 1
+    float* e1g[2];
 
     __device__ __forceinline__ int slot(int k) const { return (int)((g0 + (unsigned)k) % NS); }
     __device__ __forceinline__ unsigned phase(int k) const { return ((g0 + (unsigned)k) / NS) & 1u; }
@@ -878,7 +1055,8 @@ struct ZMarch {
     // in the CTA.
     template <int PAR>
     __device__ __forceinline__ bool iter(int j, float (&gsh_new)[Q], const float (&gsh_old)[Q], float (&up)[NUP],
-                                         float (&mid)[NMID], float& om_par)
+                                         float (&mid)[NMID], float& om_par, float* sg_new = nullptr,
+                                         const float* sg_old = nullptr, float* upg = nullptr, float* midg = nullptr)
     {
         const bool ok = mbar_wait(&bars[cs], cph);
         const float om_out = om_par;
@@ -888,12 +1066,14 @@ struct ZMarch {
         // production first 4 % faster on D3Q19 domains with walls
         if constexpr (Q == 27 || (FLAGS & F_BC) == 0) {
             prod_b<Q, NM, NUP, NMID, T, FLAGS, TYI, BCP>(a, j - 1, z0 - 2 + j, e4t[PAR ^ 1], e1t[PAR ^ 1], interior, x,
-                                                    y, gsh_old, up, mid, om_out);
-            prod_a<Q, NM, T, TYI>(a, stage_ptr(), e4t[PAR], e1t[PAR], gsh_new, om_par);
+                                                    y, gsh_old, up, mid, om_out, e4g[PAR ^ 1], e1g[PAR ^ 1], sg_old,
+                                                    upg, midg);
+            prod_a<Q, NM, T, TYI, TH>(a, stage_ptr(), e4t[PAR], e1t[PAR], gsh_new, om_par, e4g[PAR], e1g[PAR], sg_new);
         } else {
-            prod_a<Q, NM, T, TYI>(a, stage_ptr(), e4t[PAR], e1t[PAR], gsh_new, om_par);
+            prod_a<Q, NM, T, TYI, TH>(a, stage_ptr(), e4t[PAR], e1t[PAR], gsh_new, om_par, e4g[PAR], e1g[PAR], sg_new);
             prod_b<Q, NM, NUP, NMID, T, FLAGS, TYI, BCP>(a, j - 1, z0 - 2 + j, e4t[PAR ^ 1], e1t[PAR ^ 1], interior, x,
-                                                    y, gsh_old, up, mid, om_out);
+                                                    y, gsh_old, up, mid, om_out, e4g[PAR ^ 1], e1g[PAR ^ 1], sg_old,
+                                                    upg, midg);
         }
         if (__syncthreads_or(!ok)) return false;
         advance(j);
@@ -906,7 +1086,8 @@ struct ZMarch {
 // false when a bounded wait timed out (the CTA must stop).
 template <int Q, typename T, int FLAGS, int TYI, typename BCP = TableBC, int NPM>
 __device__ __forceinline__ bool zmarch_column(const StepArgs& a, const CUtensorMap* map, int X0, int Y0, int z0,
-                                              int zend, const ZSmem<Q, T, TYI, NPM>& sm, unsigned& g0)
+                                              int zend, const ZSmem<Q, T, TYI, NPM, (FLAGS & F_THERMAL) != 0>& sm,
+                                              unsigned& g0)
 {
     using ZM = ZMarch<Q, T, FLAGS, TYI, BCP, NPM>;
     constexpr int NUP = ZM::NUP, NMID = ZM::NMID;
@@ -923,7 +1104,9 @@ __device__ __forceinline__ bool zmarch_column(const StepArgs& a, const CUtensorM
           g0, warp * ZM::NP * 2 * BOX_X + 2 * ((x + XOFF) - p0), x, y, z0, Y0, p0,
           zend - z0 + 2 /* planes z0-1 .. zend */,
           lane >= 1 && lane <= TILE_X && x < a.nx && warp >= 1 && warp <= TYI && y < a.ny,
-          0, 0u};
+          0, 0u,
+          {sm.exg4 + ts, sm.exg4 + Exchange<19, ZM::NW>::buf4 + ts},
+          {sm.exg1 + ts, sm.exg1 + Exchange<19, ZM::NW>::buf1 + ts}};
     zm.cs = zm.slot(0);
     zm.cph = zm.phase(0);
 
@@ -939,12 +1122,20 @@ __device__ __forceinline__ bool zmarch_column(const StepArgs& a, const CUtensorM
 #pragma unroll
     for (int s = 0; s < NMID; s++) mid[s] = 0.f;
     float omA = a.omega0, omB = a.omega0;
+    // thermal populations: the same pipeline on the D3Q19 directions
+    constexpr int NUPG = ZM::TH ? lat_num_cz(19, 1) : 1, NMIDG = ZM::TH ? lat_num_cz(19, 0) : 1;
+    constexpr int NSG = ZM::TH ? 19 : 1;
+    float ugA[NUPG], ugB[NUPG], mg[NMIDG], sgA[NSG], sgB[NSG];
+#pragma unroll
+    for (int s = 0; s < NUPG; s++) ugA[s] = ugB[s] = 0.f;
+#pragma unroll
+    for (int s = 0; s < NMIDG; s++) mg[s] = 0.f;
 
     int kfail = -1;
     {
         // prologue: production 0 only (exchange buffer 0)
         const bool ok = mbar_wait(&sm.bars[zm.cs], zm.cph);
-        prod_a<Q, ZM::NM, T, TYI>(a, zm.stage_ptr(), zm.e4t[0], zm.e1t[0], gA, omA);
+        prod_a<Q, ZM::NM, T, TYI, ZM::TH>(a, zm.stage_ptr(), zm.e4t[0], zm.e1t[0], gA, omA, zm.e4g[0], zm.e1g[0], sgA);
         if (__syncthreads_or(!ok)) kfail = 0;
         else zm.advance(0);
     }
@@ -956,17 +1147,17 @@ __device__ __forceinline__ bool zmarch_column(const StepArgs& a, const CUtensorM
         // of production j-2, whose omega has the parity of j
         if (j >= zm.nprod) {  // j odd: last production even
             prod_b<Q, ZM::NM, NUP, NMID, T, FLAGS, TYI, BCP>(a, j - 1, z0 - 2 + j, zm.e4t[0], zm.e1t[0], zm.interior, x,
-                                                        y, gA, upA, mid, omB);
+                                                        y, gA, upA, mid, omB, zm.e4g[0], zm.e1g[0], sgA, ugA, mg);
             break;
         }
-        if (!zm.template iter<1>(j, gB, gA, upA, mid, omB)) { kfail = j; break; }
+        if (!zm.template iter<1>(j, gB, gA, upA, mid, omB, sgB, sgA, ugA, mg)) { kfail = j; break; }
         j++;
         if (j >= zm.nprod) {  // j even: last production odd
             prod_b<Q, ZM::NM, NUP, NMID, T, FLAGS, TYI, BCP>(a, j - 1, z0 - 2 + j, zm.e4t[1], zm.e1t[1], zm.interior, x,
-                                                        y, gB, upB, mid, omA);
+                                                        y, gB, upB, mid, omA, zm.e4g[1], zm.e1g[1], sgB, ugB, mg);
             break;
         }
-        if (!zm.template iter<0>(j, gA, gB, upB, mid, omA)) { kfail = j; break; }
+        if (!zm.template iter<0>(j, gA, gB, upB, mid, omA, sgA, sgB, ugB, mg)) { kfail = j; break; }
         j++;
     }
     if (kfail >= 0) {
@@ -985,11 +1176,11 @@ __device__ __forceinline__ bool zmarch_column(const StepArgs& a, const CUtensorM
     return true;
 }
 
-template <int Q, typename T, int TYI, int NPM>
-__device__ __forceinline__ void zmarch_init_barriers(const ZSmem<Q, T, TYI, NPM>& sm)
+template <int Q, typename T, int TYI, int NPM, bool TH>
+__device__ __forceinline__ void zmarch_init_barriers(const ZSmem<Q, T, TYI, NPM, TH>& sm)
 {
     if (threadIdx.x == 0) {
-        for (int s = 0; s < ZSmem<Q, T, TYI, NPM>::NS; s++) mbar_init(&sm.bars[s], 1);
+        for (int s = 0; s < ZSmem<Q, T, TYI, NPM, TH>::NS; s++) mbar_init(&sm.bars[s], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -1003,7 +1194,7 @@ __global__ void __launch_bounds__(32 * (TYI + 2), 1)
     zmarch_step(const __grid_constant__ CUtensorMap map_in, const StepArgs a)
 {
     extern __shared__ __align__(128) unsigned char smem[];
-    const ZSmem<Q, T, TYI, npairs_of(FLAGS)> sm(smem);
+    const ZSmem<Q, T, TYI, npairs_of(FLAGS), (FLAGS & F_THERMAL) != 0> sm(smem);
     zmarch_init_barriers(sm);
     unsigned g0 = 0;
     const int z0 = blockIdx.z * a.lz;
@@ -1020,7 +1211,7 @@ __host__ __device__ inline dim3 zmarch_grid(int nx, int ny, int nz, int tyi, int
 template <int Q, typename T, int FLAGS, int TYI>
 constexpr size_t step_smem_bytes()
 {
-    return ZSmem<Q, T, TYI, npairs_of(FLAGS)>::bytes;
+    return ZSmem<Q, T, TYI, npairs_of(FLAGS), (FLAGS & F_THERMAL) != 0>::bytes;
 }
 
 }  // namespace mrlbm

@@ -186,13 +186,26 @@ mrlbm_status mrlbm::build_bc_class(int q, int mq, uint32_t word, const double uv
 
 // ------------------------------------------------------------ domain setup
 
-static int moments_of(const mrlbm_desc& d) { return d.rheology != MRLBM_NEWTONIAN ? 11 : 10; }
+static int moments_of(const mrlbm_desc& d)
+{
+    return (d.rheology != MRLBM_NEWTONIAN ? 11 : 10) + (d.thermal ? 4 : 0);
+}
+
+// G_DIFF_FLUC_COEF from the thermal diffusivity with the reference's fixed
+// T_DIFF_REF = 1/6 and G_TAU = 3 T_DIFF_REF + 1/2
+// (src/cases/rayleighBenard_Periodic/constants.inc:58-65)
+static double thermal_coef(double alpha)
+{
+    const double diff_ref = 1.0 / 6.0, g_tau = diff_ref * 3.0 + 0.5, g_omega = 1.0 / g_tau;
+    const double aaa = 3.0 * (alpha - diff_ref) * g_omega;
+    return aaa / (1.0 + aaa);
+}
 
 static size_t elem_size(int storage) { return storage == MRLBM_F32 ? 4 : 2; }
 
 void mrlbm::storage_scales(int storage, float* scale, float* iscale)
 {
-    for (int k = 0; k < 11; k++) {
+    for (int k = 0; k < NM_MAX; k++) {
         float s = 1.0f;
         if (storage != MRLBM_F32) {
             // powers of two keep values of the shifted moments in the normal
@@ -215,6 +228,16 @@ static mrlbm_status validate(const mrlbm_desc* d)
     if (d->rheology < 0 || d->rheology > 2) return fail(MRLBM_EINVAL, "bad rheology");
     if (d->bc_matrix_q != 0 && d->bc_matrix_q != 19 && d->bc_matrix_q != d->lattice)
         return fail(MRLBM_EINVAL, "bc_matrix_q must be 0, 19 or the lattice size");
+    if (d->thermal != 0 && d->thermal != 1) return fail(MRLBM_EINVAL, "thermal must be 0 or 1");
+    if (d->thermal) {
+        // the second distribution's row exchange and ring fit next to the
+        // D3Q19 flow's in shared memory; the reference's thermal cases are
+        // D3Q19 Newtonian
+        if (d->lattice != 19 || d->storage != MRLBM_F32 || d->rheology != MRLBM_NEWTONIAN)
+            return fail(MRLBM_EINVAL, "the thermal scalar needs D3Q19, FP32 storage and a Newtonian fluid");
+        if (!(d->t_diffusivity > 0.0) || !std::isfinite(thermal_coef(d->t_diffusivity)))
+            return fail(MRLBM_EINVAL, "bad thermal diffusivity %g", d->t_diffusivity);
+    }
     return MRLBM_OK;
 }
 
@@ -252,7 +275,7 @@ mrlbm_status mrlbm::domain_alloc(mrlbm_domain* dom)
     CK(cudaMemset(dom->m[0], 0, mbytes));
     CK(cudaMemset(dom->m[1], 0, mbytes));
     // exterior state: the reference's initial rest state (stale wall ghosts)
-    float ext[11];
+    float ext[NM_MAX];
     {
         const int qs = (d.lattice == 27) ? 19 : 19;
         double pxx = 0, pyy = 0, pzz = 0;
@@ -262,11 +285,13 @@ mrlbm_status mrlbm::domain_alloc(mrlbm_domain* dom)
             pyy += f * lat_cy(i) * lat_cy(i);
             pzz += f * lat_cz(i) * lat_cz(i);
         }
-        for (int k = 0; k < 11; k++) ext[k] = 0.f;
+        for (int k = 0; k < NM_MAX; k++) ext[k] = 0.f;
         ext[4] = (float)(4.5 * (pxx / d.rho0 - 1.0 / 3.0));
         ext[7] = (float)(4.5 * (pyy / d.rho0 - 1.0 / 3.0));
         ext[9] = (float)(4.5 * (pzz / d.rho0 - 1.0 / 3.0));
-        ext[10] = (float)dom->omega0;
+        // thermal: exterior C at the reference temperature, no flux
+        if (d.thermal) ext[10] = (float)d.t_reference;
+        else ext[10] = (float)dom->omega0;
     }
     memcpy(dom->ext, ext, sizeof(ext));
     CK(cudaStreamCreateWithFlags(&dom->stream, cudaStreamNonBlocking));
@@ -361,9 +386,32 @@ extern "C" mrlbm_status mrlbm_domain_destroy(mrlbm_domain* dom)
     return MRLBM_OK;
 }
 
+// Thermal rule of a class (bits 13-16 of its word, include/mrlbm.h
+// MRLBM_THERMAL_*): rules 2 and 3 act along the normal of a face node, the
+// axis whose whole + or - half of the octant mask is solid.
+static mrlbm_status thermal_rule_of(uint32_t word, const double t_wall[4], BcClass* c)
+{
+    const uint32_t rule = (word >> 13) & 3u, idx = (word >> 15) & 3u;
+    const uint32_t oct = word & 0xFFu;
+    int axis = 3, side = 0, nfaces = 0;
+    for (int a = 0; a < 3; a++)
+        for (int sd = 0; sd < 2; sd++) {
+            bool all = true;
+            for (int o = 0; o < 8; o++)
+                if ((((o >> a) & 1) == sd) && !((oct >> o) & 1u)) all = false;
+            if (all) { axis = a; side = sd; nfaces++; }
+        }
+    if (nfaces != 1) axis = 3;
+    if ((rule == 2 || rule == 3) && axis == 3)
+        return fail(MRLBM_EINVAL, "node type 0x%x: thermal rule %u needs a face node (one solid half)", word, rule);
+    c->trule = rule | ((uint32_t)axis << 2) | ((uint32_t)side << 4);
+    c->twall = (float)t_wall[idx];
+    return MRLBM_OK;
+}
+
 mrlbm_status mrlbm::classify_nodes(int q, int mq, const uint32_t* nt, long long n, const double uvel[4][3],
                                    double omega0, std::vector<uint8_t>& cls, std::vector<BcClass>& table,
-                                   bool& any_bc, bool case_mode)
+                                   bool& any_bc, bool case_mode, const double* t_wall)
 {
     std::map<uint32_t, int> ids;
     table.assign(1, BcClass{});  // class 0: bulk (unused entry)
@@ -379,15 +427,18 @@ mrlbm_status mrlbm::classify_nodes(int q, int mq, const uint32_t* nt, long long 
         if (bulk) { cls[k] = CLS_BULK; continue; }
         any_bc = true;
         if (solid) { cls[k] = CLS_SOLID; continue; }
-        const uint32_t key = case_mode ? w : (w & 0x1FFFu);
+        // (thermal domains also key on the thermal rule and value index)
+        const uint32_t key = case_mode ? w : (w & (t_wall ? 0x1FFFFu : 0x1FFFu));
         auto it = ids.find(key);
         if (it == ids.end()) {
             if ((int)table.size() >= 255) return fail(MRLBM_EINVAL, "more than 254 distinct boundary node types");
             BcClass c;
             memset(&c, 0, sizeof(c));
             c.word = key;
-            mrlbm_status st = case_mode ? MRLBM_OK : build_bc_class(q, mq, key, uvel, omega0, &c);
+            mrlbm_status st = case_mode ? MRLBM_OK : build_bc_class(q, mq, key & 0x1FFFu, uvel, omega0, &c);
             if (st) return st;
+            c.word = key;
+            if (t_wall && !case_mode && (st = thermal_rule_of(key, t_wall, &c))) return st;
             const int id = (int)table.size();
             table.push_back(c);
             it = ids.emplace(key, id).first;
@@ -406,7 +457,8 @@ static mrlbm_status set_node_types_impl(mrlbm_domain* dom, const uint32_t* nt, b
     std::vector<BcClass> table;
     bool any = false;
     mrlbm_status st =
-        classify_nodes(dom->q, d.bc_matrix_q, nt, n, d.bc_velocity, dom->omega0, cls, table, any, case_mode);
+        classify_nodes(dom->q, d.bc_matrix_q, nt, n, d.bc_velocity, dom->omega0, cls, table, any, case_mode,
+                       d.thermal ? d.t_wall : nullptr);
     if (st) return st;
     // scatter into the padded plane layout
     std::vector<uint8_t> padded((size_t)dom->field, 0);
@@ -462,6 +514,8 @@ static mrlbm_status run_init(mrlbm_domain* dom, InitArgs& a)
     a.qs = 19;  // the reference's D3Q19 second-moment sums (also on D3Q27)
     a.rho0 = (float)d.rho0;
     a.omega0 = (float)dom->omega0;
+    a.thermal = d.thermal;
+    a.c0 = (float)d.t_reference;
     memcpy(a.scale, dom->scale, sizeof(a.scale));
     if (d.lattice == 19) launch_init<19>(dom, a); else launch_init<27>(dom, a);
     CK(cudaGetLastError());
@@ -521,7 +575,8 @@ void mrlbm::fill_step_args(const mrlbm_domain* dom, StepArgs& a, int parity, int
 {
     const mrlbm_desc& d = dom->d;
     a.m_out = dom->m[parity ^ 1];
-    for (int p = 0; p < 6; p++)
+    a.m_in = static_cast<const float*>(dom->m[parity]);
+    for (int p = 0; p < (NM_MAX + 1) / 2; p++)
         a.out_p[p] = 2 * p < dom->nm ? static_cast<char*>(dom->m[parity ^ 1]) + (size_t)p * 2 * dom->field * dom->esize
                                      : nullptr;
     a.err = dom->err;
@@ -537,6 +592,10 @@ void mrlbm::fill_step_args(const mrlbm_domain* dom, StepArgs& a, int parity, int
     a.fx = (float)d.force[0]; a.fy = (float)d.force[1]; a.fz = (float)d.force[2];
     a.nnf_n = (float)d.nnf_n; a.nnf_k = (float)d.nnf_k;
     a.nnf_yield = (float)d.nnf_yield; a.nnf_omega_p = (float)d.nnf_omega_p;
+    a.t_coef = d.thermal ? (float)thermal_coef(d.t_diffusivity) : 0.f;
+    a.t_ref = (float)d.t_reference;
+    for (int k = 0; k < 3; k++) a.t_gb[k] = (float)(d.t_gravity_beta[k] * d.rho0);
+    a.t_src = (float)d.t_source;
     memcpy(a.scale, dom->scale, sizeof(a.scale));
     memcpy(a.iscale, dom->iscale, sizeof(a.iscale));
     flags = 0;
@@ -545,6 +604,7 @@ void mrlbm::fill_step_args(const mrlbm_domain* dom, StepArgs& a, int parity, int
     if (d.rheology == MRLBM_POWERLAW) flags |= F_POWERLAW;
     if (d.rheology == MRLBM_BINGHAM) flags |= F_BINGHAM;
     if (flags & (F_POWERLAW | F_BINGHAM)) flags |= F_BC;  // nnf variants always read the class map
+    if (d.thermal) flags |= F_THERMAL | F_FORCE;           // the Boussinesq force is per node
 }
 
 mrlbm_status mrlbm::enqueue_step(mrlbm_domain* dom, int parity, cudaStream_t s)
@@ -738,7 +798,7 @@ extern "C" mrlbm_status mrlbm_get_macr(mrlbm_domain* dom, float* rho, float* ux,
     if (uy) memcpy(uy, &all[2 * n], n * sizeof(float));
     if (uz) memcpy(uz, &all[3 * n], n * sizeof(float));
     if (omega) {
-        if (dom->nm < 11) return fail(MRLBM_EINVAL, "domain has no omega field");
+        if (d.rheology == MRLBM_NEWTONIAN) return fail(MRLBM_EINVAL, "domain has no omega field");
         memcpy(omega, &all[10 * n], n * sizeof(float));
     }
     return MRLBM_OK;

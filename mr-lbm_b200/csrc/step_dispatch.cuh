@@ -42,8 +42,15 @@ mrlbm_status dispatch_step(const CUtensorMap& map, const StepArgs& a, int flags,
         case F_BC | F_FORCE | F_POWERLAW: return launch_step_t<Q, T, F_BC | F_FORCE | F_POWERLAW>(map, a, s);
         case F_BC | F_BINGHAM: return launch_step_t<Q, T, F_BC | F_BINGHAM>(map, a, s);
         case F_BC | F_FORCE | F_BINGHAM: return launch_step_t<Q, T, F_BC | F_FORCE | F_BINGHAM>(map, a, s);
-        default: return fail(MRLBM_EINVAL, "unsupported step flag combination %d", flags);
+        default: break;
     }
+    // thermal scalar: D3Q19 with FP32 storage only (its second row exchange
+    // fits next to the D3Q19 flow's in shared memory)
+    if constexpr (Q == 19 && is_f32<T>()) {
+        if (flags == (F_THERMAL | F_FORCE)) return launch_step_t<Q, T, F_THERMAL | F_FORCE>(map, a, s);
+        if (flags == (F_THERMAL | F_FORCE | F_BC)) return launch_step_t<Q, T, F_THERMAL | F_FORCE | F_BC>(map, a, s);
+    }
+    return fail(MRLBM_EINVAL, "unsupported step flag combination %d", flags);
 }
 
 }  // namespace mrlbm

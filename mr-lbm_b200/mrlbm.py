@@ -28,6 +28,18 @@ def BC_VELOCITY_INDEX(k):
     return (int(k) & 3) << 11
 
 
+# thermal rule of a boundary node (include/mrlbm.h MRLBM_THERMAL_*)
+THERMAL_KEEP, THERMAL_DIRICHLET, THERMAL_DIRICHLET_FLUX, THERMAL_ADIABATIC = 0, 1, 2, 3
+
+
+def THERMAL_RULE(r):
+    return (int(r) & 3) << 13
+
+
+def THERMAL_INDEX(k):
+    return (int(k) & 3) << 15
+
+
 # octant masks of the reference's nodeTypeMap (src/nodeTypeMap.h:10-44)
 WEST, EAST, SOUTH, NORTH, BACK, FRONT = 0x55, 0xAA, 0x33, 0xCC, 0x0F, 0xF0
 
@@ -53,7 +65,13 @@ class Desc(C.Structure):
         ("nnf_n", C.c_double), ("nnf_k", C.c_double),
         ("nnf_yield", C.c_double), ("nnf_omega_p", C.c_double),
         ("bc_matrix_q", C.c_int),
-        ("reserved", C.c_int * 7),
+        ("thermal", C.c_int),
+        ("t_diffusivity", C.c_double),
+        ("t_reference", C.c_double),
+        ("t_gravity_beta", C.c_double * 3),
+        ("t_source", C.c_double),
+        ("t_wall", C.c_double * 4),
+        ("reserved", C.c_int * 8),
     ]
 
 
@@ -211,7 +229,9 @@ class PinnedArray:
 
 def make_desc(nx, ny, nz, lattice=D3Q19, storage=F32, periodic=(1, 1, 1), tau=0.8, rho0=1.0,
               force=(0.0, 0.0, 0.0), bc_velocity=None, rheology=NEWTONIAN, nnf_n=1.0, nnf_k=0.0,
-              nnf_yield=0.0, nnf_omega_p=0.0, bc_matrix_q=0):
+              nnf_yield=0.0, nnf_omega_p=0.0, bc_matrix_q=0, thermal=None):
+    """thermal: None, or a dict with diffusivity, reference (1.0), gravity_beta
+    (3 values), source (0) and wall (up to 4 values): the thermal scalar."""
     d = Desc()
     d.nx, d.ny, d.nz = nx, ny, nz
     d.lattice, d.storage = lattice, storage
@@ -226,6 +246,15 @@ def make_desc(nx, ny, nz, lattice=D3Q19, storage=F32, periodic=(1, 1, 1), tau=0.
     d.rheology = rheology
     d.nnf_n, d.nnf_k, d.nnf_yield, d.nnf_omega_p = nnf_n, nnf_k, nnf_yield, nnf_omega_p
     d.bc_matrix_q = bc_matrix_q
+    if thermal is not None:
+        d.thermal = 1
+        d.t_diffusivity = float(thermal["diffusivity"])
+        d.t_reference = float(thermal.get("reference", 1.0))
+        for a, v in enumerate(thermal.get("gravity_beta", (0.0, 0.0, 0.0))):
+            d.t_gravity_beta[a] = float(v)
+        d.t_source = float(thermal.get("source", 0.0))
+        for k, v in enumerate(thermal.get("wall", ())):
+            d.t_wall[k] = float(v)
     return d
 
 

@@ -24,6 +24,10 @@ def oracle_for(desc, node_types=None, fp32=False):
     for k, c in ((4, lattice_np.CX), (7, lattice_np.CY), (9, lattice_np.CZ)):
         ext[k] = 4.5 * (sum(w[i] * c[i] ** 2 for i in range(19)) - 1 / 3)
     kw["exterior"] = ext
+    if desc.thermal:
+        kw["thermal"] = dict(alpha=desc.t_diffusivity, reference=desc.t_reference,
+                             gbeta=tuple(desc.t_gravity_beta[a] for a in range(3)), source=desc.t_source,
+                             wall=tuple(desc.t_wall[k] for k in range(4)))
     o = oracle_ffi.OracleDomain(oracle_ffi.make_desc(desc.nx, desc.ny, desc.nz, **kw), fp32=fp32)
     if node_types is not None:
         o.set_node_types(node_types)
@@ -38,9 +42,11 @@ def gpu_to_oracle_layout(m):
 # moment groups and the norm each moment's error is measured against:
 # rho - rho0 against rho (its FP32 resolution is that of rho itself), each
 # velocity component against |u|, each second moment against the group of
-# second moments, omega against omega.
+# second moments, omega against omega; with the thermal scalar, C against C
+# (moment 10) and each flux component against |flux| (moments 11-13).
 GROUPS = {0: [0], 1: [1, 2, 3], 2: [1, 2, 3], 3: [1, 2, 3], 4: [4, 5, 6, 7, 8, 9], 5: [4, 5, 6, 7, 8, 9],
-          6: [4, 5, 6, 7, 8, 9], 7: [4, 5, 6, 7, 8, 9], 8: [4, 5, 6, 7, 8, 9], 9: [4, 5, 6, 7, 8, 9], 10: [10]}
+          6: [4, 5, 6, 7, 8, 9], 7: [4, 5, 6, 7, 8, 9], 8: [4, 5, 6, 7, 8, 9], 9: [4, 5, 6, 7, 8, 9], 10: [10],
+          11: [11, 12, 13], 12: [11, 12, 13], 13: [11, 12, 13]}
 
 
 def compare(gpu_m, orc_m, fluid=None, rho0=1.0):

@@ -140,3 +140,42 @@ def test_bc_matrices_match_oracle(lattice, mq):
                 assert L.orc_bc_solve(lattice, mq, known, P(u), om, P(f), P(ref)) == 0
                 np.testing.assert_allclose(X[0], ref[0], rtol=2e-6)
                 np.testing.assert_allclose(X[1:] / X[0], ref[4:], rtol=2e-4, atol=2e-7)
+
+
+def test_thermal_descriptor_rules():
+    """The thermal scalar is accepted on D3Q19 with FP32 storage and a
+    Newtonian fluid (the reference's thermal cases), with four more stored
+    moments; other combinations are rejected before anything is allocated."""
+    import mrlbm
+    th = dict(diffusivity=0.01, reference=1.0, gravity_beta=(1e-5, 0, 0), wall=(1.5, 0.5))
+    n = C.c_size_t()
+    d = mrlbm.make_desc(16, 12, 8, lattice=19, thermal=th)
+    assert mrlbm.lib().mrlbm_domain_bytes(C.byref(d), C.byref(n)) == 0
+    pitch = (16 + 4 + 1 + 7) // 8 * 8
+    field = pitch * (12 + 2) * (8 + 2)
+    assert n.value == 2 * field * 14 * 4 + field
+    bad = [mrlbm.make_desc(16, 12, 8, lattice=27, thermal=th),
+           mrlbm.make_desc(16, 12, 8, lattice=19, storage=mrlbm.F16, thermal=th),
+           mrlbm.make_desc(16, 12, 8, lattice=19, rheology=mrlbm.POWERLAW, thermal=th),
+           mrlbm.make_desc(16, 12, 8, lattice=19, thermal=dict(th, diffusivity=0.0))]
+    for d in bad:
+        assert mrlbm.lib().mrlbm_domain_bytes(C.byref(d), C.byref(n)) == 1   # MRLBM_EINVAL
+
+
+def test_descriptor_layout_matches_header():
+    """The ctypes mirror of mrlbm_desc has the C header's size and offsets."""
+    import subprocess
+    import tempfile
+    import mrlbm
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = ('#include "mrlbm.h"\n#include <stdio.h>\n#include <stddef.h>\n'
+           'int main(void){printf("%zu %zu %zu %zu\\n", sizeof(mrlbm_desc), offsetof(mrlbm_desc, bc_matrix_q),'
+           ' offsetof(mrlbm_desc, thermal), offsetof(mrlbm_desc, t_wall)); return 0;}\n')
+    with tempfile.TemporaryDirectory() as tmp:
+        c = os.path.join(tmp, "sz.c")
+        open(c, "w").write(src)
+        exe = os.path.join(tmp, "sz")
+        subprocess.check_call(["gcc", "-I", os.path.join(root, "include"), c, "-o", exe])
+        vals = [int(v) for v in subprocess.check_output([exe]).split()]
+    D = mrlbm.Desc
+    assert vals == [C.sizeof(D), D.bc_matrix_q.offset, D.thermal.offset, D.t_wall.offset]
