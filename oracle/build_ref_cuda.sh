@@ -17,8 +17,9 @@
 #   _ref/refsim_bench256     benchmark (README table case), D3Q19, 256^3, 1000 steps
 #   _ref/refsim_lid64_edges  C1 with the lid's edges typed as edge walls
 #   _ref/refsim_lid16_trace  16^3 lid cavity writing its fields after every step
+#   _ref/refsim_rb64         rayleighBenard_Periodic (thermal), 64 x 64 x 8, 1000 steps
 #   _ref/cases/*             the same cases compiled in this library's case mode
-# CASES_ONLY=1 rebuilds only the case-mode programs.
+# CASES_ONLY=1 rebuilds only the case-mode programs; THERMAL_ONLY=1 only refsim_rb64.
 set -euo pipefail
 REF=${REF:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
@@ -28,7 +29,7 @@ mkdir -p "$OUT"
 [ -d "$REF/src" ] || { echo "reference tree not found at $REF" >&2; exit 1; }
 
 build_case() {
-    local name=$1 case=$2 lattice=$3 steps=$4 n=$5 extra=$6
+    local name=$1 case=$2 lattice=$3 steps=$4 n=$5 extra=$6 nvflags=${7:-}
     local work
     work=$(mktemp -d /tmp/mrlbm_refbuild.XXXXXX)
     cp -r "$REF/src" "$work/src"
@@ -42,14 +43,14 @@ build_case() {
     sed -i "s/^#define D3Q[0-9]*/#define $lattice/" "$c/model.inc"
     sed -i 's/^#define BIN_SAVE .*/#define BIN_SAVE (true)/; s/^#define VTK_SAVE .*/#define VTK_SAVE (false)/; s/^#define ONLY_FINAL_MACRO .*/#define ONLY_FINAL_MACRO (true)/; s/^#define MACR_SAVE .*/#define MACR_SAVE (false)/' "$c/output.inc"
     eval "$extra"
-    "$NVCC" -gencode arch=compute_100,code=sm_100 -rdc=true -O3 --restrict -DSM_100 -DTARGET_LINUX \
+    "$NVCC" -gencode arch=compute_100,code=sm_100 -rdc=true -O3 --restrict -DSM_100 -DTARGET_LINUX $nvflags \
         -diag-suppress=39 -diag-suppress=179 -w -ccbin /usr/bin/g++ *.cu -lcudadevrt -lcurand -o "$OUT/$name"
     cd /
     rm -rf "$work"
     echo "built $OUT/$name"
 }
 
-if [ -z "${CASES_ONLY:-}" ]; then
+if [ -z "${CASES_ONLY:-}" ] && [ -z "${THERMAL_ONLY:-}" ]; then
 # C1: lid-driven cavity 64^3, Re 100, lid velocity 0.05 (tau from Re, constants.inc:35-36)
 build_case refsim_lid64 lidDrivenCavity_3D D3Q19 2000 64 \
   'sed -i "s/^constexpr dfloat RE = .*/constexpr dfloat RE = 100;/; s/^constexpr dfloat U_MAX = .*/constexpr dfloat U_MAX = 0.05;/" "$c/constants.inc"; sed -i "s/^#define REPORT_SAVE .*/#define REPORT_SAVE (false)/" "$c/output.inc"'
@@ -77,6 +78,25 @@ build_case refsim_tgv256_q27 taylorGreen D3Q27 1000 256 \
 # README benchmark case, D3Q19 256^3 (the published MLUPS table), 1000 steps
 build_case refsim_bench256 benchmark D3Q19 1000 256 'true'
 fi
+
+if [ -z "${CASES_ONLY:-}" ] || [ -n "${THERMAL_ONLY:-}" ]; then
+# thermal: rayleighBenard_Periodic (D3Q19 flow + D3G19 scalar, THERMAL_MODEL),
+# 64 x 64 x 8, Pr 10, Ra 1e5, hot WEST / cold EAST walls, gravity along x,
+# 1000 steps; final rho, u and C as .bin.  The case ships NZ = 4, which is
+# below the 8^3 block (NUM_BLOCK_Z = NZ / BLOCK_NZ = 0, definitions.h:107-110)
+# and crashes on the host; NZ = 8 is the smallest depth the program runs.  Its
+# flow_initialization.inc reads randomNumbers[] (times 0) while the case leaves
+# RANDOM_NUMBERS undefined, so that buffer would never be allocated
+# (main.cuh:919-929): RANDOM_NUMBERS is switched on to give the read a buffer.
+# Built as the stock script builds it, the thermal step kernel needs more than
+# 128 registers a thread and fails to launch with its 512-thread blocks ("too
+# many resources requested"; the program then writes its initial fields), so
+# this one program gets -maxrregcount=128.
+build_case refsim_rb64 rayleighBenard_Periodic D3Q19 1000 64 \
+  'sed -i "s/^constexpr int NZ = .*/constexpr int NZ = 8;        \/\/ size z of the grid in one GPU/" "$c/constants.inc"; sed -i "s|^//#define RANDOM_NUMBERS true|#define RANDOM_NUMBERS true|" "$c/model.inc"; sed -i "s/^#define REPORT_SAVE .*/#define REPORT_SAVE (false)/" "$c/output.inc"' \
+  -maxrregcount=128
+fi
+[ -n "${THERMAL_ONLY:-}" ] && exit 0
 
 # ---------------------------------------------------------------------------
 # The same reference cases compiled, unchanged, in this library's case mode

@@ -15,6 +15,7 @@
 //   src/includeFiles/velocitySets/D3G19.inc                thermal lattice weights
 //   src/colrec/G_SCALAR/reconstruction.inc                 thermal population reconstruction
 //   src/cases/rayleighBenard_Periodic/constants.inc        thermal case constants
+//   src/cases/rayleighBenard_Periodic/bc_definition.inc    its wall closed forms
 #include <cmath>
 #include <cstdint>
 
@@ -146,6 +147,16 @@ int ref_bc_plates_q19(unsigned int nodeType, const double* pop, double omegaVar,
 {
     BC_PROLOGUE
 #include "cases/parallelPlates_D3Q19/bc_definition.inc"
+    BC_EPILOGUE
+}
+
+// the thermal Rayleigh-Benard case's walls (its own closed forms, written in
+// the wall normal l and the wall velocity)
+int ref_bc_rb_q19(unsigned int nodeType, const double* pop, double omegaVar, double* out)
+{
+    BC_PROLOGUE
+    using namespace q19;
+#include "cases/rayleighBenard_Periodic/bc_definition.inc"
     BC_EPILOGUE
 }
 

@@ -17,6 +17,8 @@ Contents (all float64):
       src/cases/parallelPlates_D3Q27/bc_definition.inc
   g19_in (N,7) / g19_out (N,19)            src/colrec/G_SCALAR/reconstruction.inc (D3G19)
       g19_in = [C, 3ux, 3uy, 3uz, udx, udy, udz]
+  rb_type, rb_pops (.,19), rb_omega, rb_out
+      src/cases/rayleighBenard_Periodic/bc_definition.inc (its 6 faces and 12 edges)
   rbp_const (10,)                          src/cases/rayleighBenard_Periodic/constants.inc:
       G_DIFF_FLUC_COEF, T_DIFFUSIVITY, T_gravity_t_beta, VISC, T_REFERENCE, T_HOT,
       T_COLD, gravity_vector[3]
@@ -116,6 +118,19 @@ def main():
     rc = np.zeros(10)
     R.ref_rb_periodic_constants(P(rc))
     out["rbp_const"] = rc
+
+    types, pops, oms, res = [], [], [], []
+    for name, t in sorted(lattice_np.wall_types().items()):
+        if name.count("_") == 2:   # the case lists faces and edges, no corners
+            continue
+        for rep in range(2):
+            f = pops_near_eq(19)
+            om = rng.uniform(0.6, 1.9)
+            r = np.zeros(10)
+            assert R.ref_bc_rb_q19(t, P(f), om, P(r)) == 1, name
+            types.append(t); pops.append(f); oms.append(om); res.append(r)
+    out["rb_type"] = np.array(types, dtype=np.uint32)
+    out["rb_pops"], out["rb_omega"], out["rb_out"] = map(np.array, (pops, oms, res))
 
     path = os.path.join(HERE, "ref_kat.npz")
     np.savez_compressed(path, **out)

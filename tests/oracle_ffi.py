@@ -104,6 +104,7 @@ def ref_kat():
     L.ref_bc_plates_q27.argtypes = [C.c_uint, D, C.c_double, D]
     L.ref_bc_plates_q19.argtypes = [C.c_uint, D, C.c_double, D]
     L.ref_reconstruct_g19.argtypes = [C.c_double, D, D, D]
+    L.ref_bc_rb_q19.argtypes = [C.c_uint, D, C.c_double, D]
     L.ref_rb_periodic_constants.argtypes = [D]
     for f in ("ref_bc_lid_q19", "ref_bc_voxel_q19", "ref_bc_plates_q27", "ref_bc_plates_q19"):
         getattr(L, f).restype = C.c_int

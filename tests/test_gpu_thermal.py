@@ -224,3 +224,68 @@ def test_thermal_checkpoint_round_trip():
         assert np.array_equal(a.moments(), b.moments())
         b.close()
     a.close()
+
+
+def test_rayleigh_benard_matches_reference_program(tmp_path):
+    """The reference's own CUDA program for rayleighBenard_Periodic (built for
+    sm_100 by oracle/build_ref_cuda.sh: 64 x 64 x 8, D3Q19 + D3G19, Pr 10,
+    Ra 1e5, hot WEST / cold EAST, gravity along x, 1000 steps) against this
+    library set up from the same constants, both against the FP64 oracle.
+    The case's wall closed forms are the library's moment-BC system
+    (tests/test_oracle_kat.py), and its neighbour-flux wall rule reads a value
+    that no thread of the step has rewritten yet, so both sides compute the
+    same arithmetic up to FP32 operation order.
+
+    With gravity normal to the walls and no perturbation the cell conducts:
+    the exact velocity is zero and what the solvers carry (|u| ~ 1e-6) is
+    FP32 round-off of the momentum sums, so velocities are compared in
+    absolute terms, against the case's free-fall velocity sqrt(g beta dT L)."""
+    import os
+    import subprocess
+    exe = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "refsim_rb64")
+    if not os.path.exists(exe):
+        pytest.skip("reference CUDA build missing (oracle/build_ref_cuda.sh needs the reference tree)")
+    r = subprocess.run([exe], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert "Kernel launch failed" not in r.stdout, r.stdout[-2000:]
+    nx, ny, nz, steps = 64, 64, 8, 1000
+    ref = {v: np.fromfile(str(tmp_path / "TEST" / "000" / ("000_%s%06d.bin" % (v, steps))), dtype=np.float32)
+           .reshape(nz, ny, nx).astype(np.float64) for v in ("rho", "ux", "uy", "uz", "C")}
+    # the case's constants (golden copy of rayleighBenard_Periodic/constants.inc)
+    const = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_kat.npz"))["rbp_const"]
+    coef, alpha, gtb, visc, tref, thot, tcold = const[:7]
+    d = thermal_desc(nx, ny, nz, (0, 1, 1), tau=0.5 + 3 * visc, alpha=alpha, gbeta=tuple(gtb * const[7:10]),
+                     wall=(thot, tcold, tref, tref))
+    rule = mrlbm.THERMAL_RULE(mrlbm.THERMAL_DIRICHLET_FLUX)
+    nt = node_types(nx, ny, nz, x_walls=(rule | mrlbm.THERMAL_INDEX(0), rule | mrlbm.THERMAL_INDEX(1)))
+    dom = mrlbm.Domain(d)
+    dom.set_node_types(nt)
+    dom.init_uniform()
+    orc = pu.oracle_for(d, nt)
+    orc.set_moments(pu.gpu_to_oracle_layout(dom.moments()))
+    dom.step(steps)
+    orc.step(steps)
+    g = dom.moments().astype(np.float64)
+    o = np.moveaxis(orc.moments(), -1, 0)
+    dom.close()
+    ours = {"rho": 1.0 + g[0], "ux": g[1], "uy": g[2], "uz": g[3], "C": g[10]}
+    fp64 = {"rho": 1.0 + o[0], "ux": o[1], "uy": o[2], "uz": o[3], "C": o[10]}
+    u_scale = 3.0 * np.sqrt(gtb * (thot - tcold) * nx)   # stored 3u of the free-fall velocity
+
+    def c_err(a, b):
+        return float(np.sqrt(np.sum((a["C"] - b["C"]) ** 2) / np.sum((b["C"] - tref) ** 2)))
+
+    def u_err(a, b):
+        return max(float(np.max(np.abs(a[k] - b[k]))) for k in ("ux", "uy", "uz")) / u_scale
+
+    def rho_err(a, b):
+        return float(np.max(np.abs(a["rho"] - b["rho"])))
+
+    pairs = {"ours-ref": (ours, ref), "ours-fp64": (ours, fp64), "ref-fp64": (ref, fp64)}
+    res = {k: (c_err(*v), u_err(*v), rho_err(*v)) for k, v in pairs.items()}
+    for k, (ce, ue, re_) in res.items():
+        print("RB 64x64x8 %-9s C rel L2 %.3e, max|du| / U %.3e, max|drho| %.3e" % (k, ce, ue, re_))
+    assert res["ours-ref"][0] < 1e-4 and res["ours-ref"][1] < 2e-4 and res["ours-ref"][2] < 1e-5
+    # no further from FP64 than the reference program itself (or FP32 level)
+    assert res["ours-fp64"][0] <= max(1e-5, 2 * res["ref-fp64"][0])
+    assert res["ours-fp64"][1] <= max(1e-5, 2 * res["ref-fp64"][1])

@@ -180,3 +180,11 @@ def test_thermal_face_normals():
         assert side.value == sd
     # an edge has two solid halves: no single normal
     assert L.orc_face_normal(lattice_np.FACES["WEST"] | lattice_np.FACES["SOUTH"], C.byref(side)) == -1
+
+
+def test_rayleigh_benard_walls_golden():
+    """The thermal Rayleigh-Benard case writes its walls in its own closed
+    forms (wall normal l, src/cases/rayleighBenard_Periodic/bc_definition.inc);
+    they are the same moment-BC system: faces and edges to round-off."""
+    for t, f, om, ref in zip(GOLD["rb_type"], GOLD["rb_pops"], GOLD["rb_omega"], GOLD["rb_out"]):
+        np.testing.assert_allclose(orc_bc(19, 19, t, (0, 0, 0), om, f), ref, rtol=1e-11, atol=1e-14)
