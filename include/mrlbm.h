@@ -53,10 +53,13 @@ typedef enum { MRLBM_NEWTONIAN = 0, MRLBM_POWERLAW = 1, MRLBM_BINGHAM = 2 } mrlb
 
 /* Node-type words follow the reference's nodeTypeMap (src/nodeTypeMap.h:10-80):
  * bits 0-7 octant solid mask (0 = bulk, 0xFF = solid), bits 8-10 BC kind
- * (0 no-slip wall, 1 prescribed-velocity wall), bits 11-12 velocity index. */
+ * (0 no-slip wall, 1 prescribed-velocity wall, 2 outflow: a face node takes
+ * its inward neighbour's previous-step moments, as the reference's
+ * mountedCube / externalFlow cases do), bits 11-12 velocity index. */
 #define MRLBM_NODE_BULK 0x00u
 #define MRLBM_NODE_SOLID 0xFFu
 #define MRLBM_BC_VELOCITY_WALL (1u << 8)
+#define MRLBM_BC_OUTFLOW (2u << 8)
 #define MRLBM_BC_VELOCITY_INDEX(k) (((uint32_t)(k) & 3u) << 11)
 /* Thermal rule of a boundary node (bits 13-14) and its wall value index into
  * mrlbm_desc.t_wall (bits 15-16): the per-case g_bc_definition.inc switch of

@@ -126,6 +126,8 @@ mrlbm_status refresh(mrlbm_batch* b)
         hd[id].flags = batch_flags(dom);
         if (!flags_supported(hd[id].flags))
             return fail(MRLBM_EINVAL, "batch member %d: physics flag set %d not supported in batches", id, hd[id].flags);
+        if (dom->has_outflow)
+            return fail(MRLBM_EINVAL, "batch member %d: outflow walls are not supported in batches", id);
         hd[id].map[0] = dom->tmap[0];
         hd[id].map[1] = dom->tmap[1];
         hd[id].parity_offset = b->offsets[id];

@@ -38,6 +38,7 @@ struct mrlbm_domain {
     mrlbm::BcClass* bc = nullptr;
     int nclasses = 0;
     bool has_bc = false;
+    bool has_outflow = false;        // some class is an outflow wall (not taken by batches)
     float ext[mrlbm::NM_MAX] = {};
     float scale[mrlbm::NM_MAX] = {}, iscale[mrlbm::NM_MAX] = {};
     int lz = 16;                     // z planes per CTA (batch members: per work item)

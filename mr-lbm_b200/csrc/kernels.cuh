@@ -49,6 +49,7 @@ enum : int {
     F_POWERLAW = 4,  // omega field, power-law viscosity
     F_BINGHAM = 8,   // omega field, Bingham viscosity
     F_THERMAL = 16,  // thermal scalar C on D3G19 (4 more stored moments, Boussinesq force)
+    F_OUTFLOW = 32,  // some wall class is an outflow (selects the OutflowBC policy at launch)
 };
 
 // most stored moments per node: 10 flow moments + omega, or + C and its flux
@@ -88,7 +89,7 @@ struct alignas(16) BcClass {
     uint32_t valid;
     uint32_t word;     // the node-type word of the class (nodeTypeMap encoding)
     uint32_t trule;    // thermal rule (bits 0-1), wall normal axis (bits 2-3, 3 = none),
-                       // solid side of the normal (bit 4: + side)
+                       // solid side of the normal (bit 4: + side), BC kind (bits 8-10)
     float twall;       // thermal wall value
 };
 static_assert(sizeof(BcClass) == 288, "BcClass is read as float4 words");
@@ -96,7 +97,8 @@ static_assert(sizeof(BcClass) == 288, "BcClass is read as float4 words");
 struct StepArgs {
     void* __restrict__ m_out;         // padded planes [nm][nz+2][ny+2][pitch]
     void* out_p[(NM_MAX + 1) / 2];    // plane stack of moment pair p (moments 2p, 2p+1)
-    const float* __restrict__ m_in;   // the buffer being read (thermal wall rules read it)
+    const void* m_in;                 // the buffer being read (outflow and thermal wall rules read it)
+    int storage;                      // its element type (mrlbm_storage)
     const uint8_t* __restrict__ cls;  // padded [nz+2][ny+2][pitch]
     const BcClass* __restrict__ bc;
     int* err;                         // bit 0: a bounded wait timed out
@@ -383,15 +385,65 @@ __device__ __forceinline__ void bc_moments(const BcClass* __restrict__ c, const 
     for (int k = 0; k < 6; k++) mac[4 + k] = X[1 + k] * ir;
 }
 
-// Boundary-node policy of the step kernels: the run-time class table solved by
-// bc_moments (the default), or a case's own bc_definition snippet compiled
-// into a policy of the same shape (case mode).
+// Stored moment m at padded node offset idx of the buffer the step reads, in
+// the stored scaling (FP32, or 16-bit times its storage scale).
+template <typename T>
+__device__ __forceinline__ float load_stored(const StepArgs& a, int m, long long idx)
+{
+    const float v = Stor<T>::ld(static_cast<const T*>(a.m_in) + mphys(m, idx, a.field));
+    return is_f32<T>() ? v : v * a.iscale[m];
+}
+
+// Outflow (nodeTypeMap BC_OUTFLOW, src/cases/mountedCube/bc_definition.inc:18-33,
+// 55-67): the node takes the moments its inward neighbour stored in the
+// previous step, unscaled, and collides them like any node.  (The reference
+// reads its in-place array, whose neighbour entry another thread may or may
+// not have rewritten already in the same step.)
+template <typename T>
+__device__ __forceinline__ void outflow_moments(const StepArgs& a, uint32_t kw, int x, int y, int z, float* mac)
+{
+    const int axis = (int)((kw >> 2) & 3u);
+    const int side = (kw >> 4) & 1u ? 1 : -1;
+    int n[3] = {x, y, z};
+    n[axis] -= side;
+    const long long idx = pidx(n[0], n[1], n[2], a.pitch, a.plane);
+    mac[0] = a.rho0 + load_stored<T>(a, 0, idx);
+    mac[1] = load_stored<T>(a, 1, idx) / 3.0f;
+    mac[2] = load_stored<T>(a, 2, idx) / 3.0f;
+    mac[3] = load_stored<T>(a, 3, idx) / 3.0f;
+    mac[4] = load_stored<T>(a, 4, idx) / 4.5f;
+    mac[5] = load_stored<T>(a, 5, idx) / 9.0f;
+    mac[6] = load_stored<T>(a, 6, idx) / 9.0f;
+    mac[7] = load_stored<T>(a, 7, idx) / 4.5f;
+    mac[8] = load_stored<T>(a, 8, idx) / 9.0f;
+    mac[9] = load_stored<T>(a, 9, idx) / 4.5f;
+}
+
+constexpr uint32_t BC_KIND_OUTFLOW = 2;  // nodeTypeMap bits 8-10
+
+// Boundary-node policies of the step kernels: the run-time class table solved
+// by bc_moments (the default), the same with outflow classes (launched only
+// for domains that have them: the extra branch costs the wall kernels 4-6 %),
+// or a case's own bc_definition snippet compiled into a policy of the same
+// shape (case mode).
 struct TableBC {
-    template <int Q>
+    template <int Q, typename T>
     static __device__ __forceinline__ void apply(const StepArgs& a, uint8_t cls, const float* p, float omega,
                                                  int x, int y, int z, float* mac)
     {
         bc_moments<Q>(a.bc + cls, p, omega, a.omega0, mac);
+    }
+};
+
+struct OutflowBC {
+    template <int Q, typename T>
+    static __device__ __forceinline__ void apply(const StepArgs& a, uint8_t cls, const float* p, float omega,
+                                                 int x, int y, int z, float* mac)
+    {
+        const BcClass* c = a.bc + cls;
+        const uint32_t kw = __ldg(&c->trule);
+        if (((kw >> 8) & 7u) == BC_KIND_OUTFLOW) outflow_moments<T>(a, kw, x, y, z, mac);
+        else bc_moments<Q>(c, p, omega, a.omega0, mac);
     }
 };
 
@@ -707,8 +759,9 @@ __device__ __forceinline__ void thermal_wall(const StepArgs& a, const BcClass* _
     const int side = (tr >> 4) & 1u ? 1 : -1;
     if (rule == 0) {
         // the stored values stand (node types without a thermal rule)
-        C = a.m_in[mphys(10, oidx, a.field)];
-        for (int k = 0; k < 3; k++) q[k] = a.m_in[mphys(11 + k, oidx, a.field)];
+        const float* m_in = static_cast<const float*>(a.m_in);   // thermal domains store FP32
+        C = m_in[mphys(10, oidx, a.field)];
+        for (int k = 0; k < 3; k++) q[k] = m_in[mphys(11 + k, oidx, a.field)];
     } else if (rule == 1 || axis == 3) {
         C = c->twall;
         q[0] = q[1] = q[2] = 0.f;
@@ -718,7 +771,7 @@ __device__ __forceinline__ void thermal_wall(const StepArgs& a, const BcClass* _
         q[0] = q[1] = q[2] = 0.f;
         const long long stride = axis == 0 ? 1LL : (axis == 1 ? (long long)a.pitch : a.plane);
         const long long nb = (long long)oidx - side * stride;
-        q[axis] = a.m_in[mphys(11 + axis, nb, a.field)];
+        q[axis] = static_cast<const float*>(a.m_in)[mphys(11 + axis, nb, a.field)];
     } else {
         // adiabatic: what arrives from the solid side is the mirror image of
         // what leaves towards it
@@ -881,7 +934,7 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
             mac[8] = P[4] * ir;
             mac[9] = P[5] * ir - (1.0f / 3.0f);
             if constexpr ((FLAGS & F_BC) != 0) {
-                if (cls != CLS_BULK && cls != CLS_SOLID) BCP::template apply<Q>(a, cls, p, omega, x, y, zd, mac);
+                if (cls != CLS_BULK && cls != CLS_SOLID) BCP::template apply<Q, T>(a, cls, p, omega, x, y, zd, mac);
             }
             collide<FLAGS>(a, mac, omega, o, Fx, Fy, Fz);
         }

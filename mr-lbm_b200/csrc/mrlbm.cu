@@ -131,9 +131,17 @@ mrlbm_status mrlbm::build_bc_class(int q, int mq, uint32_t word, const double uv
     const uint32_t oct = word & 0xFFu;
     const uint32_t kind = (word >> 8) & 7u;
     const uint32_t vidx = (word >> 11) & 3u;
-    if (kind > 1)
-        return fail(MRLBM_EINVAL, "node type 0x%x: BC kind %u not supported (only no-slip and velocity walls)",
-                    word, kind);
+    if (kind > 2)
+        return fail(MRLBM_EINVAL,
+                    "node type 0x%x: BC kind %u not supported (no-slip and velocity walls, outflow)", word, kind);
+    if (kind == 2) {
+        // outflow: the kernel copies the inward neighbour's moments, no system
+        memset(out, 0, sizeof(*out));
+        out->known = known_mask(q, oct);
+        out->valid = 1;
+        out->word = word;
+        return MRLBM_OK;
+    }
     double u[3] = {0, 0, 0};
     if (kind == 1)
         for (int a = 0; a < 3; a++) u[a] = uvel[vidx][a];
@@ -386,13 +394,13 @@ extern "C" mrlbm_status mrlbm_domain_destroy(mrlbm_domain* dom)
     return MRLBM_OK;
 }
 
-// Thermal rule of a class (bits 13-16 of its word, include/mrlbm.h
-// MRLBM_THERMAL_*): rules 2 and 3 act along the normal of a face node, the
-// axis whose whole + or - half of the octant mask is solid.
-static mrlbm_status thermal_rule_of(uint32_t word, const double t_wall[4], BcClass* c)
+// Wall normal of a face node: the axis whose whole + or - half of the octant
+// mask is solid, when exactly one such (axis, side) exists; axis 3 otherwise.
+// Stored in the class with its BC kind (outflow and the thermal rules act
+// along it).
+static mrlbm_status class_normal(uint32_t word, BcClass* c)
 {
-    const uint32_t rule = (word >> 13) & 3u, idx = (word >> 15) & 3u;
-    const uint32_t oct = word & 0xFFu;
+    const uint32_t oct = word & 0xFFu, kind = (word >> 8) & 7u;
     int axis = 3, side = 0, nfaces = 0;
     for (int a = 0; a < 3; a++)
         for (int sd = 0; sd < 2; sd++) {
@@ -402,9 +410,20 @@ static mrlbm_status thermal_rule_of(uint32_t word, const double t_wall[4], BcCla
             if (all) { axis = a; side = sd; nfaces++; }
         }
     if (nfaces != 1) axis = 3;
-    if ((rule == 2 || rule == 3) && axis == 3)
+    if (kind == 2 && axis == 3)
+        return fail(MRLBM_EINVAL, "node type 0x%x: outflow needs a face node (one solid half)", word);
+    c->trule = ((uint32_t)axis << 2) | ((uint32_t)side << 4) | (kind << 8);
+    return MRLBM_OK;
+}
+
+// Thermal rule of a class (bits 13-16 of its word, include/mrlbm.h
+// MRLBM_THERMAL_*): rules 2 and 3 act along the class's wall normal.
+static mrlbm_status thermal_rule_of(uint32_t word, const double t_wall[4], BcClass* c)
+{
+    const uint32_t rule = (word >> 13) & 3u, idx = (word >> 15) & 3u;
+    if ((rule == 2 || rule == 3) && ((c->trule >> 2) & 3u) == 3u)
         return fail(MRLBM_EINVAL, "node type 0x%x: thermal rule %u needs a face node (one solid half)", word, rule);
-    c->trule = rule | ((uint32_t)axis << 2) | ((uint32_t)side << 4);
+    c->trule |= rule;
     c->twall = (float)t_wall[idx];
     return MRLBM_OK;
 }
@@ -438,6 +457,7 @@ mrlbm_status mrlbm::classify_nodes(int q, int mq, const uint32_t* nt, long long 
             mrlbm_status st = case_mode ? MRLBM_OK : build_bc_class(q, mq, key & 0x1FFFu, uvel, omega0, &c);
             if (st) return st;
             c.word = key;
+            if (!case_mode && (st = class_normal(key, &c))) return st;
             if (t_wall && !case_mode && (st = thermal_rule_of(key, t_wall, &c))) return st;
             const int id = (int)table.size();
             table.push_back(c);
@@ -460,6 +480,11 @@ static mrlbm_status set_node_types_impl(mrlbm_domain* dom, const uint32_t* nt, b
         classify_nodes(dom->q, d.bc_matrix_q, nt, n, d.bc_velocity, dom->omega0, cls, table, any, case_mode,
                        d.thermal ? d.t_wall : nullptr);
     if (st) return st;
+    bool outflow = false;
+    for (const BcClass& c : table)
+        if (!case_mode && ((c.word >> 8) & 7u) == 2u) outflow = true;
+    if (outflow && (d.rheology != MRLBM_NEWTONIAN || d.thermal))
+        return fail(MRLBM_EINVAL, "outflow walls are supported for Newtonian domains without the thermal scalar");
     // scatter into the padded plane layout
     std::vector<uint8_t> padded((size_t)dom->field, 0);
     for (int z = 0; z < d.nz; z++)
@@ -472,6 +497,7 @@ static mrlbm_status set_node_types_impl(mrlbm_domain* dom, const uint32_t* nt, b
     CK(cudaMemcpyAsync(dom->bc, table.data(), table.size() * sizeof(BcClass), cudaMemcpyHostToDevice, dom->stream));
     CK(cudaStreamSynchronize(dom->stream));
     dom->has_bc = any;
+    dom->has_outflow = outflow;
     dom->nclasses = (int)table.size();
     if (dom->graph_exec) { cudaGraphExecDestroy(dom->graph_exec); dom->graph_exec = nullptr; }
     return MRLBM_OK;
@@ -575,7 +601,8 @@ void mrlbm::fill_step_args(const mrlbm_domain* dom, StepArgs& a, int parity, int
 {
     const mrlbm_desc& d = dom->d;
     a.m_out = dom->m[parity ^ 1];
-    a.m_in = static_cast<const float*>(dom->m[parity]);
+    a.m_in = dom->m[parity];
+    a.storage = d.storage;
     for (int p = 0; p < (NM_MAX + 1) / 2; p++)
         a.out_p[p] = 2 * p < dom->nm ? static_cast<char*>(dom->m[parity ^ 1]) + (size_t)p * 2 * dom->field * dom->esize
                                      : nullptr;
@@ -605,6 +632,7 @@ void mrlbm::fill_step_args(const mrlbm_domain* dom, StepArgs& a, int parity, int
     if (d.rheology == MRLBM_BINGHAM) flags |= F_BINGHAM;
     if (flags & (F_POWERLAW | F_BINGHAM)) flags |= F_BC;  // nnf variants always read the class map
     if (d.thermal) flags |= F_THERMAL | F_FORCE;           // the Boussinesq force is per node
+    if (dom->has_outflow) flags |= F_OUTFLOW;
 }
 
 mrlbm_status mrlbm::enqueue_step(mrlbm_domain* dom, int parity, cudaStream_t s)

@@ -9,14 +9,14 @@
 
 namespace mrlbm {
 
-template <int Q, typename T, int FLAGS>
+template <int Q, typename T, int FLAGS, typename BCP = TableBC>
 static mrlbm_status launch_step_t(const CUtensorMap& map, const StepArgs& a, cudaStream_t s)
 {
     constexpr int TYI = tile_y(Q);
     constexpr int NW = TYI + 2;
     constexpr size_t smem = step_smem_bytes<Q, T, FLAGS, TYI>();
     static_assert(smem <= 232448, "shared memory over the sm_100 limit");
-    auto kern = zmarch_step<Q, T, FLAGS, TYI>;
+    auto kern = zmarch_step<Q, T, FLAGS, TYI, BCP>;
     int dev = 0;
     cudaGetDevice(&dev);
     static int attr_done_mask = 0;  // one bit per device (up to 32)
@@ -42,6 +42,9 @@ mrlbm_status dispatch_step(const CUtensorMap& map, const StepArgs& a, int flags,
         case F_BC | F_FORCE | F_POWERLAW: return launch_step_t<Q, T, F_BC | F_FORCE | F_POWERLAW>(map, a, s);
         case F_BC | F_BINGHAM: return launch_step_t<Q, T, F_BC | F_BINGHAM>(map, a, s);
         case F_BC | F_FORCE | F_BINGHAM: return launch_step_t<Q, T, F_BC | F_FORCE | F_BINGHAM>(map, a, s);
+        // outflow walls (Newtonian domains, as the reference's outflow cases)
+        case F_BC | F_OUTFLOW: return launch_step_t<Q, T, F_BC, OutflowBC>(map, a, s);
+        case F_BC | F_FORCE | F_OUTFLOW: return launch_step_t<Q, T, F_BC | F_FORCE, OutflowBC>(map, a, s);
         default: break;
     }
     // thermal scalar: D3Q19 with FP32 storage only (its second row exchange

@@ -22,6 +22,7 @@ NEWTONIAN, POWERLAW, BINGHAM = 0, 1, 2
 NODE_BULK = 0x00
 NODE_SOLID = 0xFF
 BC_VELOCITY_WALL = 1 << 8
+BC_OUTFLOW = 2 << 8
 
 
 def BC_VELOCITY_INDEX(k):

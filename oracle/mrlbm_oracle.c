@@ -19,6 +19,7 @@
  *       sum_{i in I} f_i          = sum_{i in I} f^reg_i(rho, u, (1-w)Pi + w uu)
  *       sum_{i in I} f_i h_k(c_i) = sum_{i in I} h_k(c_i) f^reg_i(rho, u, Pi)
  *   - octant-mask known-set rule      src/lbmInitialization.cu:1080-1227, src/nodeTypeMap.h:10-80
+ *   - outflow walls (BC_OUTFLOW)      src/cases/mountedCube/bc_definition.inc:18-33, 55-67
  *   - collision (with force terms)    src/colrec/MR_LBM/collision.inc:2-14
  *   - shear magnitude + nnf omega     src/mlbm.cu:526-563, src/nnf.h:61-98
  *     (power law with the reference's three compile defects fixed: the
@@ -583,6 +584,18 @@ void orc_step(void *h, int nsteps)
                         real mac[10];
                         if ((t & 0xFFu) == 0) {
                             orc_bulk_moments(q, f, mac);
+                        } else if (((t >> 8) & 7u) == 2) {
+                            /* outflow (BC_OUTFLOW, mountedCube/bc_definition.inc:18-33): the
+                             * inward neighbour's stored moments of the previous step, unscaled */
+                            int side = 0;
+                            const int ax = orc_face_normal(t & 0xFFu, &side);
+                            int nb[3] = {x, y, z};
+                            if (ax >= 0) nb[ax] -= side;
+                            const real *mn = o->m + ((size_t)nb[0] + (size_t)nx * (nb[1] + (size_t)ny * nb[2])) * nm;
+                            mac[0] = d->rho0 + mn[0];
+                            mac[1] = mn[1] / 3.0; mac[2] = mn[2] / 3.0; mac[3] = mn[3] / 3.0;
+                            mac[4] = mn[4] / 4.5; mac[5] = mn[5] / 9.0; mac[6] = mn[6] / 9.0;
+                            mac[7] = mn[7] / 4.5; mac[8] = mn[8] / 9.0; mac[9] = mn[9] / 4.5;
                         } else {
                             int vidx = (t >> 11) & 3u;
                             int kind = (t >> 8) & 7u;

@@ -22,6 +22,7 @@ implementation of the algorithm.
 import numpy as np
 import pytest
 
+import lattice_np
 import mrlbm
 import parity_util as pu
 
@@ -287,3 +288,76 @@ def test_vtk_writer(tmp_path):
     np.testing.assert_array_equal(f["rho"], (np.float32(1.0) + m[0]).reshape(-1))
     np.testing.assert_allclose(f["velocity"], (m[1:4] / np.float32(3.0)).reshape(3, -1).T, rtol=1e-6)
     np.testing.assert_array_equal(f["omega"], m[10].reshape(-1))
+
+
+def channel_node_types(nx, ny, nz, inlet_index=0):
+    """Walled channel along z: no-slip walls on the x and y faces (edges and
+    corners with the z faces are walls too), a velocity inlet on the interior
+    of z = 0 (BACK + BC_VELOCITY_WALL) and an outflow on the interior of
+    z = nz-1 (FRONT + BC_OUTFLOW), as the reference's mountedCube and
+    externalFlow cases type them."""
+    F = lattice_np.FACES
+    z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    side = (x == 0) | (x == nx - 1) | (y == 0) | (y == ny - 1)
+    m = (np.where(x == 0, F["WEST"], 0) | np.where(x == nx - 1, F["EAST"], 0) | np.where(y == 0, F["SOUTH"], 0) |
+         np.where(y == ny - 1, F["NORTH"], 0) | np.where(side & (z == 0), F["BACK"], 0) |
+         np.where(side & (z == nz - 1), F["FRONT"], 0)).astype(np.uint32)
+    m[0][~side[0]] = F["BACK"] | mrlbm.BC_VELOCITY_WALL | mrlbm.BC_VELOCITY_INDEX(inlet_index)
+    m[-1][~side[-1]] = F["FRONT"] | mrlbm.BC_OUTFLOW
+    return m
+
+
+@pytest.mark.parametrize("lattice", [19, 27])
+def test_channel_velocity_inlet_outflow(lattice):
+    """Outflow walls take the moments their inward neighbour stored in the
+    previous step (src/cases/mountedCube/bc_definition.inc:18-33) and collide
+    them; the channel is driven by a velocity inlet, 250 steps."""
+    nx, ny, nz = 20, 18, 36
+    nt = channel_node_types(nx, ny, nz)
+    d = mrlbm.make_desc(nx, ny, nz, lattice=lattice, periodic=(0, 0, 0), tau=0.7, bc_velocity=[(0.0, 0.0, 0.03)])
+    g, o, res, yard = run_pair(d, 250, node_types=nt, yardstick=True)
+    assert_close(res, yard=yard)
+    # the outlet carries the flow out: its velocity follows the plane before it
+    uz = g[3]
+    assert float(np.mean(uz[-1, 1:-1, 1:-1])) > 0.0
+    assert np.allclose(uz[-1, 1:-1, 1:-1], uz[-2, 1:-1, 1:-1], rtol=0.1, atol=3e-3)
+
+
+@pytest.mark.parametrize("storage,tol", [(mrlbm.F16, 3e-3), (mrlbm.BF16, 3e-2)])
+def test_channel_outflow_half_storage(storage, tol):
+    """The outflow read of the 16-bit stored forms (scaled back on load)
+    against FP32 storage: relative L2 of u after 150 steps."""
+    nx, ny, nz = 20, 18, 36
+    nt = channel_node_types(nx, ny, nz)
+    out = []
+    for st in (mrlbm.F32, storage):
+        d = mrlbm.make_desc(nx, ny, nz, lattice=19, storage=st, periodic=(0, 0, 0), tau=0.7,
+                            bc_velocity=[(0.0, 0.0, 0.03)])
+        dom = mrlbm.Domain(d)
+        dom.set_node_types(nt)
+        dom.init_uniform()
+        dom.step(150)
+        out.append(dom.moments()[1:4].astype(np.float64))
+        dom.close()
+    err = float(np.sqrt(np.sum((out[1] - out[0]) ** 2) / np.sum(out[0] ** 2)))
+    assert err < tol, "storage %d: u rel L2 vs FP32 %.3e" % (storage, err)
+
+
+def test_outflow_needs_a_face_node():
+    d = mrlbm.make_desc(8, 8, 8, lattice=19, periodic=(0, 0, 0), tau=0.8)
+    dom = mrlbm.Domain(d)
+    t = np.zeros((8, 8, 8), dtype=np.uint32)
+    t[-1, 0, 0] = lattice_np.FACES["FRONT"] | lattice_np.FACES["WEST"] | mrlbm.BC_OUTFLOW
+    with pytest.raises(mrlbm.MrlbmError):
+        dom.set_node_types(t)
+    dom.close()
+
+
+def test_batch_rejects_outflow_members():
+    b = mrlbm.Batch(mrlbm.D3Q19, mrlbm.F32)
+    m = b.add(mrlbm.make_desc(20, 18, 36, lattice=19, periodic=(0, 0, 0), tau=0.7, bc_velocity=[(0, 0, 0.03)]))
+    m.set_node_types(channel_node_types(20, 18, 36))
+    m.init_uniform()
+    with pytest.raises(mrlbm.MrlbmError):
+        b.step(1)
+    b.close()
