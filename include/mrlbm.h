@@ -178,6 +178,13 @@ mrlbm_status mrlbm_step_graph(mrlbm_domain* dom, int nsteps);
 /* Device-timed nsteps: CUDA events on the domain's stream around the launches. */
 mrlbm_status mrlbm_time_steps(mrlbm_domain* dom, int nsteps, float* ms);
 mrlbm_status mrlbm_synchronize(mrlbm_domain* dom);
+/* Self-test of the bounded device waits that guard every tile load of the
+ * step kernels (no counterpart in the reference, whose kernel has none): a
+ * one-CTA kernel waits on a barrier that is never completed, gives up after
+ * `polls` polls (1..2^26; the step kernels use 2^26), raises the device error
+ * flag and exits.  Returns MRLBM_ETIMEDOUT (the expected outcome) with the
+ * kernel's duration in *seconds; the context stays usable. */
+mrlbm_status mrlbm_selftest_bounded_wait(unsigned polls, double* seconds);
 mrlbm_status mrlbm_get_step(mrlbm_domain* dom, int* step);
 
 /* Moments in the reference's idxMom layout (fMom, host float buffer of

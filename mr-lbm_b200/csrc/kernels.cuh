@@ -546,10 +546,10 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes)
 }
 
 // Bounded wait on the phase with the given parity; returns false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, unsigned limit = WAIT_LIMIT)
 {
     const uint32_t a = smem_u32(bar);
-    for (unsigned it = 0; it < WAIT_LIMIT; it++) {
+    for (unsigned it = 0; it < limit; it++) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"

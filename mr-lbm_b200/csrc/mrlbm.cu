@@ -736,6 +736,51 @@ extern "C" mrlbm_status mrlbm_synchronize(mrlbm_domain* dom)
     return check_device_error(dom);
 }
 
+// Self-test of the bounded waits: one CTA waits on an mbarrier whose single
+// expected arrival never comes, gives up after `polls` polls, raises the
+// error flag the step kernels raise, and exits; the host reads the flag.
+__global__ void bounded_wait_selftest_kernel(int* err, unsigned polls)
+{
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const bool ok = mbar_wait(&bar, 0u, polls);
+    if (!ok && threadIdx.x == 0) atomicOr(err, 1);
+}
+
+extern "C" mrlbm_status mrlbm_selftest_bounded_wait(unsigned polls, double* seconds)
+{
+    if (polls == 0 || polls > WAIT_LIMIT) return fail(MRLBM_EINVAL, "polls must be in 1..%u", WAIT_LIMIT);
+    int* d_err = nullptr;
+    CK(cudaMalloc(&d_err, sizeof(int)));
+    cudaError_t e = cudaMemset(d_err, 0, sizeof(int));
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    if (e == cudaSuccess) e = cudaEventCreate(&t0);
+    if (e == cudaSuccess) e = cudaEventCreate(&t1);
+    int h = 0;
+    float ms = 0.f;
+    if (e == cudaSuccess) {
+        cudaEventRecord(t0);
+        bounded_wait_selftest_kernel<<<1, 32>>>(d_err, polls);
+        cudaEventRecord(t1);
+        e = cudaEventSynchronize(t1);
+    }
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) cudaEventElapsedTime(&ms, t0, t1);
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
+    cudaFree(d_err);
+    if (e != cudaSuccess) return fail(MRLBM_ECUDA, "bounded-wait self-test: %s", cudaGetErrorString(e));
+    if (seconds) *seconds = ms * 1e-3;
+    if (h) return fail(MRLBM_ETIMEDOUT, "bounded-wait self-test: the wait gave up after %u polls (%.3f s)", polls,
+                       ms * 1e-3);
+    return MRLBM_OK;
+}
+
 extern "C" mrlbm_status mrlbm_get_step(mrlbm_domain* dom, int* step)
 {
     if (!dom || !step) return fail(MRLBM_EINVAL, "null argument");

@@ -180,6 +180,7 @@ def lib():
             "mrlbm_request_domain": [C.POINTER(Request), C.c_int, C.POINTER(VP)],
             "mrlbm_reduce_fp64_ref_layout_noalloc": [VP, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, VP,
                                                      C.POINTER(Sums)],
+            "mrlbm_selftest_bounded_wait": [C.c_uint, C.POINTER(C.c_double)],
         }
         for name, args in sigs.items():
             f = getattr(L, name)
@@ -196,6 +197,13 @@ def check(status):
 
 def _fp(a):
     return a.ctypes.data_as(FP)
+
+
+def selftest_bounded_wait(polls):
+    """Run the bounded-wait self-test; returns (status, seconds)."""
+    sec = C.c_double()
+    st = lib().mrlbm_selftest_bounded_wait(C.c_uint(int(polls)), C.byref(sec))
+    return st, sec.value
 
 
 def set_device(dev):

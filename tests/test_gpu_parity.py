@@ -361,3 +361,16 @@ def test_batch_rejects_outflow_members():
     with pytest.raises(mrlbm.MrlbmError):
         b.step(1)
     b.close()
+
+
+def test_bounded_wait_gives_up_and_context_survives():
+    """Failure detection without a fault: a device wait on a barrier nothing
+    completes gives up after its poll limit and raises the error flag the
+    step kernels raise (MRLBM_ETIMEDOUT on the host); the context then runs
+    a normal step.  2^16 polls: well under a second."""
+    st, sec = mrlbm.selftest_bounded_wait(1 << 16)
+    assert st == 6, "expected MRLBM_ETIMEDOUT, got %d" % st   # MRLBM_ETIMEDOUT
+    assert 0.0 < sec < 5.0
+    d = mrlbm.make_desc(24, 20, 16, lattice=19, tau=0.7)
+    g, o, res = run_pair(d, 5, init=tg_init(0.02, 24 / (2 * np.pi)))
+    assert_close(res)
