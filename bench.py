@@ -469,6 +469,51 @@ def moment_errors(a, b, rho0=1.0):
     return out, float(np.sqrt(du / uu))
 
 
+def run_thermal_workload(args):
+    """Thermal scalar (D3Q19 flow + D3G19 scalar, FP32): the Rayleigh-Benard
+    cell of src/cases/rayleighBenard_Periodic scaled to N^3 (hot / cold walls
+    in x with the neighbour-flux rule, gravity along x, periodic y and z, Pr 10,
+    Ra 1e5), device-timed like the step benchmark, next to the same walled
+    flow without the scalar."""
+    import mrlbm
+
+    mrlbm.set_device(0)
+    n = 256
+    tau = 0.55
+    nu = (tau - 0.5) / 3
+    alpha = nu / 10.0
+    gb = 1e5 * alpha * nu / n ** 3
+    t = np.zeros((n, n, n), dtype=np.uint32)
+    rule = mrlbm.THERMAL_RULE(mrlbm.THERMAL_DIRICHLET_FLUX)
+    t[:, :, 0] = mrlbm.WEST | rule | mrlbm.THERMAL_INDEX(0)
+    t[:, :, -1] = mrlbm.EAST | rule | mrlbm.THERMAL_INDEX(1)
+    out = {}
+    for th in (True, False):
+        kw = dict(thermal=dict(diffusivity=alpha, reference=1.0, gravity_beta=(gb, 0, 0), wall=(1.5, 0.5))) if th else {}
+        d = mrlbm.make_desc(n, n, n, lattice=19, periodic=(0, 1, 1), tau=tau, **kw)
+        dom = mrlbm.Domain(d)
+        dom.set_node_types(t)
+        dom.init_uniform()
+        dom.step(max(args.warmup, 3))
+        dom.synchronize()
+        ms = dom.time_steps(args.steps)
+        sums = dom.sums()
+        dom.close()
+        out["thermal" if th else "flow"] = {"mlups": round(args.steps * n ** 3 / (ms * 1e-3) / 1e6, 1),
+                                            "ms_per_step": round(ms / args.steps, 5),
+                                            "finite": bool(sums["nonfinite"] == 0)}
+    b_alg = 2 * 14 * 4 + 1
+    line = {"metric": "MLUPS (fused step with the thermal scalar)", "value": out["thermal"]["mlups"], "unit": "MLUPS",
+            "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3), "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic (rest state, hot and cold walls)",
+            "config": {"workload": "rayleigh_benard_%d^3_d3q19_d3g19_fp32" % n, "pr": 10, "ra": 1e5,
+                       "bytes_per_lup_algorithmic": b_alg},
+            "hbm_gbs_algorithmic": round(out["thermal"]["mlups"] * 1e6 * b_alg / 1e9, 1),
+            "same_walls_without_scalar": out["flow"], "thermal": out["thermal"]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_precision_workload(args):
     """Storage precision study: the Taylor-Green vortex, D3Q27, n^3 (512 by
     default), Re 1600, u0 0.04, 1000 steps, with the moments stored as FP32,
@@ -539,9 +584,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
-    ap.add_argument("--workload", default="tgv", choices=["tgv", "batch", "serve", "precision"],
-                    help="tgv: the headline step benchmark (default); batch / serve / precision: the "
-                         "batched-cavity, serving and storage-precision workloads (longer, run on their own)")
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "batch", "serve", "precision", "thermal"],
+                    help="tgv: the headline step benchmark (default); batch / serve / precision / thermal: the "
+                         "batched-cavity, serving, storage-precision and thermal-scalar workloads (run on their own)")
     ap.add_argument("--lattice", type=int, default=27, choices=[19, 27],
                     help="tgv workload: velocity set (D3Q27 is the benchmark's; D3Q19 for comparison)")
     ap.add_argument("--n", type=int, default=512, help="precision workload: grid edge")
@@ -565,6 +610,8 @@ def main():
         return run_serve_workload(args)
     if args.workload == "precision":
         return run_precision_workload(args)
+    if args.workload == "thermal":
+        return run_thermal_workload(args)
     return run_gpu_arm(args)
 
 
