@@ -236,6 +236,15 @@ static mrlbm_status validate(const mrlbm_desc* d)
     if (d->rheology < 0 || d->rheology > 2) return fail(MRLBM_EINVAL, "bad rheology");
     if (d->bc_matrix_q != 0 && d->bc_matrix_q != 19 && d->bc_matrix_q != d->lattice)
         return fail(MRLBM_EINVAL, "bc_matrix_q must be 0, 19 or the lattice size");
+    {
+        // the step kernel addresses a node within one moment's plane stack
+        // with 32-bit offsets
+        const long long pitch = (d->nx + XOFF + 1 + 7) / 8 * 8;
+        const long long field = pitch * (d->ny + 2) * (long long)(d->nz + 2);
+        if (field >= (1LL << 32))
+            return fail(MRLBM_EINVAL, "domain %d x %d x %d: %lld padded nodes per moment, the limit is 2^32", d->nx,
+                        d->ny, d->nz, field);
+    }
     if (d->thermal != 0 && d->thermal != 1) return fail(MRLBM_EINVAL, "thermal must be 0 or 1");
     if (d->thermal) {
         // the second distribution's row exchange and ring fit next to the

@@ -179,3 +179,16 @@ def test_descriptor_layout_matches_header():
         vals = [int(v) for v in subprocess.check_output([exe]).split()]
     D = mrlbm.Desc
     assert vals == [C.sizeof(D), D.bc_matrix_q.offset, D.thermal.offset, D.t_wall.offset]
+
+
+def test_size_limits():
+    """Grids up to 8192 per axis whose padded plane stack of one moment stays
+    below 2^32 nodes (the step kernel's 32-bit offsets) are accepted; larger
+    ones and empty axes are rejected before anything is allocated."""
+    import mrlbm
+    n = C.c_size_t()
+    ok = mrlbm.make_desc(1600, 1600, 1600, lattice=19, storage=mrlbm.F16)
+    assert mrlbm.lib().mrlbm_domain_bytes(C.byref(ok), C.byref(n)) == 0
+    for shape in ((2048, 2048, 2048), (0, 8, 8), (8, 8, 8193)):
+        d = mrlbm.make_desc(*shape, lattice=19)
+        assert mrlbm.lib().mrlbm_domain_bytes(C.byref(d), C.byref(n)) == 1, shape

@@ -374,3 +374,19 @@ def test_bounded_wait_gives_up_and_context_survives():
     d = mrlbm.make_desc(24, 20, 16, lattice=19, tau=0.7)
     g, o, res = run_pair(d, 5, init=tg_init(0.02, 24 / (2 * np.pi)))
     assert_close(res)
+
+
+@pytest.mark.parametrize("shape,lattice", [((1, 12, 10), 19), ((9, 1, 7), 19), ((8, 6, 1), 27), ((30, 14, 5), 19),
+                                           ((31, 15, 3), 27), ((61, 29, 2), 19), ((2, 2, 2), 27)])
+def test_edge_shapes_random_field(shape, lattice):
+    """Shapes at the edges of the decomposition: one-node axes (a node is its
+    own periodic neighbour and holds both ghost copies), columns exactly one
+    tile wide and one node over, z depths below the chunk, a 2^3 box; seeded
+    random field, periodic, against the oracle."""
+    nx, ny, nz = shape
+    d = mrlbm.make_desc(nx, ny, nz, lattice=lattice, tau=0.7)
+    rng = np.random.default_rng(nx * 10000 + ny * 100 + nz)
+    rho = 1 + 0.01 * rng.standard_normal((nz, ny, nx))
+    u = 0.02 * rng.standard_normal((3, nz, ny, nx))
+    g, o, res = run_pair(d, 12, init=lambda dom: dom.init_flow(rho, u[0], u[1], u[2]))
+    assert_close(res)
