@@ -5,7 +5,8 @@
 //   f_i*(x) = f_i^post(x - c_i)   with f^post reconstructed from the stored
 //                                 post-collision moments of the source node,
 // then the new moments (bulk sums, or the moment-space wall BC), and collides
-// them in moment space.  Only the 10 (11) moments live in HBM.
+// them in moment space.  Only the 10 moments (11 with an omega field, 14 with
+// the thermal scalar C and its flux) live in HBM.
 //
 // B200 design (z-marching, ping-pong moments, TMA-fed):
 //   * Moments are stored in pairs (moments 2p and 2p + 1 side by side per
@@ -31,6 +32,12 @@
 //     stay in registers: a plane's c_z=+1 populations are held until the next
 //     plane, its c_z=0 ones until the output of the same plane is formed one
 //     step later.  Output plane z is completed when plane z+1 is produced.
+//     A pipeline step holds the consumption of plane k-1 and the production
+//     of plane k between plain per-plane barriers; they are independent, and
+//     their order in the source only steers the compiler's schedule.
+//   * The thermal scalar (D3G19) rides the same pipeline with a second row
+//     exchange; outflow walls read the inward neighbour from the buffer the
+//     step reads (kernel variants launched only for domains that have them).
 //   * DRAM traffic is the algorithmic 2*M*s bytes per node; halo re-reads of
 //     neighbouring columns hit L2.
 #pragma once
