@@ -111,4 +111,21 @@ constexpr dfloat OMEGA_P = (dfloat)(1.0) / (3.0 * VISC + 0.5);
 #error "case model.inc must define COLLISION_TYPE"
 #endif
 #define CASE_API_COLLISION_MR_LBM 1
+// moment indices of fMom (src/arrayIndex.h:8-50): the flow's, omega, then the
+// thermal scalar's
+constexpr int M_RHO_INDEX = 0, M_UX_INDEX = 1, M_UY_INDEX = 2, M_UZ_INDEX = 3, M_MXX_INDEX = 4, M_MXY_INDEX = 5,
+              M_MXZ_INDEX = 6, M_MYY_INDEX = 7, M_MYZ_INDEX = 8, M_MZZ_INDEX = 9;
+#if defined(OMEGA_FIELD)
+constexpr int M_OMEGA_INDEX = 10;
+constexpr int CASE_API_M_NEXT = 11;
+#else
+constexpr int CASE_API_M_NEXT = 10;
+#endif
+#if defined(SECOND_DIST)
+constexpr int M2_C_INDEX = CASE_API_M_NEXT, M2_CX_INDEX = CASE_API_M_NEXT + 1, M2_CY_INDEX = CASE_API_M_NEXT + 2,
+              M2_CZ_INDEX = CASE_API_M_NEXT + 3;
+// D3G19 weights (src/includeFiles/velocitySets/D3G19.inc)
+constexpr unsigned char GQ = 19;
+constexpr dfloat gW0 = 1.0 / 3, gW1 = 1.0 / 18, gW2 = 1.0 / 36;
+#endif
 #endif

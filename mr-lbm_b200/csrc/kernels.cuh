@@ -433,12 +433,22 @@ constexpr uint32_t BC_KIND_OUTFLOW = 2;  // nodeTypeMap bits 8-10
 // for domains that have them: the extra branch costs the wall kernels 4-6 %),
 // or a case's own bc_definition snippet compiled into a policy of the same
 // shape (case mode).
+__device__ __forceinline__ void thermal_wall(const StepArgs& a, const BcClass* __restrict__ c, const float* pg,
+                                             unsigned oidx, float& C, float* q);
+
 struct TableBC {
     template <int Q, typename T>
     static __device__ __forceinline__ void apply(const StepArgs& a, uint8_t cls, const float* p, float omega,
                                                  int x, int y, int z, float* mac)
     {
         bc_moments<Q>(a.bc + cls, p, omega, a.omega0, mac);
+    }
+    // C and 3 sum g c at a thermal boundary node: the class's run-time rule
+    template <typename T>
+    static __device__ __forceinline__ void thermal(const StepArgs& a, uint8_t cls, const float* pg, unsigned oidx,
+                                                   int x, int y, int z, float& C, float* q)
+    {
+        thermal_wall(a, a.bc + cls, pg, oidx, C, q);
     }
 };
 
@@ -451,6 +461,12 @@ struct OutflowBC {
         const uint32_t kw = __ldg(&c->trule);
         if (((kw >> 8) & 7u) == BC_KIND_OUTFLOW) outflow_moments<T>(a, kw, x, y, z, mac);
         else bc_moments<Q>(c, p, omega, a.omega0, mac);
+    }
+    template <typename T>
+    static __device__ __forceinline__ void thermal(const StepArgs& a, uint8_t cls, const float* pg, unsigned oidx,
+                                                   int x, int y, int z, float& C, float* q)
+    {
+        thermal_wall(a, a.bc + cls, pg, oidx, C, q);
     }
 };
 
@@ -919,7 +935,7 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
                 Fy = fmaf(a.t_gb[1], dC, Fy);
                 Fz = fmaf(a.t_gb[2], dC, Fz);
             } else if (cls != CLS_SOLID) {
-                thermal_wall(a, a.bc + cls, pg, oidx, tC, tq);
+                BCP::template thermal<T>(a, cls, pg, oidx, x, y, zd, tC, tq);
             }
         }
         if constexpr ((FLAGS & (F_BC | F_POWERLAW | F_BINGHAM)) == 0) {

@@ -112,4 +112,7 @@ $PY "$CB" "$REF/src/cases/lidDrivenCavity_3D" -o "$OUT/cases/lid64" --set N=64 -
 $PY "$CB" "$REF/src/cases/taylorGreen" -o "$OUT/cases/tgv256_q27" --lattice 27 --set N=256 --set RE=1600 \
     --set U_MAX=0.04 --set N_STEPS=1000 --set "REPORT_SAVE=(100)" --set "SAVEDATA=(true)" $common_out
 $PY "$CB" "$REF/src/cases/benchmark" -o "$OUT/cases/bench256" --set N_STEPS=1000 $common_out
+# thermal: rayleighBenard_Periodic as refsim_rb64 runs it (NZ = 8, 1000 steps)
+$PY "$CB" "$REF/src/cases/rayleighBenard_Periodic" -o "$OUT/cases/rb64" --set NZ=8 --set N_STEPS=1000 \
+    --set "REPORT_SAVE=(false)" $common_out
 echo "built case-mode programs in $OUT/cases"

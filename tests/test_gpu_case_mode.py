@@ -98,3 +98,29 @@ def test_lid_case_bc_snippet_equals_generic_solver(tmp_path):
     e = u_err(case, lib)
     print("lid64: case's own bc_definition vs generic solver, u rel L2 %.2e" % e)
     assert e < 1e-4
+
+
+def test_thermal_case_matches_reference_program(tmp_path):
+    """rayleighBenard_Periodic (D3Q19 + D3G19, 64 x 64 x 8, 1000 steps)
+    compiled unchanged in case mode -- its bc_definition.inc and its
+    g_bc_definition.inc, whose walls read fMom[idxMom(threadIdx.x - 1, ...)],
+    run inside the step kernel -- against the reference's own program on the
+    same case: C and rho agree to FP32 operation order, velocity (a rest state
+    up to round-off, |u| ~ 1e-6) in absolute terms against the free-fall
+    velocity of the case."""
+    run(os.path.join(REF, "refsim_rb64"), tmp_path / "ref")
+    run(os.path.join(REF, "cases", "rb64"), tmp_path / "ours")
+    shape = (8, 64, 64)
+    out = {}
+    for who in ("ref", "ours"):
+        base = os.path.join(tmp_path / who, "TEST", "000", "000_")
+        out[who] = {v: np.fromfile(base + "%s%06d.bin" % (v, 1000), dtype=np.float32).reshape(shape).astype(np.float64)
+                    for v in ("rho", "ux", "uy", "uz", "C")}
+    a, b = out["ours"], out["ref"]
+    c_err = float(np.sqrt(np.sum((a["C"] - b["C"]) ** 2) / np.sum((b["C"] - 1.0) ** 2)))
+    const = np.load(os.path.join(ROOT, "tests", "golden", "ref_kat.npz"))["rbp_const"]
+    u_scale = 3.0 * np.sqrt(const[2] * (const[5] - const[6]) * 64)
+    u_err = max(float(np.max(np.abs(a[k] - b[k]))) for k in ("ux", "uy", "uz")) / u_scale
+    rho_err = float(np.max(np.abs(a["rho"] - b["rho"])))
+    print("RB case mode vs reference program: C rel L2 %.3e, max|du| / U %.3e, max|drho| %.3e" % (c_err, u_err, rho_err))
+    assert c_err < 1e-4 and u_err < 2e-4 and rho_err < 1e-5
