@@ -45,6 +45,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cstdint>
+#include <type_traits>
 
 #include "lattice.cuh"
 
@@ -164,6 +165,15 @@ template <typename T>
 constexpr bool is_f32()
 {
     return sizeof(T) == 4;
+}
+
+// FP16 storage carries power-of-two scales per moment (the shifted moments
+// would otherwise fall into its subnormal range); BF16 has FP32's exponent
+// range and is stored unscaled, so its loads and stores skip the multiplies.
+template <typename T>
+constexpr bool scaled_storage()
+{
+    return std::is_same<T, __half>::value;
 }
 
 // a moment pair of one node: 8 bytes (FP32) or 4 bytes (FP16 / BF16)
@@ -398,7 +408,7 @@ template <typename T>
 __device__ __forceinline__ float load_stored(const StepArgs& a, int m, long long idx)
 {
     const float v = Stor<T>::ld(static_cast<const T*>(a.m_in) + mphys(m, idx, a.field));
-    return is_f32<T>() ? v : v * a.iscale[m];
+    return scaled_storage<T>() ? v * a.iscale[m] : v;
 }
 
 // Outflow (nodeTypeMap BC_OUTFLOW, src/cases/mountedCube/bc_definition.inc:18-33,
@@ -692,8 +702,8 @@ __device__ __forceinline__ void prod_a(const StepArgs& a, const T* sp, float4* e
 #pragma unroll
     for (int p = 0; p < (NM + 1) / 2; p++) {
         const float2 v = Stor2<T>::lds(sp + p * 2 * BOX_X);
-        mc[2 * p] = is_f32<T>() ? v.x : v.x * a.iscale[2 * p];
-        if (2 * p + 1 < NM) mc[2 * p + 1] = is_f32<T>() ? v.y : v.y * a.iscale[2 * p + 1];
+        mc[2 * p] = scaled_storage<T>() ? v.x * a.iscale[2 * p] : v.x;
+        if (2 * p + 1 < NM) mc[2 * p + 1] = scaled_storage<T>() ? v.y * a.iscale[2 * p + 1] : v.y;
     }
     float f[Q];
     reconstruct<Q>(mc, a.rho0, f);
@@ -965,7 +975,7 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
             o[10] = tC;
             o[11] = tq[0]; o[12] = tq[1]; o[13] = tq[2];
         }
-        if constexpr (!is_f32<T>()) {
+        if constexpr (scaled_storage<T>()) {
 #pragma unroll
             for (int m = 0; m < NM; m++) o[m] = o[m] * a.scale[m];
         }

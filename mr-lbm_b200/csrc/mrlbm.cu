@@ -215,9 +215,10 @@ void mrlbm::storage_scales(int storage, float* scale, float* iscale)
 {
     for (int k = 0; k < NM_MAX; k++) {
         float s = 1.0f;
-        if (storage != MRLBM_F32) {
+        if (storage == MRLBM_F16) {
             // powers of two keep values of the shifted moments in the normal
-            // range of fp16 (exact, no rounding from the scaling itself)
+            // range of fp16 (exact, no rounding from the scaling itself);
+            // bf16 has fp32's exponent range and needs none
             s = k == 0 ? 256.0f : (k <= 3 ? 8.0f : (k <= 9 ? 64.0f : 1.0f));
         }
         scale[k] = s;
