@@ -514,6 +514,70 @@ def run_thermal_workload(args):
     return 0
 
 
+def run_zslab_workload(args):
+    """Z-slab decomposition on one GPU: the benchmark vortex (D3Q27, 256^3,
+    FP32) cut into 2 and 4 slabs, each a library domain on its own stream with
+    the plane exchange (device copies) after every step, device-timed next to
+    the undivided domain.  On one GPU the slabs share the SMs, so this measures
+    what the cut and the exchange cost, not multi-GPU scaling; the moments
+    after the timed steps are checked equal to the undivided run's."""
+    import torch
+
+    import mrlbm
+    import zslab
+
+    mrlbm.set_device(0)
+    torch.cuda.set_device(0)
+    n = 256
+    L = n / (2 * np.pi)
+    tau = 0.5 + 3.0 * 0.04 * L / 1600.0
+    d = mrlbm.make_desc(n, n, n, lattice=27, tau=tau)
+    warm = max(args.warmup, 3)
+    mono = mrlbm.Domain(d)
+    mono.init_taylor_green(0.04, L)
+    m0 = mono.moments()
+    mono.step(warm)
+    mono.synchronize()
+    ms = mono.time_steps(args.steps)
+    want = mono.moments()
+    mono.close()
+    out = {"undivided": {"mlups": round(args.steps * n ** 3 / (ms * 1e-3) / 1e6, 1),
+                         "ms_per_step": round(ms / args.steps, 5)}}
+    for parts in (2, 4):
+        zs = zslab.ZSlabDomain.local(d, parts)
+        zs.set_moments(m0)
+        zs.step(warm)
+        zs.synchronize()
+        streams = [torch.cuda.ExternalStream(s.dom.get_stream()) for s in zs.slabs]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(streams[0])
+        for st in streams[1:]:
+            st.wait_event(e0)
+        zs.step(args.steps)
+        for st in streams[1:]:
+            ev = torch.cuda.Event()
+            ev.record(st)
+            streams[0].wait_event(ev)
+        e1.record(streams[0])
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        p = zs.slabs[0].dom.zplane(mrlbm.ZPLANE_FIRST)
+        equal = bool(np.array_equal(zs.moments(), want))
+        zs.close()
+        out["slabs_%d" % parts] = {"mlups": round(args.steps * n ** 3 / (ms * 1e-3) / 1e6, 1),
+                                   "ms_per_step": round(ms / args.steps, 5),
+                                   "exchange_bytes_per_step": 2 * parts * p["npairs"] * p["bytes"],
+                                   "equal_to_undivided": equal}
+    line = {"metric": "MLUPS (z-slab decomposition on one GPU)", "value": out["slabs_4"]["mlups"], "unit": "MLUPS",
+            "n_gpus": 1, "steps": args.steps, "warmup": warm, "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic (analytic Taylor-Green initial field)",
+            "config": {"workload": "taylor_green_256^3_d3q27_fp32_zslabs", "slabs": [2, 4],
+                       "l2": "inputs larger than L2"},
+            **out}
+    print(json.dumps(line), flush=True)
+    return 0 if all(v.get("equal_to_undivided", True) for v in out.values()) else 1
+
+
 def run_precision_workload(args):
     """Storage precision study: the Taylor-Green vortex, D3Q27, n^3 (512 by
     default), Re 1600, u0 0.04, 1000 steps, with the moments stored as FP32,
@@ -584,9 +648,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
-    ap.add_argument("--workload", default="tgv", choices=["tgv", "batch", "serve", "precision", "thermal"],
-                    help="tgv: the headline step benchmark (default); batch / serve / precision / thermal: the "
-                         "batched-cavity, serving, storage-precision and thermal-scalar workloads (run on their own)")
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "batch", "serve", "precision", "thermal", "zslab"],
+                    help="tgv: the headline step benchmark (default); batch / serve / precision / thermal / zslab: "
+                         "the batched-cavity, serving, storage-precision, thermal-scalar and z-slab workloads (run "
+                         "on their own)")
     ap.add_argument("--lattice", type=int, default=27, choices=[19, 27],
                     help="tgv workload: velocity set (D3Q27 is the benchmark's; D3Q19 for comparison)")
     ap.add_argument("--n", type=int, default=512, help="precision workload: grid edge")
@@ -612,6 +677,8 @@ def main():
         return run_precision_workload(args)
     if args.workload == "thermal":
         return run_thermal_workload(args)
+    if args.workload == "zslab":
+        return run_zslab_workload(args)
     return run_gpu_arm(args)
 
 

@@ -187,6 +187,43 @@ mrlbm_status mrlbm_synchronize(mrlbm_domain* dom);
 mrlbm_status mrlbm_selftest_bounded_wait(unsigned polls, double* seconds);
 mrlbm_status mrlbm_get_step(mrlbm_domain* dom, int* step);
 
+/* Launch on a caller's stream (a cudaStream_t of the domain's device; NULL
+ * returns to the domain's own stream, so the legacy default stream cannot be
+ * chosen).  The stream must outlive the domain or be reset first.  Work already queued on the previous
+ * stream is ordered before anything queued afterwards.  No reference
+ * counterpart (the reference launches on the default stream, src/main.cu:183). */
+mrlbm_status mrlbm_set_stream(mrlbm_domain* dom, void* stream);
+mrlbm_status mrlbm_get_stream(mrlbm_domain* dom, void** stream);
+
+/* Z-slab decomposition: one domain cut into slabs of whole z planes, each an
+ * ordinary domain (non-periodic in z) on its own GPU or all on one.  After
+ * every step each slab's z ghost planes are filled from its neighbours'
+ * boundary planes; the step kernel then reads them locally.  The reference is
+ * single-GPU (README.md:38); the exchanged planes play the part of its Z_0 /
+ * Z_1 ghost faces (src/globalStructs.h ghostInterfaceData, the z faces).
+ *
+ * A plane is, for every moment pair, one padded z plane of the buffer the next
+ * step reads (x/y ghost shell included, so periodic x/y copies travel with
+ * it): npairs blocks of `bytes` bytes, `pair_stride` bytes apart, starting at
+ * device address `base`.  The pointers change after every step (ping-pong). */
+#define MRLBM_ZPLANE_FIRST 0        /* interior plane z = 0: goes to the slab below */
+#define MRLBM_ZPLANE_LAST 1         /* interior plane z = nz - 1: goes to the slab above */
+#define MRLBM_ZGHOST_BELOW 2        /* ghost plane z = -1: filled from the slab below */
+#define MRLBM_ZGHOST_ABOVE 3        /* ghost plane z = nz: filled from the slab above */
+typedef struct {
+    void* base;
+    long long pair_stride;
+    long long bytes;
+    int npairs;
+    int device;
+} mrlbm_zplane;
+mrlbm_status mrlbm_zslab_plane(mrlbm_domain* dom, int which, mrlbm_zplane* out);
+/* Device copy of src's plane `src_which` (FIRST or LAST) into dst's ghost plane
+ * `dst_which` (BELOW or ABOVE): one strided copy on src's stream, ordered after
+ * the work queued on both domains' streams and before dst's later work.  The
+ * two domains must have the same nx, ny, lattice, storage and moments. */
+mrlbm_status mrlbm_zslab_copy(mrlbm_domain* src, int src_which, mrlbm_domain* dst, int dst_which);
+
 /* Moments in the reference's idxMom layout (fMom, host float buffer of
  * nx*ny*nz*num_moments).  Used by checkpoints and drop-in callers. */
 mrlbm_status mrlbm_num_moments(mrlbm_domain* dom, int* nm);

@@ -43,8 +43,11 @@ struct mrlbm_domain {
     float scale[mrlbm::NM_MAX] = {}, iscale[mrlbm::NM_MAX] = {};
     int lz = 16;                     // z planes per CTA (batch members: per work item)
     int nsm = 148;                   // SMs of the device the domain lives on
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;      // where the domain's work is queued
+    cudaStream_t own_stream = nullptr;  // the stream the domain created (stream unless mrlbm_set_stream)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t xev = nullptr;          // stream ordering (set_stream, z-slab copies)
+    int device = 0;
     double* red_scratch = nullptr;  // block partials + 8 results
     double* red_host = nullptr;     // pinned
     int red_blocks = 0;

@@ -313,8 +313,11 @@ mrlbm_status mrlbm::domain_alloc(mrlbm_domain* dom)
     }
     memcpy(dom->ext, ext, sizeof(ext));
     CK(cudaStreamCreateWithFlags(&dom->stream, cudaStreamNonBlocking));
+    dom->own_stream = dom->stream;
+    CK(cudaGetDevice(&dom->device));
     CK(cudaEventCreate(&dom->ev0));
     CK(cudaEventCreate(&dom->ev1));
+    CK(cudaEventCreateWithFlags(&dom->xev, cudaEventDisableTiming));
     CK(cudaMalloc(&dom->cls, (size_t)dom->field));
     CK(cudaMemset(dom->cls, 0, (size_t)dom->field));
     CK(cudaMalloc(&dom->err, sizeof(int)));
@@ -399,7 +402,8 @@ extern "C" mrlbm_status mrlbm_domain_destroy(mrlbm_domain* dom)
     if (dom->red_host) cudaFreeHost(dom->red_host);
     if (dom->ev0) cudaEventDestroy(dom->ev0);
     if (dom->ev1) cudaEventDestroy(dom->ev1);
-    if (dom->stream) cudaStreamDestroy(dom->stream);
+    if (dom->xev) cudaEventDestroy(dom->xev);
+    if (dom->own_stream) cudaStreamDestroy(dom->own_stream);
     delete dom;
     return MRLBM_OK;
 }

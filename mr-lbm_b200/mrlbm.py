@@ -88,6 +88,15 @@ class Sums(C.Structure):
 REQ_LID_CAVITY, REQ_DUCT = 0, 1
 
 
+# z-slab plane selectors (include/mrlbm.h MRLBM_ZPLANE_* / MRLBM_ZGHOST_*)
+ZPLANE_FIRST, ZPLANE_LAST, ZGHOST_BELOW, ZGHOST_ABOVE = 0, 1, 2, 3
+
+
+class ZPlane(C.Structure):
+    _fields_ = [("base", C.c_void_p), ("pair_stride", C.c_longlong), ("bytes", C.c_longlong),
+                ("npairs", C.c_int), ("device", C.c_int)]
+
+
 class Request(C.Structure):
     _fields_ = [("kind", C.c_int), ("n", C.c_int), ("re", C.c_double), ("lid_u", C.c_double),
                 ("nnf_n", C.c_double), ("tau", C.c_double), ("force_z", C.c_double),
@@ -181,6 +190,10 @@ def lib():
             "mrlbm_reduce_fp64_ref_layout_noalloc": [VP, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, VP,
                                                      C.POINTER(Sums)],
             "mrlbm_selftest_bounded_wait": [C.c_uint, C.POINTER(C.c_double)],
+            "mrlbm_set_stream": [VP, VP],
+            "mrlbm_get_stream": [VP, C.POINTER(VP)],
+            "mrlbm_zslab_plane": [VP, C.c_int, C.POINTER(ZPlane)],
+            "mrlbm_zslab_copy": [VP, C.c_int, VP, C.c_int],
         }
         for name, args in sigs.items():
             f = getattr(L, name)
@@ -332,6 +345,25 @@ class Domain:
 
     def synchronize(self):
         check(self.L.mrlbm_synchronize(self.h))
+
+    def set_stream(self, stream):
+        """Queue the domain's work on `stream` (an integer cudaStream_t of the
+        domain's device, e.g. torch.cuda.current_stream().cuda_stream); None
+        or 0 returns to the domain's own stream."""
+        check(self.L.mrlbm_set_stream(self.h, C.c_void_p(stream or None)))
+
+    def get_stream(self):
+        s = VP()
+        check(self.L.mrlbm_get_stream(self.h, C.byref(s)))
+        return s.value or 0
+
+    def zplane(self, which):
+        """Device address, pair stride, bytes per pair and pair count of a z
+        plane of the buffer the next step reads (ZPLANE_* / ZGHOST_*)."""
+        z = ZPlane()
+        check(self.L.mrlbm_zslab_plane(self.h, int(which), C.byref(z)))
+        return {"base": z.base or 0, "pair_stride": z.pair_stride, "bytes": z.bytes, "npairs": z.npairs,
+                "device": z.device}
 
     @property
     def step_count(self):
