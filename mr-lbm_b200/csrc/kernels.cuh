@@ -850,7 +850,7 @@ __device__ __forceinline__ void store_node(const StepArgs& a, long long idx, con
 // c_z = +1 and 0 ones enter the z pipeline.  The arithmetic is branch-free
 // over the warp (so it interleaves with the next production); only the BC
 // solve and the stores are predicated.
-template <int Q, int NM, int NUP, int NMID, typename T, int FLAGS, int TYI, typename BCP>
+template <int Q, int NM, int NUP, int NMID, typename T, int FLAGS, int TYI, typename BCP, bool LIGHT = false>
 __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const float4* e4t, const float* e1t,
                                        bool interior, int x, int y, const float (&gsh)[Q], float (&up_old)[NUP],
                                        float (&mid)[NMID], float om_out, const float4* e4g = nullptr,
@@ -901,10 +901,9 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
         if constexpr (lat_cy(i) == 0) g[i] = gsh[i];
     });
 
-    {
-        // consumptions 0 and 1 complete no plane: computed like the others
-        // (one straight block the compiler can interleave with the
-        // production), nothing read from the class map or stored
+    if constexpr (!LIGHT) {
+        // consumptions 0 and 1 complete no plane: the column runs them LIGHT
+        // (only the z pipeline below moves)
         const bool live = interior && k >= 2;
         const int zd = zp - 1;
         float p[Q];
@@ -1144,7 +1143,7 @@ struct ZMarch {
     // whose stored omega is in om_par (same parity as j) until production j
     // overwrites it.  Returns false when a bounded wait timed out somewhere
     // in the CTA.
-    template <int PAR>
+    template <int PAR, bool LIGHT = false>
     __device__ __forceinline__ bool iter(int j, float (&gsh_new)[Q], const float (&gsh_old)[Q], float (&up)[NUP],
                                          float (&mid)[NMID], float& om_par, float* sg_new = nullptr,
                                          const float* sg_old = nullptr, float* upg = nullptr, float* midg = nullptr)
@@ -1156,15 +1155,15 @@ struct ZMarch {
         // consumption first measured 4 % faster on bulk and D3Q27 domains,
         // production first 4 % faster on D3Q19 domains with walls
         if constexpr (Q == 27 || (FLAGS & F_BC) == 0) {
-            prod_b<Q, NM, NUP, NMID, T, FLAGS, TYI, BCP>(a, j - 1, z0 - 2 + j, e4t[PAR ^ 1], e1t[PAR ^ 1], interior, x,
-                                                    y, gsh_old, up, mid, om_out, e4g[PAR ^ 1], e1g[PAR ^ 1], sg_old,
-                                                    upg, midg);
+            prod_b<Q, NM, NUP, NMID, T, FLAGS, TYI, BCP, LIGHT>(a, j - 1, z0 - 2 + j, e4t[PAR ^ 1], e1t[PAR ^ 1],
+                                                           interior, x, y, gsh_old, up, mid, om_out, e4g[PAR ^ 1],
+                                                           e1g[PAR ^ 1], sg_old, upg, midg);
             prod_a<Q, NM, T, TYI, TH>(a, stage_ptr(), e4t[PAR], e1t[PAR], gsh_new, om_par, e4g[PAR], e1g[PAR], sg_new);
         } else {
             prod_a<Q, NM, T, TYI, TH>(a, stage_ptr(), e4t[PAR], e1t[PAR], gsh_new, om_par, e4g[PAR], e1g[PAR], sg_new);
-            prod_b<Q, NM, NUP, NMID, T, FLAGS, TYI, BCP>(a, j - 1, z0 - 2 + j, e4t[PAR ^ 1], e1t[PAR ^ 1], interior, x,
-                                                    y, gsh_old, up, mid, om_out, e4g[PAR ^ 1], e1g[PAR ^ 1], sg_old,
-                                                    upg, midg);
+            prod_b<Q, NM, NUP, NMID, T, FLAGS, TYI, BCP, LIGHT>(a, j - 1, z0 - 2 + j, e4t[PAR ^ 1], e1t[PAR ^ 1],
+                                                           interior, x, y, gsh_old, up, mid, om_out, e4g[PAR ^ 1],
+                                                           e1g[PAR ^ 1], sg_old, upg, midg);
         }
         if (!ok) raise_timeout();
         __syncthreads();
@@ -1235,8 +1234,13 @@ __device__ __forceinline__ bool zmarch_column(const StepArgs& a, const CUtensorM
         else zm.advance(0);
     }
     // even productions use gA / upA and exchange buffer 0, odd ones gB / upB
-    // and buffer 1: no register copies, no buffer selection at run time
-    int j = 1;
+    // and buffer 1: no register copies, no buffer selection at run time.
+    // Consumptions 0 and 1 would complete planes z0 - 2 and z0 - 1, which
+    // are not this column's: they only move the z pipeline (nprod >= 3, so
+    // productions 1 and 2 exist).
+    if (kfail < 0 && !zm.template iter<1, true>(1, gB, gA, upA, mid, omB, sgB, sgA, ugA, mg)) kfail = 1;
+    if (kfail < 0 && !zm.template iter<0, true>(2, gA, gB, upB, mid, omA, sgA, sgB, ugB, mg)) kfail = 2;
+    int j = 3;
     while (kfail < 0) {
         // epilogues consume the last production j-1; its output plane is that
         // of production j-2, whose omega has the parity of j
