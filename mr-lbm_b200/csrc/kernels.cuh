@@ -1237,10 +1237,15 @@ __device__ __forceinline__ bool zmarch_column(const StepArgs& a, const CUtensorM
     // and buffer 1: no register copies, no buffer selection at run time.
     // Consumptions 0 and 1 would complete planes z0 - 2 and z0 - 1, which
     // are not this column's: they only move the z pipeline (nprod >= 3, so
-    // productions 1 and 2 exist).
-    if (kfail < 0 && !zm.template iter<1, true>(1, gB, gA, upA, mid, omB, sgB, sgA, ugA, mg)) kfail = 1;
-    if (kfail < 0 && !zm.template iter<0, true>(2, gA, gB, upB, mid, omA, sgA, sgB, ugB, mg)) kfail = 2;
-    int j = 3;
+    // productions 1 and 2 exist).  The thermal variants keep them in the
+    // loop: two more inlined pipeline steps raise their register spills and
+    // cost 6 % there.
+    int j = 1;
+    if constexpr (!ZM::TH) {
+        if (kfail < 0 && !zm.template iter<1, true>(1, gB, gA, upA, mid, omB, sgB, sgA, ugA, mg)) kfail = 1;
+        if (kfail < 0 && !zm.template iter<0, true>(2, gA, gB, upB, mid, omA, sgA, sgB, ugB, mg)) kfail = 2;
+        j = 3;
+    }
     while (kfail < 0) {
         // epilogues consume the last production j-1; its output plane is that
         // of production j-2, whose omega has the parity of j
