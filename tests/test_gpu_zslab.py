@@ -170,3 +170,31 @@ def test_one_nccl_rank_on_torch_stream():
         assert s["fluid_nodes"] == ws["fluid_nodes"]
     finally:
         dist.destroy_process_group()
+
+
+
+def test_outflow_channel_with_a_one_plane_top_slab():
+    """Velocity inlet at z = 0 and an outflow face at z = nz - 1, cut into 7
+    slabs whose top one is a single plane: its outflow nodes read their
+    inward neighbour's previous-step moments from the ghost plane the slab
+    below filled."""
+    from test_gpu_parity import channel_node_types
+
+    nx, ny, nz = 20, 18, 13
+    assert zslab.slab_bounds(nz, 7)[-1] == (12, 13)
+    d = mrlbm.make_desc(nx, ny, nz, lattice=mrlbm.D3Q19, periodic=(0, 0, 0), tau=0.7,
+                        bc_velocity=[(0.0, 0.0, 0.03)])
+    want, got, _ = _run_both(d, 7, 60, nt=channel_node_types(nx, ny, nz), init=lambda dom: dom.init_uniform())
+    assert float(np.mean(want[3, -1, 1:-1, 1:-1])) > 0.0
+    assert np.array_equal(got, want)
+
+
+def test_power_law_cavity_omega_travels_with_the_planes():
+    """Power-law fluid: omega is stored as moment 10 (six moment pairs, the
+    last one padded) and the slabs' ghost planes carry it."""
+    d = mrlbm.make_desc(30, 28, 26, lattice=mrlbm.D3Q19, periodic=(0, 0, 0), tau=0.6,
+                        bc_velocity=[(0.05, 0.0, 0.0)] + [(0.0, 0.0, 0.0)] * 3,
+                        rheology=mrlbm.POWERLAW, nnf_n=0.7)
+    want, got, _ = _run_both(d, 3, 40, nt=mrlbm.lid_cavity_node_types(30, 28, 26, 1))
+    assert want.shape[0] == 11
+    assert np.array_equal(got, want)
