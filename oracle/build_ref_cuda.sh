@@ -57,9 +57,11 @@ build_case refsim_lid64 lidDrivenCavity_3D D3Q19 2000 64 \
 
 # C1 again, with the lid's edges and corners typed as the edge/corner wall
 # types of nodeTypeMap.h (zero velocity) instead of the moving lid: then no
-# node reads a population from outside the domain as known (see DESIGN.md,
-# "lid edges"), and the run pins the solver independently of the reference's
-# 8^3 ghost-block layout.  The override is appended to the case's
+# node reads a population from outside the domain as known (the case as
+# shipped types every y = NY-1 node NORTH, so its lid edges and corners take
+# some outside populations as known, fed from the reference's ghost-face
+# arrays), and the run pins the solver independently of the reference's 8^3
+# ghost-block layout.  The override is appended to the case's
 # bc_initialization.inc, which runs after its if/else chain.
 build_case refsim_lid64_edges lidDrivenCavity_3D D3Q19 2000 64 \
   'sed -i "s/^constexpr dfloat RE = .*/constexpr dfloat RE = 100;/; s/^constexpr dfloat U_MAX = .*/constexpr dfloat U_MAX = 0.05;/" "$c/constants.inc"; sed -i "s/^#define REPORT_SAVE .*/#define REPORT_SAVE (false)/" "$c/output.inc"; printf "\nif (y == (NY - 1) && (x == 0 || x == (NX - 1) || z == 0 || z == (NZ_TOTAL - 1))) {\n    nodeType = NORTH | (x == 0 ? WEST : 0) | (x == (NX - 1) ? EAST : 0) | (z == 0 ? BACK : 0) | (z == (NZ_TOTAL - 1) ? FRONT : 0);\n}\n" >> "$c/bc_initialization.inc"'

@@ -8,7 +8,7 @@ cold walls in x with the neighbour-flux rule, gravity along x, periodic y and
 z); a closed cell with Dirichlet side walls and adiabatic (mirrored) top and
 bottom, src/cases/rayleighBenard_Closed; and walls that keep their stored
 values next to an internal heat source.  Both sides start from the same
-stored moments.  FP32 drift is judged against the oracle's FP32 build run
+stored moments.  FP32 drift is measured against the oracle's FP32 build run
 from the same start (the yardstick of test_gpu_parity.py): each moment's
 error must stay within twice that build's error or the fixed bound below.
 """
