@@ -104,7 +104,7 @@ fi
 # The same reference cases compiled, unchanged, in this library's case mode
 # (mr-lbm_b200/casebuild.py reads the case folder and pastes its snippets into
 # the sm_100a step kernel).  Test fixtures for the drop-in path: they run on the
-# GPU box next to the reference programs above, on identical inputs.
+# GPU next to the reference programs above, on identical inputs.
 PY=${PY:-python}
 CB="$HERE/../mr-lbm_b200/casebuild.py"
 mkdir -p "$OUT/cases"

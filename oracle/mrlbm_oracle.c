@@ -2,8 +2,8 @@
  * mrlbm_oracle.c -- TEST INFRASTRUCTURE ONLY.
  *
  * FP64 CPU restatement of the moment-representation LBM (MR-LBM) step of the
- * reference solver, written from the method's equations.  It is the checker
- * for the CUDA library (tests/, __graft_entry__.smoke() and bench.py's
+ * reference solver, written from the method's equations.  The CUDA library's
+ * results are compared against it (tests/, __graft_entry__.smoke() and bench.py's
  * cpu_baseline leg use it) and is never linked into or called by the product.
  *
  * What it restates (reference file:line it follows):
