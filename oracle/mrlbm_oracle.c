@@ -4,7 +4,7 @@
  * FP64 CPU restatement of the moment-representation LBM (MR-LBM) step of the
  * reference solver, written from the method's equations.  The CUDA library's
  * results are compared against it (tests/, __graft_entry__.smoke() and bench.py's
- * cpu_baseline leg use it) and is never linked into or called by the product.
+ * cpu_baseline leg use it); it is never linked into or called by the product.
  *
  * What it restates (reference file:line it follows):
  *   - lattice ordering / weights      src/includeFiles/velocitySets/D3Q19.inc:8-24,
