@@ -255,15 +255,16 @@ mrlbm_status mrlbm_residual(mrlbm_domain* dom, double* residual);
  * buffer on every call.
  * Scratch: a file-scope __device__ array of 37,952 bytes per device (592 block
  * partials + 8 results); the call always uses 592 blocks and strides over
- * larger fields, and a request beyond the array's size is rejected with
- * MRLBM_EINVAL.  Nothing in it has to start at zero (each call writes what it
- * reads).  The first call on a device looks up the array's address
- * (cudaGetSymbolAddress, with that device current): make it before any stream
- * capture begins.  Calls share the array per device, so calls whose
- * executions overlap on one device (two host threads, or unordered streams)
- * race and return wrong sums: serialise them.  Synchronises `stream`.  For a
- * field with the same values as a domain's F32 moments the result equals
- * mrlbm_reduce_fp64's for that domain (same blocks, same summation order). */
+ * larger fields, so every field size fits it.  Nothing in it has to start at
+ * zero (each call writes what it reads).  The first call in each CUDA context
+ * of a device looks up the array's address (cudaGetSymbolAddress, with that
+ * device current).  Every call synchronises `stream` to return the sums on
+ * the host, so no call can be made while `stream` is being captured.  Calls
+ * share the array per device, so calls whose executions overlap on one device
+ * (two host threads, or unordered streams) race and return wrong sums:
+ * serialise them.  fmom may also be managed memory.  For a field with the same
+ * values as a domain's F32 moments the result equals mrlbm_reduce_fp64's for
+ * that domain (same blocks, same summation order). */
 mrlbm_status mrlbm_reduce_fp64_ref_layout_noalloc(const float* fmom, int nx, int ny, int nz, int num_moments,
                                                   double rho0, void* stream, mrlbm_sums* out);
 

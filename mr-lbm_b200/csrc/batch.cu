@@ -128,8 +128,8 @@ mrlbm_status refresh(mrlbm_batch* b)
             return fail(MRLBM_EINVAL, "batch member %d: physics flag set %d not supported in batches", id, hd[id].flags);
         if (dom->has_outflow)
             return fail(MRLBM_EINVAL, "batch member %d: outflow walls are not supported in batches", id);
-        hd[id].map[0] = dom->tmap[0];
-        hd[id].map[1] = dom->tmap[1];
+        hd[id].map[0] = dom->tmap[0][tile_kind(batch_tyi(dom->q))];
+        hd[id].map[1] = dom->tmap[1][tile_kind(batch_tyi(dom->q))];
         hd[id].parity_offset = b->offsets[id];
         const int ty = batch_tyi(dom->q);
         const int gx = (dom->d.nx + TILE_X - 1) / TILE_X, gy = (dom->d.ny + ty - 1) / ty;

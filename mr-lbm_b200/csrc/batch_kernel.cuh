@@ -10,8 +10,9 @@
 
 namespace mrlbm {
 
-// rows per CTA: the single-domain kernel's (members share its tensor maps)
-__host__ __device__ constexpr int batch_tyi(int q) { return tile_y(q); }
+// rows per CTA: the single-domain kernel's for wall domains (members share
+// its tensor maps; the batch's flag sets include walls)
+__host__ __device__ constexpr int batch_tyi(int q) { return TYI_WALL; }
 
 // Per-domain data the batched kernel needs; both parities are precomputed so
 // the kernel only selects.  64-byte aligned for the tensor maps.

@@ -34,14 +34,15 @@ struct mrlbm_domain {
     int step = 0;
     uint8_t* cls = nullptr;
     int* err = nullptr;              // device flag: a bounded wait timed out
-    CUtensorMap tmap[2];             // TMA maps of the two moment buffers
+    CUtensorMap tmap[2][2];          // TMA maps [moment buffer][tile kind: TYI_BULK, TYI_WALL rows]
     mrlbm::BcClass* bc = nullptr;
     int nclasses = 0;
     bool has_bc = false;
     bool has_outflow = false;        // some class is an outflow wall (not taken by batches)
     float ext[mrlbm::NM_MAX] = {};
     float scale[mrlbm::NM_MAX] = {}, iscale[mrlbm::NM_MAX] = {};
-    int lz = 16;                     // z planes per CTA (batch members: per work item)
+    int lz = 0;                      // z planes per work item when a batch has set it (0: single-domain choice)
+    int lz_t[2] = {16, 16};          // single-domain z planes per CTA, per tile kind
     int nsm = 148;                   // SMs of the device the domain lives on
     cudaStream_t stream = nullptr;      // where the domain's work is queued
     cudaStream_t own_stream = nullptr;  // the stream the domain created (stream unless mrlbm_set_stream)
@@ -67,11 +68,12 @@ mrlbm_status classify_nodes(int q, int mq, const uint32_t* nt, long long n, cons
                             bool case_mode = false, const double* t_wall = nullptr);
 void storage_scales(int storage, float* scale, float* iscale);
 mrlbm_status domain_alloc(mrlbm_domain* dom);
-int choose_lz(const mrlbm_domain* dom);
+int choose_lz(const mrlbm_domain* dom, int tyi);
 void fill_step_args(const mrlbm_domain* dom, StepArgs& a, int parity, int& flags);
 mrlbm_status enqueue_step(mrlbm_domain* dom, int parity, cudaStream_t s);
+// maps: the read buffer's two tensor maps (tile kinds TYI_BULK, TYI_WALL)
 template <int Q, typename T>
-mrlbm_status dispatch_step(const CUtensorMap& map, const StepArgs& a, int flags, cudaStream_t s);
+mrlbm_status dispatch_step(const CUtensorMap* maps, const StepArgs& a, int flags, cudaStream_t s);
 mrlbm_status make_tensor_maps(mrlbm_domain* dom);
 mrlbm_status fill_ghosts(mrlbm_domain* dom);
 mrlbm_status check_device_error(mrlbm_domain* dom);

@@ -338,8 +338,13 @@ extern "C" mrlbm_status mrlbm_save_info(mrlbm_domain* dom, const char* path_file
     fprintf(f, "             Nsteps: %d\n", nsteps);
     fprintf(f, "              MLUPS: %.6e\n", mlups);
     fprintf(f, "                 BX: %d\n", TILE_X);
-    fprintf(f, "                 BY: %d\n", tile_y(dom->q));
-    fprintf(f, "                 BZ: %d\n", dom->lz);
+    {
+        StepArgs sa;
+        int flags = 0;
+        fill_step_args(dom, sa, dom->cur, flags);
+        fprintf(f, "                 BY: %d\n", tile_rows(flags));
+        fprintf(f, "                 BZ: %d\n", sa.lz);
+    }
     fprintf(f, "--------------------------------------------------------------------------------\n");
     fprintf(f, "\n------------------------------ BOUNDARY CONDITIONS -----------------------------\n");
     fprintf(f, "            BC mode: Moment Based \n");

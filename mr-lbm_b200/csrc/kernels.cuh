@@ -63,18 +63,33 @@ enum : int {
 // most stored moments per node: 10 flow moments + omega, or + C and its flux
 constexpr int NM_MAX = 14;
 
-constexpr int TILE_X = 30;   // interior nodes per warp row
+// CTA geometry: 32 x TYI interior nodes of an (x, y) column (warp w < TYI is
+// row y = Y0 + w, lane l is x = X0 + l) plus two helper warps that produce
+// what crosses into the column from outside it.
+constexpr int TILE_X = 32;   // interior nodes per row (one per lane)
 constexpr int XOFF = 4;      // padded column of x = 0 (x = -1 is the ghost column)
-constexpr int BOX_X = 40;    // TMA box width (elements) covering the 32 lanes
+// TMA box width in nodes: covers x = X0 - 1 .. X0 + 32 from a 16-byte
+// aligned start (X0 - 2 for FP32 pairs, X0 - 4 for 16-bit pairs)
+template <typename T>
+__host__ __device__ constexpr int box_x()
+{
+    return sizeof(T) == 4 ? 36 : 40;
+}
+__host__ __device__ constexpr int box_x_nodes(int esize) { return esize == 4 ? 36 : 40; }
 // TMA ring depth: 4 stages where the ring and the row exchange fit in shared
-// memory (4 measured 1-3 % faster than 3), else 3
+// memory (4 measured 1-3 % faster than 3), else 3 (or 2)
 constexpr int NSTAGE_MAX = 4;
-// interior rows per CTA (warps = rows + 2 halo rows): 16 warps at 128
-// registers fill the register file.  (18 rows at 96 registers measured
-// slower: the compiler's schedule needs the registers more than the SM needs
-// the extra warps.)
-constexpr int TYI19 = 14, TYI27 = 14;
-__host__ __device__ constexpr int tile_y(int q) { return q == 27 ? TYI27 : TYI19; }
+// interior rows per CTA: 16 (18 warps, up to 112 registers a thread) for the
+// bulk-only flag sets, 14 (16 warps, up to 128 registers) for the heavier
+// wall, non-Newtonian and thermal sets
+constexpr int TYI_BULK = 16, TYI_WALL = 14;
+__host__ __device__ constexpr int tile_rows(int flags)
+{
+    return (flags & (F_BC | F_POWERLAW | F_BINGHAM | F_THERMAL)) ? TYI_WALL : TYI_BULK;
+}
+// index of a tile height among the domain's tensor maps and z chunks
+__host__ __device__ constexpr int tile_kind(int tyi) { return tyi == TYI_BULK ? 0 : 1; }
+__host__ __device__ constexpr int tile_rows_of_kind(int kind) { return kind == 0 ? TYI_BULK : TYI_WALL; }
 constexpr uint8_t CLS_BULK = 0;
 constexpr uint8_t CLS_SOLID = 255;
 constexpr unsigned WAIT_LIMIT = 1u << 26;  // mbarrier polls before giving up (~seconds)
@@ -632,27 +647,30 @@ __host__ __device__ constexpr bool ex_group_used()
 __host__ __device__ constexpr int ex_npack(int Q) { return Q == 27 ? 6 : 2; }
 __host__ __device__ constexpr int ex_slot4(int Q, int G) { return Q == 27 ? G : (G == 1 ? 0 : 1); }
 
-// Exchange buffers hold NW + 2 rows of EX_COLS slots per group; a thread's
-// own slot is row warp + 1, column lane + 1, and the slot it reads a group
-// from (row warp - c_y, lane - c_x) is a compile-time offset from it, so no
-// index arithmetic runs per access.  The halo rows and lanes read the padding
-// rows and columns (their results are never stored).
-constexpr int EX_COLS = 34;
+// Exchange buffers hold TYI + 2 rows of EX_COLS slots per group: row
+// er = y - Y0 + 1 (0: the row below the column, TYI + 1: the row above it),
+// column ec = x - X0 + 1 (0 and 33: the nodes left and right of the column).
+// An interior node's own slot is (w + 1, lane + 1), and the slot it reads a
+// group from (row w + 1 - c_y, column lane + 1 - c_x) is a compile-time offset
+// from it, so no index arithmetic runs per access.  The outer rows and
+// columns are written by the helper warps.
+constexpr int EX_COLS = TILE_X + 2;
 
-template <int Q, int NW>
+template <int Q, int TYI>
 struct Exchange {
     static constexpr int NPACK = ex_npack(Q);        // float4 groups
     static constexpr int NSCAL = Q == 19 ? 4 : 0;    // scalar slots
-    static constexpr int plane = (NW + 2) * EX_COLS;  // slots of one group
+    static constexpr int rows = TYI + 2;
+    static constexpr int plane = rows * EX_COLS;     // slots of one group
     static constexpr int buf4 = NPACK * plane;       // float4 per buffer
     static constexpr int buf1 = NSCAL * plane;       // floats per buffer
     static constexpr size_t bytes_per_buffer = (size_t)plane * (NPACK * 16 + NSCAL * 4);
-    __device__ __forceinline__ static int thread_slot(int warp, int lane) { return (warp + 1) * EX_COLS + lane + 1; }
+    __host__ __device__ __forceinline__ static constexpr int slot(int er, int ec) { return er * EX_COLS + ec; }
 };
 
 // store group G of this lane's populations (its c_z = -1, 0, +1 members);
 // e4t is this thread's slot of group 0 in the buffer being written
-template <int Q, int G, int NW>
+template <int Q, int G, int TYI>
 __device__ __forceinline__ void ex_write(const float* f, float4* e4t)
 {
     if constexpr (ex_group_used<Q, G>()) {
@@ -665,17 +683,66 @@ __device__ __forceinline__ void ex_write(const float* f, float4* e4t)
                 else v.z = f[i];
             }
         });
-        e4t[ex_slot4(Q, G) * Exchange<Q, NW>::plane] = v;
+        e4t[ex_slot4(Q, G) * Exchange<Q, TYI>::plane] = v;
     }
 }
 
-// fetch group G arriving from row warp - c_y, lane - c_x
-template <int Q, int G, int NW>
+// every exchanged population (c_y != 0) of this node: packed groups and, on
+// D3Q19, the four scalar slots
+template <int Q, int TYI>
+__device__ __forceinline__ void ex_write_all(const float* f, float4* e4t, float* e1t)
+{
+    ex_write<Q, 0, TYI>(f, e4t);
+    ex_write<Q, 1, TYI>(f, e4t);
+    ex_write<Q, 2, TYI>(f, e4t);
+    ex_write<Q, 3, TYI>(f, e4t);
+    ex_write<Q, 4, TYI>(f, e4t);
+    ex_write<Q, 5, TYI>(f, e4t);
+    if constexpr (Q == 19) {
+        static_for<1, Q>([&](auto I) {
+            constexpr int i = I;
+            if constexpr (lat_cy(i) != 0 && !ex_packed(Q, i)) e1t[ex_scalar_slot(i) * Exchange<Q, TYI>::plane] = f[i];
+        });
+    }
+}
+
+// the exchanged populations of a node outside the column that cross into it:
+// CY = +1 / -1 selects the c_y of a row below / above the column (any c_x),
+// CX = +1 / -1 the c_x of a node left / right of it (c_y = +-1; its c_y = 0
+// members go to the edge buffer, ex_write_edge)
+template <int Q, int TYI, int CX, int CY>
+__device__ __forceinline__ void ex_write_sel(const float* f, float4* e4t, float* e1t)
+{
+    static_for<0, 6>([&](auto GG) {
+        constexpr int G = GG;
+        constexpr int gx = (G % 3) - 1, gy = G >= 3 ? 1 : -1;
+        if constexpr ((CX == 0 || gx == CX) && (CY == 0 || gy == CY)) ex_write<Q, G, TYI>(f, e4t);
+    });
+    if constexpr (Q == 19) {
+        static_for<1, Q>([&](auto I) {
+            constexpr int i = I;
+            if constexpr (lat_cy(i) != 0 && !ex_packed(Q, i) && (CX == 0 || lat_cx(i) == CX) &&
+                          (CY == 0 || lat_cy(i) == CY))
+                e1t[ex_scalar_slot(i) * Exchange<Q, TYI>::plane] = f[i];
+        });
+    }
+}
+
+// the c_y = 0 populations with c_x = CX of an edge node (c_z = -1, 0, +1)
+template <int Q, int CX>
+__device__ __forceinline__ float4 edge_pops(const float* f)
+{
+    constexpr int im = lat_find(Q, CX, 0, -1), i0 = lat_find(Q, CX, 0, 0), ip = lat_find(Q, CX, 0, 1);
+    return make_float4(f[im], f[i0], f[ip], 0.f);
+}
+
+// fetch group G arriving from row w - c_y, lane - c_x
+template <int Q, int G, int TYI>
 __device__ __forceinline__ void ex_read(float* g, const float4* e4t)
 {
     if constexpr (ex_group_used<Q, G>()) {
         constexpr int cx = (G % 3) - 1, cy = G >= 3 ? 1 : -1;
-        const float4 v = e4t[ex_slot4(Q, G) * Exchange<Q, NW>::plane - cy * EX_COLS - cx];
+        const float4 v = e4t[ex_slot4(Q, G) * Exchange<Q, TYI>::plane - cy * EX_COLS - cx];
         static_for<1, Q>([&](auto I) {
             constexpr int i = I;
             if constexpr (lat_cy(i) != 0 && ex_group(i) == G && ex_packed(Q, i))
@@ -684,42 +751,89 @@ __device__ __forceinline__ void ex_read(float* g, const float4* e4t)
     }
 }
 
-// Production of plane k (first half of a pipeline step): the plane's moments
-// come from TMA stage `stage`, its post-collision populations are
-// reconstructed, the c_y != 0 ones are written to exchange buffer k&1 and the
-// c_y = 0 ones are exchanged along x with shuffles into gsh (kept in
-// registers until the plane is consumed, one step later).
-// sp: this thread's element pair of moments 0, 1 in the plane's TMA stage
-// (pair p is 2 BOX_X elements further); e4t / e1t: this thread's exchange
-// slots in the buffer this production writes.
+// every population arriving at an interior node through the exchange
+// (c_y != 0) and along x (c_y = 0: the shuffled gsh, or at the column's two
+// outer lanes the edge buffer's float4 ee)
+template <int Q, int TYI>
+__device__ __forceinline__ void gather_pops(float* g, const float4* e4t, const float* e1t, const float (&gsh)[Q],
+                                            float4 ee, bool xlo, bool xhi)
+{
+    ex_read<Q, 0, TYI>(g, e4t);
+    ex_read<Q, 1, TYI>(g, e4t);
+    ex_read<Q, 2, TYI>(g, e4t);
+    ex_read<Q, 3, TYI>(g, e4t);
+    ex_read<Q, 4, TYI>(g, e4t);
+    ex_read<Q, 5, TYI>(g, e4t);
+    if constexpr (Q == 19) {
+        static_for<1, Q>([&](auto I) {
+            constexpr int i = I;
+            if constexpr (lat_cy(i) != 0 && !ex_packed(Q, i))
+                g[i] = e1t[ex_scalar_slot(i) * Exchange<Q, TYI>::plane - lat_cy(i) * EX_COLS - lat_cx(i)];
+        });
+    }
+    static_for<0, Q>([&](auto I) {
+        constexpr int i = I;
+        if constexpr (lat_cy(i) == 0) {
+            constexpr int cz = lat_cz(i);
+            const float e = cz < 0 ? ee.x : (cz == 0 ? ee.y : ee.z);
+            if constexpr (lat_cx(i) > 0) g[i] = xlo ? e : gsh[i];
+            else if constexpr (lat_cx(i) < 0) g[i] = xhi ? e : gsh[i];
+            else g[i] = gsh[i];
+        }
+    });
+}
+
+// a node's stored moments (unscaled to the FP32 stored form) from its element
+// pair of moments 0, 1 in a TMA stage (pair p is 2 box_x<T>() elements further)
+template <int NM, typename T>
+__device__ __forceinline__ void stage_moments(const StepArgs& a, const T* sp, float* mc)
+{
+#pragma unroll
+    for (int p = 0; p < (NM + 1) / 2; p++) {
+        const float2 v = Stor2<T>::lds(sp + p * 2 * box_x<T>());
+        mc[2 * p] = scaled_storage<T>() ? v.x * a.iscale[2 * p] : v.x;
+        if (2 * p + 1 < NM) mc[2 * p + 1] = scaled_storage<T>() ? v.y * a.iscale[2 * p + 1] : v.y;
+    }
+}
+
+// thermal populations on D3G19 (the D3Q19 directions and weights):
+// g_i = C w_i (1 + c_i . (u3 + ud3)), ud3 = coef (q3 / C - u3) with the
+// node's stored flow velocity u3 = 3u and flux q3 = 3 sum g c
+// (src/colrec/G_SCALAR/reconstruction.inc:1-25, src/mlbm.cu:159-169)
+__device__ __forceinline__ void thermal_pops(const StepArgs& a, const float* mc, float* g)
+{
+    const float C = mc[10], iC = 1.0f / C;
+    const float vx = fmaf(a.t_coef, fmaf(mc[11], iC, -mc[1]), mc[1]);
+    const float vy = fmaf(a.t_coef, fmaf(mc[12], iC, -mc[2]), mc[2]);
+    const float vz = fmaf(a.t_coef, fmaf(mc[13], iC, -mc[3]), mc[3]);
+    static_for<0, 19>([&](auto I) {
+        constexpr int i = I;
+        float t = 1.0f;
+        if constexpr (lat_cx(i) > 0) t += vx; else if constexpr (lat_cx(i) < 0) t -= vx;
+        if constexpr (lat_cy(i) > 0) t += vy; else if constexpr (lat_cy(i) < 0) t -= vy;
+        if constexpr (lat_cz(i) > 0) t += vz; else if constexpr (lat_cz(i) < 0) t -= vz;
+        g[i] = (C * (float)lat_w(19, i)) * t;
+    });
+}
+
+// Production of plane k at an interior node (first half of a pipeline
+// step): the plane's moments come from TMA stage `stage`, its post-collision
+// populations are reconstructed, the c_y != 0 ones are written to exchange
+// buffer k&1 and the c_y = 0 ones are exchanged along x with shuffles into gsh
+// (kept in registers until the plane is consumed, one step later; lanes 0 and
+// 31 take their inward c_x members from the edge buffer then).
+// sp: this thread's element pair of moments 0, 1 in the plane's TMA stage;
+// e4t / e1t: this thread's exchange slots in the buffer this production writes.
 template <int Q, int NM, typename T, int TYI, bool TH = false>
 __device__ __forceinline__ void prod_a(const StepArgs& a, const T* sp, float4* e4t, float* e1t, float (&gsh)[Q],
                                        float& om_node, float4* e4g = nullptr, float* e1g = nullptr,
                                        float* gshg = nullptr)
 {
-    constexpr int NW = TYI + 2;
     float mc[NM];
-#pragma unroll
-    for (int p = 0; p < (NM + 1) / 2; p++) {
-        const float2 v = Stor2<T>::lds(sp + p * 2 * BOX_X);
-        mc[2 * p] = scaled_storage<T>() ? v.x * a.iscale[2 * p] : v.x;
-        if (2 * p + 1 < NM) mc[2 * p + 1] = scaled_storage<T>() ? v.y * a.iscale[2 * p + 1] : v.y;
-    }
+    stage_moments<NM, T>(a, sp, mc);
     float f[Q];
     reconstruct<Q>(mc, a.rho0, f);
-    ex_write<Q, 0, NW>(f, e4t);
-    ex_write<Q, 1, NW>(f, e4t);
-    ex_write<Q, 2, NW>(f, e4t);
-    ex_write<Q, 3, NW>(f, e4t);
-    ex_write<Q, 4, NW>(f, e4t);
-    ex_write<Q, 5, NW>(f, e4t);
-    if constexpr (Q == 19) {
-        static_for<1, Q>([&](auto I) {
-            constexpr int i = I;
-            if constexpr (lat_cy(i) != 0 && !ex_packed(Q, i))
-                e1t[ex_scalar_slot(i) * Exchange<Q, NW>::plane] = f[i];
-        });
-    }
+    ex_write_all<Q, TYI>(f, e4t, e1t);
     static_for<0, Q>([&](auto I) {
         constexpr int i = I;
         if constexpr (lat_cy(i) == 0) {
@@ -730,33 +844,9 @@ __device__ __forceinline__ void prod_a(const StepArgs& a, const T* sp, float4* e
     });
     om_node = mc[NM - 1];
     if constexpr (TH) {
-        // thermal populations on D3G19 (the D3Q19 directions and weights):
-        // g_i = C w_i (1 + c_i . (u3 + ud3)), ud3 = coef (q3 / C - u3) with the
-        // node's stored flow velocity u3 = 3u and flux q3 = 3 sum g c
-        // (src/colrec/G_SCALAR/reconstruction.inc:1-25, src/mlbm.cu:159-169)
-        const float C = mc[10], iC = 1.0f / C;
-        const float vx = fmaf(a.t_coef, fmaf(mc[11], iC, -mc[1]), mc[1]);
-        const float vy = fmaf(a.t_coef, fmaf(mc[12], iC, -mc[2]), mc[2]);
-        const float vz = fmaf(a.t_coef, fmaf(mc[13], iC, -mc[3]), mc[3]);
         float g[19];
-        static_for<0, 19>([&](auto I) {
-            constexpr int i = I;
-            float t = 1.0f;
-            if constexpr (lat_cx(i) > 0) t += vx; else if constexpr (lat_cx(i) < 0) t -= vx;
-            if constexpr (lat_cy(i) > 0) t += vy; else if constexpr (lat_cy(i) < 0) t -= vy;
-            if constexpr (lat_cz(i) > 0) t += vz; else if constexpr (lat_cz(i) < 0) t -= vz;
-            g[i] = (C * (float)lat_w(19, i)) * t;
-        });
-        ex_write<19, 0, NW>(g, e4g);
-        ex_write<19, 1, NW>(g, e4g);
-        ex_write<19, 2, NW>(g, e4g);
-        ex_write<19, 3, NW>(g, e4g);
-        ex_write<19, 4, NW>(g, e4g);
-        ex_write<19, 5, NW>(g, e4g);
-        static_for<1, 19>([&](auto I) {
-            constexpr int i = I;
-            if constexpr (lat_cy(i) != 0 && !ex_packed(19, i)) e1g[ex_scalar_slot(i) * Exchange<19, NW>::plane] = g[i];
-        });
+        thermal_pops(a, mc, g);
+        ex_write_all<19, TYI>(g, e4g, e1g);
         static_for<0, 19>([&](auto I) {
             constexpr int i = I;
             if constexpr (lat_cy(i) == 0) {
@@ -765,6 +855,47 @@ __device__ __forceinline__ void prod_a(const StepArgs& a, const T* sp, float4* e
                 else gshg[i] = g[i];
             }
         });
+    }
+}
+
+// Production of plane k by a helper warp: SIDE = -1 (bottom helper) produces
+// the c_y = +1 populations of row Y0 - 1 (lane l: x = X0 + l) and the c_x = +1
+// populations of the nodes x = X0 - 1 of rows Y0 - 1 .. Y0 + TYI (lane k:
+// exchange row k); SIDE = +1 (top helper) the c_y = -1 populations of row
+// Y0 + TYI and the c_x = -1 populations of the nodes x = X0 + 32.  Only the
+// populations that cross into the column are formed (the others are dead code).
+// hp / ep: the halo-row and edge node's element pair of moments 0, 1 in the
+// stage; e4h / e1h and e4e / e1e: their exchange slots; edge: the edge buffer
+// of this side and parity (one float4 per exchange row).
+template <int Q, int NM, typename T, int TYI, int SIDE, bool TH = false>
+__device__ __forceinline__ void prod_helper(const StepArgs& a, int lane, const T* hp, const T* ep, float4* e4h,
+                                            float* e1h, float4* e4e, float* e1e, float4* edge, float4* e4hg = nullptr,
+                                            float* e1hg = nullptr, float4* e4eg = nullptr, float* e1eg = nullptr,
+                                            float4* edgeg = nullptr)
+{
+    {
+        float mc[NM], f[Q];
+        stage_moments<NM, T>(a, hp, mc);
+        reconstruct<Q>(mc, a.rho0, f);
+        ex_write_sel<Q, TYI, 0, -SIDE>(f, e4h, e1h);
+        if constexpr (TH) {
+            float g[19];
+            thermal_pops(a, mc, g);
+            ex_write_sel<19, TYI, 0, -SIDE>(g, e4hg, e1hg);
+        }
+    }
+    if (lane < TYI + 2) {
+        float mc[NM], f[Q];
+        stage_moments<NM, T>(a, ep, mc);
+        reconstruct<Q>(mc, a.rho0, f);
+        ex_write_sel<Q, TYI, -SIDE, 0>(f, e4e, e1e);
+        edge[lane] = edge_pops<Q, -SIDE>(f);
+        if constexpr (TH) {
+            float g[19];
+            thermal_pops(a, mc, g);
+            ex_write_sel<19, TYI, -SIDE, 0>(g, e4eg, e1eg);
+            edgeg[lane] = edge_pops<19, -SIDE>(g);
+        }
     }
 }
 
@@ -852,30 +983,21 @@ __device__ __forceinline__ void store_node(const StepArgs& a, long long idx, con
 // solve and the stores are predicated.
 template <int Q, int NM, int NUP, int NMID, typename T, int FLAGS, int TYI, typename BCP, bool LIGHT = false>
 __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const float4* e4t, const float* e1t,
-                                       bool interior, int x, int y, const float (&gsh)[Q], float (&up_old)[NUP],
-                                       float (&mid)[NMID], float om_out, const float4* e4g = nullptr,
-                                       const float* e1g = nullptr, const float* gshg = nullptr,
+                                       const float4* eet, bool xlo, bool xhi, bool interior, int x, int y,
+                                       const float (&gsh)[Q], float (&up_old)[NUP], float (&mid)[NMID], float om_out,
+                                       const float4* e4g = nullptr, const float* e1g = nullptr,
+                                       const float4* eetg = nullptr, const float* gshg = nullptr,
                                        float* upg_old = nullptr, float* midg = nullptr)
 {
-    constexpr int NW = TYI + 2;
     constexpr bool TH = (FLAGS & F_THERMAL) != 0;
     // thermal populations arriving at the node (same three sources as the flow's)
     float gg[19], pg[19];
     if constexpr (TH) {
-        ex_read<19, 0, NW>(gg, e4g);
-        ex_read<19, 1, NW>(gg, e4g);
-        ex_read<19, 2, NW>(gg, e4g);
-        ex_read<19, 3, NW>(gg, e4g);
-        ex_read<19, 4, NW>(gg, e4g);
-        ex_read<19, 5, NW>(gg, e4g);
-        static_for<1, 19>([&](auto I) {
-            constexpr int i = I;
-            if constexpr (lat_cy(i) != 0 && !ex_packed(19, i))
-                gg[i] = e1g[ex_scalar_slot(i) * Exchange<19, NW>::plane - lat_cy(i) * EX_COLS - lat_cx(i)];
-        });
+        float gshg19[19];
+        static_for<0, 19>([&](auto I) { gshg19[I] = gshg[I]; });
+        gather_pops<19, TYI>(gg, e4g, e1g, gshg19, *eetg, xlo, xhi);
         static_for<0, 19>([&](auto I) {
             constexpr int i = I;
-            if constexpr (lat_cy(i) == 0) gg[i] = gshg[i];
             constexpr int slot = lat_cz_slot(19, i);
             if constexpr (lat_cz(i) > 0) pg[i] = upg_old[slot];
             else if constexpr (lat_cz(i) == 0) pg[i] = midg[slot];
@@ -883,23 +1005,7 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
         });
     }
     float g[Q];
-    ex_read<Q, 0, NW>(g, e4t);
-    ex_read<Q, 1, NW>(g, e4t);
-    ex_read<Q, 2, NW>(g, e4t);
-    ex_read<Q, 3, NW>(g, e4t);
-    ex_read<Q, 4, NW>(g, e4t);
-    ex_read<Q, 5, NW>(g, e4t);
-    if constexpr (Q == 19) {
-        static_for<1, Q>([&](auto I) {
-            constexpr int i = I;
-            if constexpr (lat_cy(i) != 0 && !ex_packed(Q, i))
-                g[i] = e1t[ex_scalar_slot(i) * Exchange<Q, NW>::plane - lat_cy(i) * EX_COLS - lat_cx(i)];
-        });
-    }
-    static_for<0, Q>([&](auto I) {
-        constexpr int i = I;
-        if constexpr (lat_cy(i) == 0) g[i] = gsh[i];
-    });
+    gather_pops<Q, TYI>(g, e4t, e1t, gsh, *eet, xlo, xhi);
 
     if constexpr (!LIGHT) {
         // consumptions 0 and 1 complete no plane: the column runs them LIGHT
@@ -1033,33 +1139,45 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
 }
 
 // Shared-memory carve-up used by every z-march kernel: barriers, TMA ring,
-// double-buffered exchange.  Ring slots hold NPM moment pairs (kernels that
-// switch between flag sets at run time size them for the largest set), and
-// the ring has NSTAGE_MAX stages when they fit next to the exchange buffers,
-// else one fewer.
+// double-buffered exchange, edge buffers.  Ring slots hold NPM moment pairs
+// (kernels that switch between flag sets at run time size them for the
+// largest set), and the ring has NSTAGE_MAX stages when they fit next to the
+// exchange buffers, else fewer.
 template <int Q, typename T, int TYI, int NPM, bool TH = false>
 struct ZSmem {
-    static constexpr int NW = TYI + 2;
-    static constexpr size_t stage_max = ((size_t)NW * NPM * 2 * BOX_X * sizeof(T) + 127) / 128 * 128;
+    static constexpr int NR = TYI + 2;  // stage rows = exchange rows
+    static constexpr size_t stage_max = ((size_t)NR * NPM * 2 * box_x<T>() * sizeof(T) + 127) / 128 * 128;
     // the thermal populations have a row exchange of their own (D3Q19 layout)
     static constexpr size_t ex_bytes =
-        2 * Exchange<Q, NW>::bytes_per_buffer + (TH ? 2 * Exchange<19, NW>::bytes_per_buffer : 0);
-    static constexpr int NS = 128 + NSTAGE_MAX * stage_max + ex_bytes <= 232448 ? NSTAGE_MAX : NSTAGE_MAX - 1;
-    static constexpr size_t bytes = 128 + NS * stage_max + ex_bytes;
+        2 * Exchange<Q, TYI>::bytes_per_buffer + (TH ? 2 * Exchange<19, TYI>::bytes_per_buffer : 0);
+    // c_y = 0 populations of the edge nodes: [side][parity][row] float4
+    // (flow, then thermal)
+    static constexpr int edge_n = 2 * 2 * NR;
+    static constexpr size_t edge_bytes = (size_t)(TH ? 2 : 1) * edge_n * 16;
+    static constexpr size_t fixed = 128 + ex_bytes + edge_bytes;
+    static constexpr int NS = fixed + NSTAGE_MAX * stage_max <= 232448         ? NSTAGE_MAX
+                              : fixed + (NSTAGE_MAX - 1) * stage_max <= 232448 ? NSTAGE_MAX - 1
+                                                                               : NSTAGE_MAX - 2;
+    static constexpr size_t bytes = fixed + NS * stage_max;
+    static_assert(bytes <= 232448, "shared memory over the sm_100 limit");
     uint64_t* bars;   // the ring's mbarriers, then the CTA's timeout flag (bars + NSTAGE_MAX)
     unsigned char* stages;
     float4* ex4;
     float* ex1;
     float4* exg4;   // thermal exchange (TH only)
     float* exg1;
+    float4* edge;   // flow edge buffer
+    float4* edgeg;  // thermal edge buffer (TH only)
     __device__ __forceinline__ explicit ZSmem(unsigned char* smem)
     {
         bars = reinterpret_cast<uint64_t*>(smem);
         stages = smem + 128;
         ex4 = reinterpret_cast<float4*>(stages + NS * stage_max);
-        ex1 = reinterpret_cast<float*>(ex4 + 2 * Exchange<Q, NW>::buf4);
-        exg4 = reinterpret_cast<float4*>(ex1 + 2 * Exchange<Q, NW>::buf1);
-        exg1 = reinterpret_cast<float*>(exg4 + 2 * Exchange<19, NW>::buf4);
+        ex1 = reinterpret_cast<float*>(ex4 + 2 * Exchange<Q, TYI>::buf4);
+        exg4 = reinterpret_cast<float4*>(ex1 + 2 * Exchange<Q, TYI>::buf1);
+        exg1 = reinterpret_cast<float*>(exg4 + (TH ? 2 * Exchange<19, TYI>::buf4 : 0));
+        edge = reinterpret_cast<float4*>(exg1 + (TH ? 2 * Exchange<19, TYI>::buf1 : 0));
+        edgeg = edge + edge_n;
     }
 };
 
@@ -1070,64 +1188,61 @@ __host__ __device__ constexpr int nmoments_of(int flags)
 }
 __host__ __device__ constexpr int npairs_of(int flags) { return (nmoments_of(flags) + 1) / 2; }
 
-// Per-CTA pipeline state and the loop of the z-march over one column.  The
-// TMA ring is indexed by a running production count `g0 + k` so a persistent
-// CTA can chain columns without re-initialising its mbarriers.
+// Per-CTA pipeline state of the z-march over one column.  The TMA ring is
+// indexed by a running production count `g0 + k` so a persistent CTA can
+// chain columns without re-initialising its mbarriers.  Warps 0 .. TYI-1 run
+// the interior pipeline (interior_loop), warps TYI and TYI+1 the helper one
+// (helper_loop); both take the same barriers in the same order.
 template <int Q, typename T, int FLAGS, int TYI, typename BCP, int NPM>
 struct ZMarch {
-    static constexpr int NW = TYI + 2;
+    static constexpr int NR = TYI + 2;
+    static constexpr int BX = box_x<T>();
     static constexpr int NUP = lat_num_cz(Q, 1);
     static constexpr int NMID = lat_num_cz(Q, 0);
     static constexpr bool OMF = (FLAGS & (F_POWERLAW | F_BINGHAM)) != 0;
     static constexpr bool TH = (FLAGS & F_THERMAL) != 0;
     static constexpr int NM = nmoments_of(FLAGS);
     static constexpr int NP = (NM + 1) / 2;  // moment pairs in a stage row
-    static constexpr size_t stage_bytes = (size_t)NW * NP * 2 * BOX_X * sizeof(T);
-    static constexpr size_t stage_al = (stage_bytes + 127) / 128 * 128;
-    using EX = Exchange<Q, NW>;
+    static constexpr int ROW = NP * 2 * BX;  // elements of a stage row
+    static constexpr size_t stage_bytes = (size_t)NR * ROW * sizeof(T);
+    using EX = Exchange<Q, TYI>;
+    using EXG = Exchange<19, TYI>;
     using SM = ZSmem<Q, T, TYI, NPM, TH>;
     static constexpr int NS = SM::NS;
+    static constexpr int TMA_THREAD = 32 * TYI;  // lane 0 of the bottom helper
     static_assert(NP <= NPM, "ring slots sized for fewer moment pairs");
 
     const StepArgs& a;
     const CUtensorMap* map;
-    uint64_t* bars;
-    unsigned char* stages;
-    float4* e4t[2];   // this thread's exchange slots, buffer 0 and 1
-    float* e1t[2];
+    const SM& sm;
     unsigned g0;
-    int toff;         // this thread's element offset in a stage
-    int x, y, z0, Y0, p0, nprod;
-    bool interior;
+    int X0, Y0, z0, p0, nprod;
     int cs;           // ring slot of the next production to wait for
     unsigned cph;     // its mbarrier phase parity
-    float4* e4g[2];   // thermal: this thread's exchange slots, buffer 0 and 1
-    float* e1g[2];
 
     __device__ __forceinline__ int slot(int k) const { return (int)((g0 + (unsigned)k) % NS); }
     __device__ __forceinline__ unsigned phase(int k) const { return ((g0 + (unsigned)k) / NS) & 1u; }
     static constexpr size_t ring_stride = SM::stage_max;
-    __device__ __forceinline__ const T* stage_ptr() const
-    {
-        return reinterpret_cast<const T*>(stages + cs * ring_stride) + toff;
-    }
+    __device__ __forceinline__ const T* stage_base() const { return reinterpret_cast<const T*>(sm.stages + cs * ring_stride); }
+    // element offset of node x of stage row er (pair of moments 0, 1)
+    __device__ __forceinline__ int stage_off(int er, int x) const { return er * ROW + 2 * ((x + XOFF) - p0); }
     __device__ __forceinline__ void load_slot(int s, int k) const
     {
-        mbar_expect_tx(&bars[s], (unsigned)stage_bytes);
+        mbar_expect_tx(&sm.bars[s], (unsigned)stage_bytes);
         // x runs over the interleaved pair elements: 2 per node
-        tma_load_4d(stages + s * ring_stride, map, 2 * p0, 0, Y0, z0 + k, &bars[s]);
+        tma_load_4d(sm.stages + s * ring_stride, map, 2 * p0, 0, Y0, z0 + k, &sm.bars[s]);
     }
     __device__ __forceinline__ void load(int k) const { load_slot(slot(k), k); }
     // CTA-wide timeout flag next to the ring barriers: a thread whose bounded
     // wait gave up raises it before the per-plane barrier, every thread reads
     // it after (a plain barrier measured 3 % faster than a reducing one)
-    __device__ __forceinline__ void raise_timeout() const { *reinterpret_cast<volatile int*>(bars + NSTAGE_MAX) = 1; }
-    __device__ __forceinline__ bool timed_out() const { return *reinterpret_cast<volatile int*>(bars + NSTAGE_MAX) != 0; }
+    __device__ __forceinline__ void raise_timeout() const { *reinterpret_cast<volatile int*>(sm.bars + NSTAGE_MAX) = 1; }
+    __device__ __forceinline__ bool timed_out() const { return *reinterpret_cast<volatile int*>(sm.bars + NSTAGE_MAX) != 0; }
     // after production k: reload its slot with production k + NS, then move
     // to the next slot
     __device__ __forceinline__ void advance(int k)
     {
-        if (threadIdx.x == 0 && k + NS < nprod) {
+        if (threadIdx.x == TMA_THREAD && k + NS < nprod) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             load_slot(cs, k + NS);
         }
@@ -1136,6 +1251,28 @@ struct ZMarch {
             cph ^= 1u;
         }
     }
+    // end of pipeline step k: barrier, timeout check, ring advance
+    __device__ __forceinline__ bool end_step(int k, bool ok)
+    {
+        if (!ok) raise_timeout();
+        __syncthreads();
+        if (timed_out()) return false;
+        advance(k);
+        return true;
+    }
+
+    // ---- interior warps: row w, lane l = node (X0 + l, Y0 + w)
+    struct Interior {
+        float4* e4t[2];   // this thread's exchange slots, buffer 0 and 1
+        float* e1t[2];
+        const float4* eet[2];  // its edge-buffer float4 (used by lanes 0 and 31)
+        float4* e4g[2];   // thermal
+        float* e1g[2];
+        const float4* eetg[2];
+        int toff;         // its element offset in a stage
+        int x, y;
+        bool interior, xlo, xhi;
+    };
 
     // pipeline step j (parity PAR = j & 1): production j into exchange
     // buffer PAR and consumption j-1 from buffer PAR ^ 1, one barrier.  The
@@ -1144,32 +1281,135 @@ struct ZMarch {
     // overwrites it.  Returns false when a bounded wait timed out somewhere
     // in the CTA.
     template <int PAR, bool LIGHT = false>
-    __device__ __forceinline__ bool iter(int j, float (&gsh_new)[Q], const float (&gsh_old)[Q], float (&up)[NUP],
-                                         float (&mid)[NMID], float& om_par, float* sg_new = nullptr,
+    __device__ __forceinline__ bool iter(const Interior& it, int j, float (&gsh_new)[Q], const float (&gsh_old)[Q],
+                                         float (&up)[NUP], float (&mid)[NMID], float& om_par, float* sg_new = nullptr,
                                          const float* sg_old = nullptr, float* upg = nullptr, float* midg = nullptr)
     {
-        const bool ok = mbar_wait(&bars[cs], cph);
+        const bool ok = mbar_wait(&sm.bars[cs], cph);
         const float om_out = om_par;
         // the two halves are independent; which comes first in the source
         // only steers the compiler's schedule (results are bit-identical):
         // consumption first measured 4 % faster on bulk and D3Q27 domains,
         // production first 4 % faster on D3Q19 domains with walls
         if constexpr (Q == 27 || (FLAGS & F_BC) == 0) {
-            prod_b<Q, NM, NUP, NMID, T, FLAGS, TYI, BCP, LIGHT>(a, j - 1, z0 - 2 + j, e4t[PAR ^ 1], e1t[PAR ^ 1],
-                                                           interior, x, y, gsh_old, up, mid, om_out, e4g[PAR ^ 1],
-                                                           e1g[PAR ^ 1], sg_old, upg, midg);
-            prod_a<Q, NM, T, TYI, TH>(a, stage_ptr(), e4t[PAR], e1t[PAR], gsh_new, om_par, e4g[PAR], e1g[PAR], sg_new);
+            prod_b<Q, NM, NUP, NMID, T, FLAGS, TYI, BCP, LIGHT>(
+                a, j - 1, z0 - 2 + j, it.e4t[PAR ^ 1], it.e1t[PAR ^ 1], it.eet[PAR ^ 1], it.xlo, it.xhi, it.interior,
+                it.x, it.y, gsh_old, up, mid, om_out, it.e4g[PAR ^ 1], it.e1g[PAR ^ 1], it.eetg[PAR ^ 1], sg_old, upg,
+                midg);
+            prod_a<Q, NM, T, TYI, TH>(a, stage_base() + it.toff, it.e4t[PAR], it.e1t[PAR], gsh_new, om_par,
+                                      it.e4g[PAR], it.e1g[PAR], sg_new);
         } else {
-            prod_a<Q, NM, T, TYI, TH>(a, stage_ptr(), e4t[PAR], e1t[PAR], gsh_new, om_par, e4g[PAR], e1g[PAR], sg_new);
-            prod_b<Q, NM, NUP, NMID, T, FLAGS, TYI, BCP, LIGHT>(a, j - 1, z0 - 2 + j, e4t[PAR ^ 1], e1t[PAR ^ 1],
-                                                           interior, x, y, gsh_old, up, mid, om_out, e4g[PAR ^ 1],
-                                                           e1g[PAR ^ 1], sg_old, upg, midg);
+            prod_a<Q, NM, T, TYI, TH>(a, stage_base() + it.toff, it.e4t[PAR], it.e1t[PAR], gsh_new, om_par,
+                                      it.e4g[PAR], it.e1g[PAR], sg_new);
+            prod_b<Q, NM, NUP, NMID, T, FLAGS, TYI, BCP, LIGHT>(
+                a, j - 1, z0 - 2 + j, it.e4t[PAR ^ 1], it.e1t[PAR ^ 1], it.eet[PAR ^ 1], it.xlo, it.xhi, it.interior,
+                it.x, it.y, gsh_old, up, mid, om_out, it.e4g[PAR ^ 1], it.e1g[PAR ^ 1], it.eetg[PAR ^ 1], sg_old, upg,
+                midg);
         }
-        if (!ok) raise_timeout();
-        __syncthreads();
-        if (timed_out()) return false;
-        advance(j);
-        return true;
+        return end_step(j, ok);
+    }
+
+    // the interior pipeline; returns the production whose step timed out, or -1
+    __device__ __forceinline__ int interior_loop(int lane, int warp)
+    {
+        const int er = warp + 1;
+        const int ts = EX::slot(er, lane + 1);
+        const int eside = lane >= TILE_X / 2 ? 1 : 0;
+        Interior it;
+        it.e4t[0] = sm.ex4 + ts; it.e4t[1] = sm.ex4 + EX::buf4 + ts;
+        it.e1t[0] = sm.ex1 + ts; it.e1t[1] = sm.ex1 + EX::buf1 + ts;
+        it.eet[0] = sm.edge + (eside * 2 + 0) * NR + er; it.eet[1] = sm.edge + (eside * 2 + 1) * NR + er;
+        it.e4g[0] = sm.exg4 + ts; it.e4g[1] = sm.exg4 + EXG::buf4 + ts;
+        it.e1g[0] = sm.exg1 + ts; it.e1g[1] = sm.exg1 + EXG::buf1 + ts;
+        it.eetg[0] = sm.edgeg + (eside * 2 + 0) * NR + er; it.eetg[1] = sm.edgeg + (eside * 2 + 1) * NR + er;
+        it.x = X0 + lane;
+        it.y = Y0 + warp;
+        it.toff = stage_off(er, it.x);
+        it.interior = it.x < a.nx && it.y < a.ny;
+        it.xlo = lane == 0;
+        it.xhi = lane == TILE_X - 1;
+
+        float upA[NUP], upB[NUP], mid[NMID], gA[Q], gB[Q];
+#pragma unroll
+        for (int s = 0; s < NUP; s++) upA[s] = upB[s] = 0.f;
+#pragma unroll
+        for (int s = 0; s < NMID; s++) mid[s] = 0.f;
+        float omA = a.omega0, omB = a.omega0;
+        // thermal populations: the same pipeline on the D3Q19 directions
+        constexpr int NUPG = TH ? lat_num_cz(19, 1) : 1, NMIDG = TH ? lat_num_cz(19, 0) : 1;
+        constexpr int NSG = TH ? 19 : 1;
+        float ugA[NUPG], ugB[NUPG], mg[NMIDG], sgA[NSG], sgB[NSG];
+#pragma unroll
+        for (int s = 0; s < NUPG; s++) ugA[s] = ugB[s] = 0.f;
+#pragma unroll
+        for (int s = 0; s < NMIDG; s++) mg[s] = 0.f;
+
+        {
+            // prologue: production 0 only (exchange buffer 0)
+            const bool ok = mbar_wait(&sm.bars[cs], cph);
+            prod_a<Q, NM, T, TYI, TH>(a, stage_base() + it.toff, it.e4t[0], it.e1t[0], gA, omA, it.e4g[0], it.e1g[0],
+                                      sgA);
+            if (!end_step(0, ok)) return 0;
+        }
+        // even productions use gA / upA and exchange buffer 0, odd ones gB / upB
+        // and buffer 1: no register copies, no buffer selection at run time.
+        // Consumptions 0 and 1 would complete planes z0 - 2 and z0 - 1, which
+        // are not this column's: they only move the z pipeline (nprod >= 3, so
+        // productions 1 and 2 exist).  The thermal variants keep them in the
+        // loop: two more inlined pipeline steps raise their register spills.
+        int j = 1;
+        if constexpr (!TH) {
+            if (!iter<1, true>(it, 1, gB, gA, upA, mid, omB, sgB, sgA, ugA, mg)) return 1;
+            if (!iter<0, true>(it, 2, gA, gB, upB, mid, omA, sgA, sgB, ugB, mg)) return 2;
+            j = 3;
+        }
+        for (;;) {
+            // epilogues consume the last production j-1; its output plane is that
+            // of production j-2, whose omega has the parity of j
+            if (j >= nprod) {  // j odd: last production even
+                prod_b<Q, NM, NUP, NMID, T, FLAGS, TYI, BCP>(a, j - 1, z0 - 2 + j, it.e4t[0], it.e1t[0], it.eet[0],
+                                                            it.xlo, it.xhi, it.interior, it.x, it.y, gA, upA, mid, omB,
+                                                            it.e4g[0], it.e1g[0], it.eetg[0], sgA, ugA, mg);
+                return -1;
+            }
+            if (!iter<1>(it, j, gB, gA, upA, mid, omB, sgB, sgA, ugA, mg)) return j;
+            j++;
+            if (j >= nprod) {  // j even: last production odd
+                prod_b<Q, NM, NUP, NMID, T, FLAGS, TYI, BCP>(a, j - 1, z0 - 2 + j, it.e4t[1], it.e1t[1], it.eet[1],
+                                                            it.xlo, it.xhi, it.interior, it.x, it.y, gB, upB, mid, omA,
+                                                            it.e4g[1], it.e1g[1], it.eetg[1], sgB, ugB, mg);
+                return -1;
+            }
+            if (!iter<0>(it, j, gA, gB, upB, mid, omA, sgA, sgB, ugB, mg)) return j;
+            j++;
+        }
+    }
+
+    // the helper pipeline (SIDE -1: bottom row and left edge, +1: top row and
+    // right edge); returns the production whose step timed out, or -1
+    template <int SIDE>
+    __device__ __forceinline__ int helper_loop(int lane)
+    {
+        constexpr int erh = SIDE < 0 ? 0 : TYI + 1;          // exchange row of the halo row
+        constexpr int ece = SIDE < 0 ? 0 : EX_COLS - 1;      // exchange column of the edge nodes
+        const int hoff = stage_off(erh, X0 + lane);
+        const int eoff = stage_off(lane, SIDE < 0 ? X0 - 1 : X0 + TILE_X);
+        const int sh = EX::slot(erh, lane + 1), se = EX::slot(lane, ece);
+        const int side = SIDE < 0 ? 0 : 1;
+        for (int j = 0; j < nprod; j++) {
+            const bool ok = mbar_wait(&sm.bars[cs], cph);
+            const int par = j & 1;
+            const T* st = stage_base();
+            float4* e4 = sm.ex4 + par * EX::buf4;
+            float* e1 = sm.ex1 + par * EX::buf1;
+            float4* g4 = sm.exg4 + par * EXG::buf4;
+            float* g1 = sm.exg1 + par * EXG::buf1;
+            prod_helper<Q, NM, T, TYI, SIDE, TH>(a, lane, st + hoff, st + eoff, e4 + sh, e1 + sh, e4 + se, e1 + se,
+                                                 sm.edge + (side * 2 + par) * NR, g4 + sh, g1 + sh, g4 + se, g1 + se,
+                                                 sm.edgeg + (side * 2 + par) * NR);
+            if (!end_step(j, ok)) return j;
+        }
+        return -1;
     }
 };
 
@@ -1182,92 +1422,28 @@ __device__ __forceinline__ bool zmarch_column(const StepArgs& a, const CUtensorM
                                               unsigned& g0)
 {
     using ZM = ZMarch<Q, T, FLAGS, TYI, BCP, NPM>;
-    constexpr int NUP = ZM::NUP, NMID = ZM::NMID;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int x = X0 - 1 + lane, y = Y0 - 1 + warp;
-    constexpr int ALIGN = 16 / (int)sizeof(T);      // elements per 16 bytes (TMA x alignment)
-    const int p0 = (X0 - 1 + XOFF) & ~(ALIGN - 1);  // aligned box start (padded column)
-    // stage rows are [row][pair][2 * BOX_X]: this thread's pair of moments
-    // 0, 1 is at element 2 * col of its row
-    const int ts = ZM::EX::thread_slot(warp, lane);
-    ZM zm{a, map, sm.bars, sm.stages,
-          {sm.ex4 + ts, sm.ex4 + ZM::EX::buf4 + ts},
-          {sm.ex1 + ts, sm.ex1 + ZM::EX::buf1 + ts},
-          g0, warp * ZM::NP * 2 * BOX_X + 2 * ((x + XOFF) - p0), x, y, z0, Y0, p0,
-          zend - z0 + 2 /* planes z0-1 .. zend */,
-          lane >= 1 && lane <= TILE_X && x < a.nx && warp >= 1 && warp <= TYI && y < a.ny,
-          0, 0u,
-          {sm.exg4 + ts, sm.exg4 + Exchange<19, ZM::NW>::buf4 + ts},
-          {sm.exg1 + ts, sm.exg1 + Exchange<19, ZM::NW>::buf1 + ts}};
+    // aligned box start (padded column): the TMA x coordinate, 2 elements a
+    // node, must be a multiple of 16 bytes
+    constexpr int NODE_ALIGN = 8 / (int)sizeof(T);
+    const int p0 = (X0 - 1 + XOFF) & ~(NODE_ALIGN - 1);
+    ZM zm{a, map, sm, g0, X0, Y0, z0, p0, zend - z0 + 2 /* planes z0-1 .. zend */, 0, 0u};
     zm.cs = zm.slot(0);
     zm.cph = zm.phase(0);
 
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == ZM::TMA_THREAD) {
         // the ring was last read through the generic proxy (previous column)
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         for (int s = 0; s < ZM::NS && s < zm.nprod; s++) zm.load(s);
     }
-
-    float upA[NUP], upB[NUP], mid[NMID], gA[Q], gB[Q];
-#pragma unroll
-    for (int s = 0; s < NUP; s++) upA[s] = upB[s] = 0.f;
-#pragma unroll
-    for (int s = 0; s < NMID; s++) mid[s] = 0.f;
-    float omA = a.omega0, omB = a.omega0;
-    // thermal populations: the same pipeline on the D3Q19 directions
-    constexpr int NUPG = ZM::TH ? lat_num_cz(19, 1) : 1, NMIDG = ZM::TH ? lat_num_cz(19, 0) : 1;
-    constexpr int NSG = ZM::TH ? 19 : 1;
-    float ugA[NUPG], ugB[NUPG], mg[NMIDG], sgA[NSG], sgB[NSG];
-#pragma unroll
-    for (int s = 0; s < NUPG; s++) ugA[s] = ugB[s] = 0.f;
-#pragma unroll
-    for (int s = 0; s < NMIDG; s++) mg[s] = 0.f;
-
-    int kfail = -1;
-    {
-        // prologue: production 0 only (exchange buffer 0)
-        const bool ok = mbar_wait(&sm.bars[zm.cs], zm.cph);
-        prod_a<Q, ZM::NM, T, TYI, ZM::TH>(a, zm.stage_ptr(), zm.e4t[0], zm.e1t[0], gA, omA, zm.e4g[0], zm.e1g[0], sgA);
-        if (!ok) zm.raise_timeout();
-        __syncthreads();
-        if (zm.timed_out()) kfail = 0;
-        else zm.advance(0);
-    }
-    // even productions use gA / upA and exchange buffer 0, odd ones gB / upB
-    // and buffer 1: no register copies, no buffer selection at run time.
-    // Consumptions 0 and 1 would complete planes z0 - 2 and z0 - 1, which
-    // are not this column's: they only move the z pipeline (nprod >= 3, so
-    // productions 1 and 2 exist).  The thermal variants keep them in the
-    // loop: two more inlined pipeline steps raise their register spills and
-    // cost 6 % there.
-    int j = 1;
-    if constexpr (!ZM::TH) {
-        if (kfail < 0 && !zm.template iter<1, true>(1, gB, gA, upA, mid, omB, sgB, sgA, ugA, mg)) kfail = 1;
-        if (kfail < 0 && !zm.template iter<0, true>(2, gA, gB, upB, mid, omA, sgA, sgB, ugB, mg)) kfail = 2;
-        j = 3;
-    }
-    while (kfail < 0) {
-        // epilogues consume the last production j-1; its output plane is that
-        // of production j-2, whose omega has the parity of j
-        if (j >= zm.nprod) {  // j odd: last production even
-            prod_b<Q, ZM::NM, NUP, NMID, T, FLAGS, TYI, BCP>(a, j - 1, z0 - 2 + j, zm.e4t[0], zm.e1t[0], zm.interior, x,
-                                                        y, gA, upA, mid, omB, zm.e4g[0], zm.e1g[0], sgA, ugA, mg);
-            break;
-        }
-        if (!zm.template iter<1>(j, gB, gA, upA, mid, omB, sgB, sgA, ugA, mg)) { kfail = j; break; }
-        j++;
-        if (j >= zm.nprod) {  // j even: last production odd
-            prod_b<Q, ZM::NM, NUP, NMID, T, FLAGS, TYI, BCP>(a, j - 1, z0 - 2 + j, zm.e4t[1], zm.e1t[1], zm.interior, x,
-                                                        y, gB, upB, mid, omA, zm.e4g[1], zm.e1g[1], sgB, ugB, mg);
-            break;
-        }
-        if (!zm.template iter<0>(j, gA, gB, upB, mid, omA, sgA, sgB, ugB, mg)) { kfail = j; break; }
-        j++;
-    }
+    int kfail;
+    if (warp < TYI) kfail = zm.interior_loop(lane, warp);
+    else if (warp == TYI) kfail = zm.template helper_loop<-1>(lane);
+    else kfail = zm.template helper_loop<1>(lane);
     if (kfail >= 0) {
         // a bounded wait gave up: flag it, give the copies still in flight a
         // bounded time to land, and leave together
-        if (threadIdx.x == 0) {
+        if (threadIdx.x == ZM::TMA_THREAD) {
             atomicOr(a.err, 1);
             for (int q = kfail; q < zm.nprod && q < kfail + ZM::NS; q++) (void)mbar_wait(&sm.bars[zm.slot(q)], zm.phase(q));
         }

@@ -337,7 +337,7 @@ mrlbm_status mrlbm::domain_alloc(mrlbm_domain* dom)
         CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
         dom->nsm = nsm > 0 ? nsm : 148;
     }
-    dom->lz = choose_lz(dom);
+    for (int k = 0; k < 2; k++) dom->lz_t[k] = choose_lz(dom, tile_rows_of_kind(k));
     return MRLBM_OK;
 }
 
@@ -345,10 +345,9 @@ mrlbm_status mrlbm::domain_alloc(mrlbm_domain* dom)
 // lz outputs, and the grid runs in ceil(CTAs / SMs) waves, so the step time
 // goes as waves * (lz + 2 + start-up): pick the chunk count that minimises it (the last
 // wave full, few restarts).
-int mrlbm::choose_lz(const mrlbm_domain* dom)
+int mrlbm::choose_lz(const mrlbm_domain* dom, int ty)
 {
     const mrlbm_desc& d = dom->d;
-    const int ty = tile_y(dom->q);
     const long long cols = (long long)((d.nx + TILE_X - 1) / TILE_X) * ((d.ny + ty - 1) / ty);
     long long best_cost = -1;
     int best = d.nz;
@@ -626,7 +625,6 @@ void mrlbm::fill_step_args(const mrlbm_domain* dom, StepArgs& a, int parity, int
     a.nx = d.nx; a.ny = d.ny; a.nz = d.nz; a.pitch = dom->pitch;
     a.plane = dom->plane; a.field = dom->field;
     a.periodic = (d.periodic[0] ? 1 : 0) | (d.periodic[1] ? 2 : 0) | (d.periodic[2] ? 4 : 0);
-    a.lz = dom->lz;
     a.step = dom->step;
     a.rho0 = (float)d.rho0;
     a.omega0 = (float)dom->omega0;
@@ -647,6 +645,7 @@ void mrlbm::fill_step_args(const mrlbm_domain* dom, StepArgs& a, int parity, int
     if (flags & (F_POWERLAW | F_BINGHAM)) flags |= F_BC;  // nnf variants always read the class map
     if (d.thermal) flags |= F_THERMAL | F_FORCE;           // the Boussinesq force is per node
     if (dom->has_outflow) flags |= F_OUTFLOW;
+    a.lz = dom->lz > 0 ? dom->lz : dom->lz_t[tile_kind(tile_rows(flags))];
 }
 
 mrlbm_status mrlbm::enqueue_step(mrlbm_domain* dom, int parity, cudaStream_t s)
@@ -657,15 +656,15 @@ mrlbm_status mrlbm::enqueue_step(mrlbm_domain* dom, int parity, cudaStream_t s)
     const int q = dom->q;
     const int stg = dom->d.storage;
     mrlbm_status st;
-    const CUtensorMap& map = dom->tmap[parity];
+    const CUtensorMap* maps = dom->tmap[parity];
     if (q == 19) {
-        if (stg == MRLBM_F32) st = dispatch_step<19, float>(map, a, flags, s);
-        else if (stg == MRLBM_F16) st = dispatch_step<19, __half>(map, a, flags, s);
-        else st = dispatch_step<19, __nv_bfloat16>(map, a, flags, s);
+        if (stg == MRLBM_F32) st = dispatch_step<19, float>(maps, a, flags, s);
+        else if (stg == MRLBM_F16) st = dispatch_step<19, __half>(maps, a, flags, s);
+        else st = dispatch_step<19, __nv_bfloat16>(maps, a, flags, s);
     } else {
-        if (stg == MRLBM_F32) st = dispatch_step<27, float>(map, a, flags, s);
-        else if (stg == MRLBM_F16) st = dispatch_step<27, __half>(map, a, flags, s);
-        else st = dispatch_step<27, __nv_bfloat16>(map, a, flags, s);
+        if (stg == MRLBM_F32) st = dispatch_step<27, float>(maps, a, flags, s);
+        else if (stg == MRLBM_F16) st = dispatch_step<27, __half>(maps, a, flags, s);
+        else st = dispatch_step<27, __nv_bfloat16>(maps, a, flags, s);
     }
     return st;
 }
@@ -910,10 +909,10 @@ static EncodeTiledFn encode_fn()
     return fn;
 }
 
-// 4-D map over one padded moment buffer with dimension order (x and pair
-// element, moment pair, y, z) so that a box of (2 * 40, pairs, tile_y(q) + 2,
+// 4-D maps over each padded moment buffer with dimension order (x and pair
+// element, moment pair, y, z) so that a box of (2 * box width, pairs, rows + 2,
 // 1) lands in shared memory as [row][pair][x][2]: one plane of a CTA column
-// per copy.
+// and its two outer rows per copy; one map per tile height.
 mrlbm_status mrlbm::make_tensor_maps(mrlbm_domain* dom)
 {
     EncodeTiledFn enc = encode_fn();
@@ -929,13 +928,16 @@ mrlbm_status mrlbm::make_tensor_maps(mrlbm_domain* dom)
     const cuuint64_t dims[4] = {(cuuint64_t)(2 * dom->pitch), npairs, (cuuint64_t)(d.ny + 2), (cuuint64_t)(d.nz + 2)};
     const cuuint64_t strides[3] = {(cuuint64_t)(2 * dom->field) * es, (cuuint64_t)(2 * dom->pitch) * es,
                                    (cuuint64_t)(2 * dom->plane) * es};
-    const cuuint32_t box[4] = {(cuuint32_t)(2 * BOX_X), npairs, (cuuint32_t)(tile_y(dom->q) + 2), 1};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
-    for (int b = 0; b < 2; b++) {
-        CUresult r = enc(&dom->tmap[b], dt, 4, dom->m[b], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-        if (r != CUDA_SUCCESS) return fail(MRLBM_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    for (int k = 0; k < 2; k++) {
+        const cuuint32_t box[4] = {(cuuint32_t)(2 * box_x_nodes((int)es)), npairs,
+                                   (cuuint32_t)(tile_rows_of_kind(k) + 2), 1};
+        for (int b = 0; b < 2; b++) {
+            CUresult r = enc(&dom->tmap[b][k], dt, 4, dom->m[b], dims, strides, box, estr,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r != CUDA_SUCCESS) return fail(MRLBM_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+        }
     }
     return MRLBM_OK;
 }

@@ -4,18 +4,21 @@
 // caller holds on the device in the reference's idxMom layout (the fMom array
 // of the reference's host loop, src/arrayIndex.h:8-17).  Its block partials
 // live in a file-scope __device__ array, so the call performs no allocation:
-// no cudaMalloc/cudaFree and no allocating library routine.
+// no cudaMalloc, no cudaFree and no allocating library routine.
 //
 // Limits and rules (also stated at the declaration in include/mrlbm.h):
 //   * scratch: NOALLOC_SCRATCH doubles (37,952 bytes) per device: 592 block
 //     partials of 8 sums plus the 8 results.  The call always launches 592
-//     blocks of 256 threads and strides over larger fields, so any field fits;
-//     a request for more partials than the array holds is rejected.
+//     blocks of 256 threads and strides over larger fields, so every field
+//     size fits the array (checked at compile time).
 //   * nothing in the scratch has to start at zero: each call writes every
 //     partial before the finishing kernel reads it, and writes all 8 results.
-//   * the first call on a device looks up the array's address with
-//     cudaGetSymbolAddress (once per device, with that device current); make
-//     that first call before any stream capture begins.
+//   * the array's device address is looked up with cudaGetSymbolAddress, with
+//     the device current, on the first call in each CUDA context of a device
+//     (again after a cudaDeviceReset, which replaces the context and may move
+//     the array).
+//   * every call synchronises `stream` to return the sums on the host, so no
+//     call can be made while `stream` is being captured into a graph.
 //   * calls share the one array per device: calls whose executions overlap on
 //     a device (two host threads, or two streams with no ordering between
 //     them) race on it and return wrong sums.  Serialise them.
@@ -34,6 +37,7 @@ constexpr int NOALLOC_THREADS = 256;
 constexpr int NOALLOC_BLOCKS = 148 * 4;
 constexpr int NOALLOC_SCRATCH = NOALLOC_BLOCKS * 8 + 8;
 constexpr int NOALLOC_MAX_DEVICES = 64;
+static_assert(NOALLOC_BLOCKS * 8 + 8 <= NOALLOC_SCRATCH, "the static scratch holds every block partial");
 
 // FP64 block partials over all nodes of an FP32 idxMom field:
 //   [0] rho, [1..3] rho u, [4] rho |u|^2 / 2, [5] nodes, [6] max |u|,
@@ -98,6 +102,22 @@ __global__ void noalloc_reduce_finish(const double* partial, int nblocks, double
 
 std::mutex g_setup_mutex;
 double* g_scratch_ptr[NOALLOC_MAX_DEVICES] = {};
+void* g_scratch_ctx[NOALLOC_MAX_DEVICES] = {};  // the CUDA context the address belongs to
+
+// cuCtxGetCurrent through the runtime's driver entry point (no libcuda link)
+typedef int (*CtxGetCurrentFn)(void**);
+CtxGetCurrentFn ctx_get_current()
+{
+    static CtxGetCurrentFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (CtxGetCurrentFn)p;
+    }
+    return fn;
+}
 
 }  // namespace
 
@@ -114,29 +134,35 @@ extern "C" mrlbm_status mrlbm_reduce_fp64_ref_layout_noalloc(const float* fmom, 
         return fail(MRLBM_EINVAL, "grid %d x %d x %d: the idxMom layout needs positive multiples of 8", nx, ny, nz);
     if (num_moments < 4) return fail(MRLBM_EINVAL, "num_moments %d: need at least rho and u (4)", num_moments);
     const int blocks = NOALLOC_BLOCKS;
-    if ((long long)blocks * 8 + 8 > NOALLOC_SCRATCH)
-        return fail(MRLBM_EINVAL, "reduction needs %lld doubles of scratch, the static array holds %d",
-                    (long long)blocks * 8 + 8, NOALLOC_SCRATCH);
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return fail(MRLBM_ECUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
     if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(MRLBM_EINVAL, "device %d beyond %d", dev, NOALLOC_MAX_DEVICES);
-    // the field must be device memory of the current device
+    // the field must be device memory of the current device, or managed
+    // memory (which every device can read, wherever it was allocated)
     cudaPointerAttributes pa{};
     e = cudaPointerGetAttributes(&pa, fmom);
     if (e != cudaSuccess) return fail(MRLBM_EINVAL, "cudaPointerGetAttributes: %s", cudaGetErrorString(e));
     if (pa.type != cudaMemoryTypeDevice && pa.type != cudaMemoryTypeManaged)
         return fail(MRLBM_EINVAL, "fmom is not device memory (the field must be resident on the current device)");
-    if (pa.device != dev)
+    if (pa.type == cudaMemoryTypeDevice && pa.device != dev)
         return fail(MRLBM_EINVAL, "fmom is on device %d, the current device is %d", pa.device, dev);
     double* scratch = nullptr;
     {
+        // the array's address, looked up once per device and CUDA context
+        // (the pointer query above has made the device's context current)
+        CtxGetCurrentFn gc = ctx_get_current();
+        if (!gc) return fail(MRLBM_ECUDA, "cuCtxGetCurrent unavailable");
+        void* ctx = nullptr;
+        if (gc(&ctx) != 0) ctx = nullptr;
         std::lock_guard<std::mutex> lock(g_setup_mutex);
-        if (!g_scratch_ptr[dev]) {
+        if (!g_scratch_ptr[dev] || !ctx || g_scratch_ctx[dev] != ctx) {
             void* p = nullptr;
             e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
             if (e != cudaSuccess) return fail(MRLBM_ECUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
+            if (gc(&ctx) != 0) ctx = nullptr;
             g_scratch_ptr[dev] = static_cast<double*>(p);
+            g_scratch_ctx[dev] = ctx;
         }
         scratch = g_scratch_ptr[dev];
     }

@@ -278,7 +278,7 @@ extern "C" mrlbm_status mrlbm_server_tick(mrlbm_server* s, int* active_out)
         if ((st = mrlbm_batch_domain(s->batch, s->reqs[s->active[0]].member, &dom))) return st;
         // the single-domain grid's own z chunking (the batch sets its own
         // chunk again before its next step)
-        dom->lz = mrlbm::choose_lz(dom);
+        dom->lz = 0;
         if ((st = mrlbm_step(dom, s->steps_per_tick))) return st;
     } else if (!s->active.empty()) {
         if ((st = mrlbm_batch_step(s->batch, s->steps_per_tick))) return st;

@@ -10,10 +10,11 @@
 namespace mrlbm {
 
 template <int Q, typename T, int FLAGS, typename BCP = TableBC>
-static mrlbm_status launch_step_t(const CUtensorMap& map, const StepArgs& a, cudaStream_t s)
+static mrlbm_status launch_step_t(const CUtensorMap* maps, const StepArgs& a, cudaStream_t s)
 {
-    constexpr int TYI = tile_y(Q);
+    constexpr int TYI = tile_rows(FLAGS);
     constexpr int NW = TYI + 2;
+    const CUtensorMap& map = maps[tile_kind(TYI)];
     constexpr size_t smem = step_smem_bytes<Q, T, FLAGS, TYI>();
     static_assert(smem <= 232448, "shared memory over the sm_100 limit");
     auto kern = zmarch_step<Q, T, FLAGS, TYI, BCP>;
@@ -31,27 +32,27 @@ static mrlbm_status launch_step_t(const CUtensorMap& map, const StepArgs& a, cud
 }
 
 template <int Q, typename T>
-mrlbm_status dispatch_step(const CUtensorMap& map, const StepArgs& a, int flags, cudaStream_t s)
+mrlbm_status dispatch_step(const CUtensorMap* maps, const StepArgs& a, int flags, cudaStream_t s)
 {
     switch (flags) {
-        case 0: return launch_step_t<Q, T, 0>(map, a, s);
-        case F_BC: return launch_step_t<Q, T, F_BC>(map, a, s);
-        case F_FORCE: return launch_step_t<Q, T, F_FORCE>(map, a, s);
-        case F_BC | F_FORCE: return launch_step_t<Q, T, F_BC | F_FORCE>(map, a, s);
-        case F_BC | F_POWERLAW: return launch_step_t<Q, T, F_BC | F_POWERLAW>(map, a, s);
-        case F_BC | F_FORCE | F_POWERLAW: return launch_step_t<Q, T, F_BC | F_FORCE | F_POWERLAW>(map, a, s);
-        case F_BC | F_BINGHAM: return launch_step_t<Q, T, F_BC | F_BINGHAM>(map, a, s);
-        case F_BC | F_FORCE | F_BINGHAM: return launch_step_t<Q, T, F_BC | F_FORCE | F_BINGHAM>(map, a, s);
+        case 0: return launch_step_t<Q, T, 0>(maps, a, s);
+        case F_BC: return launch_step_t<Q, T, F_BC>(maps, a, s);
+        case F_FORCE: return launch_step_t<Q, T, F_FORCE>(maps, a, s);
+        case F_BC | F_FORCE: return launch_step_t<Q, T, F_BC | F_FORCE>(maps, a, s);
+        case F_BC | F_POWERLAW: return launch_step_t<Q, T, F_BC | F_POWERLAW>(maps, a, s);
+        case F_BC | F_FORCE | F_POWERLAW: return launch_step_t<Q, T, F_BC | F_FORCE | F_POWERLAW>(maps, a, s);
+        case F_BC | F_BINGHAM: return launch_step_t<Q, T, F_BC | F_BINGHAM>(maps, a, s);
+        case F_BC | F_FORCE | F_BINGHAM: return launch_step_t<Q, T, F_BC | F_FORCE | F_BINGHAM>(maps, a, s);
         // outflow walls (Newtonian domains, as the reference's outflow cases)
-        case F_BC | F_OUTFLOW: return launch_step_t<Q, T, F_BC, OutflowBC>(map, a, s);
-        case F_BC | F_FORCE | F_OUTFLOW: return launch_step_t<Q, T, F_BC | F_FORCE, OutflowBC>(map, a, s);
+        case F_BC | F_OUTFLOW: return launch_step_t<Q, T, F_BC, OutflowBC>(maps, a, s);
+        case F_BC | F_FORCE | F_OUTFLOW: return launch_step_t<Q, T, F_BC | F_FORCE, OutflowBC>(maps, a, s);
         default: break;
     }
     // thermal scalar: D3Q19 with FP32 storage only (its second row exchange
     // fits next to the D3Q19 flow's in shared memory)
     if constexpr (Q == 19 && is_f32<T>()) {
-        if (flags == (F_THERMAL | F_FORCE)) return launch_step_t<Q, T, F_THERMAL | F_FORCE>(map, a, s);
-        if (flags == (F_THERMAL | F_FORCE | F_BC)) return launch_step_t<Q, T, F_THERMAL | F_FORCE | F_BC>(map, a, s);
+        if (flags == (F_THERMAL | F_FORCE)) return launch_step_t<Q, T, F_THERMAL | F_FORCE>(maps, a, s);
+        if (flags == (F_THERMAL | F_FORCE | F_BC)) return launch_step_t<Q, T, F_THERMAL | F_FORCE | F_BC>(maps, a, s);
     }
     return fail(MRLBM_EINVAL, "unsupported step flag combination %d", flags);
 }

@@ -4,7 +4,7 @@
 # itself, used as a parity pin and as the reference GPU baseline; nothing in
 # the product links or calls them.
 #
-#   bash oracle/build_ref_cuda.sh [REF=/root/reference]
+#   REF=<reference checkout> bash oracle/build_ref_cuda.sh
 #
 # The reference tree is copied to a scratch folder under /tmp and only that
 # copy is edited (the reference stays read-only):
@@ -21,7 +21,7 @@
 #   _ref/cases/*             the same cases compiled in this library's case mode
 # CASES_ONLY=1 rebuilds only the case-mode programs; THERMAL_ONLY=1 only refsim_rb64.
 set -euo pipefail
-REF=${REF:-/root/reference}
+REF=${REF:?set REF to the reference checkout (its src/ folder is read)}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
 NVCC=${NVCC:-/usr/local/cuda/bin/nvcc}

@@ -70,6 +70,21 @@ def test_noalloc_reduction_matches_domain_reduction_two_calls_in_a_row():
         dom2.close()
 
 
+def test_noalloc_reduction_strides_over_fields_larger_than_its_grid():
+    # 96 x 64 x 64 = 393,216 nodes: more than the 592 blocks x 256 threads
+    # (151,552) the call launches, so every thread loops over several nodes
+    dom, dev = field_pair(mrlbm.D3Q19, 96, 64, 64, 3)
+    try:
+        ref = dom.sums()
+        a = mrlbm.reduce_ref_layout_noalloc(dev.data_ptr(), 96, 64, 64, dom.nm, 1.0)
+        b = mrlbm.reduce_ref_layout_noalloc(dev.data_ptr(), 96, 64, 64, dom.nm, 1.0)
+        equal(a, b)
+        close(a, ref)
+        assert a["fluid_nodes"] == 96 * 64 * 64 and a["nonfinite"] == 0
+    finally:
+        dom.close()
+
+
 def test_noalloc_reduction_rejects_bad_arguments_before_launching():
     import torch
 
