@@ -186,6 +186,12 @@ mrlbm_status mrlbm_synchronize(mrlbm_domain* dom);
  * kernel's duration in *seconds; the context stays usable. */
 mrlbm_status mrlbm_selftest_bounded_wait(unsigned polls, double* seconds);
 mrlbm_status mrlbm_get_step(mrlbm_domain* dom, int* step);
+/* z planes each CTA of the single-domain step marches (0: chosen from the
+ * grid so the last wave of CTAs is full; otherwise 1..nz).  A tuning knob with
+ * no effect on results: every chunk gives bit-identical moments.  The
+ * reference's counterpart is its fixed 8^3 block (src/definitions.h:87-92). */
+mrlbm_status mrlbm_set_z_chunk(mrlbm_domain* dom, int lz);
+mrlbm_status mrlbm_get_z_chunk(mrlbm_domain* dom, int* lz);
 
 /* Launch on a caller's stream (a cudaStream_t of the domain's device; NULL
  * returns to the domain's own stream, so the legacy default stream cannot be

@@ -79,13 +79,23 @@ __host__ __device__ constexpr int box_x_nodes(int esize) { return esize == 4 ? 3
 // TMA ring depth: 4 stages where the ring and the row exchange fit in shared
 // memory (4 measured 1-3 % faster than 3), else 3 (or 2)
 constexpr int NSTAGE_MAX = 4;
-// interior rows per CTA: 16 (18 warps, up to 112 registers a thread) for the
-// bulk-only flag sets, 14 (16 warps, up to 128 registers) for the heavier
-// wall, non-Newtonian and thermal sets
-constexpr int TYI_BULK = 16, TYI_WALL = 14;
+// interior rows per CTA: 8 (two CTAs of 10 warps per SM, up to 102 registers
+// a thread) for the bulk-only flag sets, 14 (one CTA of 16 warps, up to 128
+// registers) for the heavier wall, non-Newtonian and thermal sets
+constexpr int TYI_BULK = 8, TYI_WALL = 14;
 __host__ __device__ constexpr int tile_rows(int flags)
 {
     return (flags & (F_BC | F_POWERLAW | F_BINGHAM | F_THERMAL)) ? TYI_WALL : TYI_BULK;
+}
+// CTAs resident per SM: two for short columns (their per-plane barriers
+// interleave, which measured 2-3 % faster for 8 rows than one CTA of 16), else one
+__host__ __device__ constexpr int ctas_per_sm(int tyi) { return tyi <= 8 ? 2 : 1; }
+// dynamic shared memory a CTA may take: the opt-in per-block limit for one
+// CTA per SM, else an even share of the SM's 228 KB less the 1 KB each
+// block reserves
+__host__ __device__ constexpr size_t smem_budget(int tyi)
+{
+    return ctas_per_sm(tyi) == 1 ? 232448 : 233472 / ctas_per_sm(tyi) - 1024;
 }
 // index of a tile height among the domain's tensor maps and z chunks
 __host__ __device__ constexpr int tile_kind(int tyi) { return tyi == TYI_BULK ? 0 : 1; }
@@ -1155,11 +1165,12 @@ struct ZSmem {
     static constexpr int edge_n = 2 * 2 * NR;
     static constexpr size_t edge_bytes = (size_t)(TH ? 2 : 1) * edge_n * 16;
     static constexpr size_t fixed = 128 + ex_bytes + edge_bytes;
-    static constexpr int NS = fixed + NSTAGE_MAX * stage_max <= 232448         ? NSTAGE_MAX
-                              : fixed + (NSTAGE_MAX - 1) * stage_max <= 232448 ? NSTAGE_MAX - 1
+    static constexpr size_t budget = smem_budget(TYI);
+    static constexpr int NS = fixed + NSTAGE_MAX * stage_max <= budget         ? NSTAGE_MAX
+                              : fixed + (NSTAGE_MAX - 1) * stage_max <= budget ? NSTAGE_MAX - 1
                                                                                : NSTAGE_MAX - 2;
     static constexpr size_t bytes = fixed + NS * stage_max;
-    static_assert(bytes <= 232448, "shared memory over the sm_100 limit");
+    static_assert(bytes <= budget, "shared memory over the sm_100 limit");
     uint64_t* bars;   // the ring's mbarriers, then the CTA's timeout flag (bars + NSTAGE_MAX)
     unsigned char* stages;
     float4* ex4;
@@ -1471,7 +1482,7 @@ __device__ __forceinline__ void zmarch_init_barriers(const ZSmem<Q, T, TYI, NPM,
 // Launch order runs x tiles fastest, so the CTAs resident at one time march
 // neighbouring columns through the same planes and their halo reads hit L2.
 template <int Q, typename T, int FLAGS, int TYI, typename BCP = TableBC>
-__global__ void __launch_bounds__(32 * (TYI + 2), 1)
+__global__ void __launch_bounds__(32 * (TYI + 2), ctas_per_sm(TYI))
     zmarch_step(const __grid_constant__ CUtensorMap map_in, const StepArgs a)
 {
     extern __shared__ __align__(128) unsigned char smem[];

@@ -354,7 +354,8 @@ int mrlbm::choose_lz(const mrlbm_domain* dom, int ty)
     for (int nzc = 1; nzc <= d.nz; nzc++) {
         const int lz = (d.nz + nzc - 1) / nzc;
         const long long ctas = cols * ((d.nz + lz - 1) / lz);
-        const long long waves = (ctas + dom->nsm - 1) / dom->nsm;
+        const long long slots = (long long)dom->nsm * ctas_per_sm(ty);
+        const long long waves = (ctas + slots - 1) / slots;
         const long long cost = waves * (lz + 2 + 3);  // + a CTA start-up of about 3 planes
         if (best_cost < 0 || cost < best_cost) {
             best_cost = cost;
@@ -798,6 +799,28 @@ extern "C" mrlbm_status mrlbm_get_step(mrlbm_domain* dom, int* step)
 {
     if (!dom || !step) return fail(MRLBM_EINVAL, "null argument");
     *step = dom->step;
+    return MRLBM_OK;
+}
+
+extern "C" mrlbm_status mrlbm_set_z_chunk(mrlbm_domain* dom, int lz)
+{
+    if (!dom) return fail(MRLBM_EINVAL, "null argument");
+    if (lz < 0 || lz > dom->d.nz) return fail(MRLBM_EINVAL, "z chunk %d outside 0..%d", lz, dom->d.nz);
+    if (dom->graph_exec) {
+        cudaGraphExecDestroy(dom->graph_exec);  // the captured launches carry the old chunk
+        dom->graph_exec = nullptr;
+    }
+    dom->lz = lz;
+    return MRLBM_OK;
+}
+
+extern "C" mrlbm_status mrlbm_get_z_chunk(mrlbm_domain* dom, int* lz)
+{
+    if (!dom || !lz) return fail(MRLBM_EINVAL, "null argument");
+    StepArgs a;
+    int flags = 0;
+    fill_step_args(dom, a, dom->cur, flags);
+    *lz = a.lz;
     return MRLBM_OK;
 }
 

@@ -16,7 +16,7 @@ static mrlbm_status launch_step_t(const CUtensorMap* maps, const StepArgs& a, cu
     constexpr int NW = TYI + 2;
     const CUtensorMap& map = maps[tile_kind(TYI)];
     constexpr size_t smem = step_smem_bytes<Q, T, FLAGS, TYI>();
-    static_assert(smem <= 232448, "shared memory over the sm_100 limit");
+    static_assert(smem <= smem_budget(TYI), "shared memory over the sm_100 limit");
     auto kern = zmarch_step<Q, T, FLAGS, TYI, BCP>;
     int dev = 0;
     cudaGetDevice(&dev);

@@ -191,6 +191,8 @@ def lib():
                                                      C.POINTER(Sums)],
             "mrlbm_selftest_bounded_wait": [C.c_uint, C.POINTER(C.c_double)],
             "mrlbm_set_stream": [VP, VP],
+            "mrlbm_set_z_chunk": [VP, C.c_int],
+            "mrlbm_get_z_chunk": [VP, C.POINTER(C.c_int)],
             "mrlbm_get_stream": [VP, C.POINTER(VP)],
             "mrlbm_zslab_plane": [VP, C.c_int, C.POINTER(ZPlane)],
             "mrlbm_zslab_copy": [VP, C.c_int, VP, C.c_int],
@@ -342,6 +344,15 @@ class Domain:
         ms = C.c_float()
         check(self.L.mrlbm_time_steps(self.h, int(n), C.byref(ms)))
         return ms.value
+
+    def set_z_chunk(self, lz):
+        """z planes per CTA of the step (0: automatic); results do not depend on it."""
+        check(self.L.mrlbm_set_z_chunk(self.h, int(lz)))
+
+    def z_chunk(self):
+        v = C.c_int()
+        check(self.L.mrlbm_get_z_chunk(self.h, C.byref(v)))
+        return v.value
 
     def synchronize(self):
         check(self.L.mrlbm_synchronize(self.h))
