@@ -632,8 +632,9 @@ def run_zslab_workload(args):
 
 def run_precision_workload(args):
     """Storage precision study: the Taylor-Green vortex, D3Q27, n^3 (512 by
-    default), Re 1600, u0 0.04, 1000 steps, with the moments stored as FP32,
-    FP16 and BF16 (FP32 arithmetic throughout).  Reports device-timed MLUPS of
+    default), Re 1600 (--precision-re), u0 0.04, 1000 steps, with the moments
+    stored as FP32, FP16, FP16 with split velocity (F16U) and BF16 (FP32
+    arithmetic throughout).  Reports device-timed MLUPS of
     each, and per-moment relative L2 / Linf errors of FP16 / BF16 against FP32
     over the whole field; with --reference (a file written by
     oracle/tgv_reference.py) also every storage against the FP64 oracle on the
@@ -641,9 +642,9 @@ def run_precision_workload(args):
     import mrlbm
 
     mrlbm.set_device(0)
-    n, steps = args.n, args.precision_steps
+    n, steps, re = args.n, args.precision_steps, args.precision_re
     L = n / (2 * np.pi)
-    tau = 0.5 + 3.0 * U0 * L / RE
+    tau = 0.5 + 3.0 * U0 * L / re
     ref = None
     if args.reference:
         ref = np.load(args.reference)
@@ -652,7 +653,8 @@ def run_precision_workload(args):
     planes = [int(p) for p in ref["planes"]] if ref is not None else []
     res = {}
     full32 = None
-    for storage, name in ((mrlbm.F32, "fp32"), (mrlbm.F16, "fp16"), (mrlbm.BF16, "bf16")):
+    words = {mrlbm.F32: (10, 4), mrlbm.F16: (10, 2), mrlbm.F16U: (13, 2), mrlbm.BF16: (10, 2)}
+    for storage, name in ((mrlbm.F32, "fp32"), (mrlbm.F16, "fp16"), (mrlbm.F16U, "fp16u"), (mrlbm.BF16, "bf16")):
         d = mrlbm.make_desc(n, n, n, lattice=27, storage=storage, tau=tau)
         dom = mrlbm.Domain(d)
         dom.init_taylor_green(U0, L)
@@ -665,7 +667,7 @@ def run_precision_workload(args):
             ms = dom.time_steps(steps)
         m = dom.moments()
         r = {"mlups": round(steps * n ** 3 / (ms * 1e-3) / 1e6, 1), "ms": round(ms, 2),
-             "bytes_per_lup": 2 * 10 * (4 if storage == mrlbm.F32 else 2), "clocks": clk.summary()}
+             "bytes_per_lup": 2 * words[storage][0] * words[storage][1], "clocks": clk.summary()}
         if ref is not None:
             o = np.moveaxis(ref["moments"].astype(np.float64), -1, 0)  # [m][planes][y][x]
             e, ue = moment_errors(m[:, planes], o)
@@ -683,10 +685,11 @@ def run_precision_workload(args):
     line = {"metric": "storage precision: MLUPS and error vs FP64 (TGV D3Q27)", "value": res["fp16"]["mlups"],
             "unit": "MLUPS", "n_gpus": 1, "steps": steps, "higher_is_better": True,
             "dtype": "fp16/bf16 storage, f32 arithmetic", "data": "synthetic (analytic Taylor-Green initial field)",
-            "config": {"workload": "taylor_green_%d^3_d3q27_precision" % n, "re": RE, "u0": U0, "tau": tau,
+            "config": {"workload": "taylor_green_%d^3_d3q27_precision" % n, "re": re, "u0": U0, "tau": tau,
                        "reference": ("FP64 oracle, z planes %s" % planes) if ref is not None else None},
             "fp16_over_fp32": round(res["fp16"]["mlups"] / res["fp32"]["mlups"], 3),
             "bf16_over_fp32": round(res["bf16"]["mlups"] / res["fp32"]["mlups"], 3),
+            "fp16u_over_fp32": round(res["fp16u"]["mlups"] / res["fp32"]["mlups"], 3),
             "storages": res}
     print(json.dumps(line), flush=True)
     return 0
@@ -710,6 +713,7 @@ def main():
                     help="tgv workload: velocity set (D3Q27 is the benchmark's; D3Q19 for comparison)")
     ap.add_argument("--n", type=int, default=512, help="precision workload: grid edge")
     ap.add_argument("--precision-steps", type=int, default=1000)
+    ap.add_argument("--precision-re", type=float, default=RE)
     ap.add_argument("--reference", default=None, help="precision workload: FP64 planes from oracle/tgv_reference.py")
     ap.add_argument("--domains", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=5000)

@@ -48,7 +48,14 @@ typedef enum {
 } mrlbm_status;
 
 typedef enum { MRLBM_D3Q19 = 19, MRLBM_D3Q27 = 27 } mrlbm_lattice;
-typedef enum { MRLBM_F32 = 0, MRLBM_F16 = 1, MRLBM_BF16 = 2 } mrlbm_storage;
+/* Stored precision of the moments (arithmetic is FP32 in every case).
+ * MRLBM_F16U ("split velocity"): rho - rho0 and the second moments in fp16,
+ * each component of 3u in two fp16 words (the high word and what it rounds
+ * away), 26 bytes a node instead of 20 (fp16) or 40 (fp32): velocity keeps
+ * about 22 significant bits, which plain 16-bit storage loses step by step
+ * at low viscosity.  Not with the thermal scalar or outflow walls.  No
+ * reference counterpart (its dfloat is float or double, src/var.h:13-21). */
+typedef enum { MRLBM_F32 = 0, MRLBM_F16 = 1, MRLBM_BF16 = 2, MRLBM_F16U = 3 } mrlbm_storage;
 typedef enum { MRLBM_NEWTONIAN = 0, MRLBM_POWERLAW = 1, MRLBM_BINGHAM = 2 } mrlbm_rheology;
 
 /* Node-type words follow the reference's nodeTypeMap (src/nodeTypeMap.h:10-80):
@@ -394,6 +401,11 @@ mrlbm_status mrlbm_server_keep_results(mrlbm_server* srv, int on);
  * its batch member (description, node types, initial state): for solving a
  * request alone with the single-domain calls. */
 mrlbm_status mrlbm_request_domain(const mrlbm_request* req, int storage, mrlbm_domain** out);
+/* What a request expands to, on the host only (no device work): its domain
+ * description and, when node_types is not NULL, its n^3 node-type words
+ * (x-fastest), as the server builds them.  No reference counterpart (a
+ * reference case fixes both at compile time). */
+mrlbm_status mrlbm_request_describe(const mrlbm_request* req, int storage, mrlbm_desc* desc, uint32_t* node_types);
 
 /* Host-side node-type builders (no device work).
  * Voxel geometry: solid (x-fastest, nonzero = solid) -> nodeTypeMap words: solid

@@ -48,8 +48,16 @@ struct InitArgs {
     float tg_u0, tg_L;
     int thermal;  // moments 10..13 are C and its flux: C = c0, no flux
     float c0;     // (the thermal cases' flow_initialization.inc: cVar = T_REFERENCE, q = 0)
+    int lo0;      // split velocity: stored word of the low part of 3u_x (-1: none)
     float scale[NM_MAX];
 };
+
+// Split velocity: the part of 3u that its fp16 high word (storage scale s)
+// rounds away, stored in the low word.
+__device__ __forceinline__ float split_low(float u3, float s)
+{
+    return u3 - __half2float(__float2half_rn(u3 * s)) / s;
+}
 
 template <int Q, typename T>
 __global__ void init_kernel(const InitArgs a)
@@ -82,6 +90,8 @@ __global__ void init_kernel(const InitArgs a)
         } else {
             m[10] = a.omega0;
         }
+        if (a.lo0 >= 0)
+            for (int c = 0; c < 3; c++) m[a.lo0 + c] = split_low(m[1 + c], a.scale[1 + c]);
         const long long idx = pidx(x, y, z, a.pitch, a.plane);
         T* p0 = reinterpret_cast<T*>(a.m0);
         T* p1 = reinterpret_cast<T*>(a.m1);
@@ -103,6 +113,7 @@ struct ConvArgs {
     int nx, ny, nz, pitch;
     long long plane, field;
     int nm, mode;
+    int lo0;  // split velocity: stored word of the low part of 3u_x (-1: none)
     float scale[NM_MAX], iscale[NM_MAX];
 };
 
@@ -127,13 +138,23 @@ __global__ void convert_kernel(const ConvArgs a)
             const long long blk = (x >> 3) + (long long)nbx * ((y >> 3) + (long long)nby * (z >> 3));
             fi = (x & 7) + 8 * ((y & 7) + 8 * ((z & 7) + 8 * (k + (long long)a.nm * blk)));
         }
+        // split velocity: 3u = high word + low word (stored word lo0 + k - 1)
+        const bool split = a.lo0 >= 0 && k >= 1 && k <= 3;
+        const long long lidx = split ? mphys(a.lo0 + k - 1, pidx(x, y, z, a.pitch, a.plane), a.field) : 0;
         if (a.mode == 0 || a.mode == 2) {
             const float v = Stor<T>::ld(reinterpret_cast<const T*>(a.m0) + idx);
-            a.f[fi] = is_f32<T>() ? v : v * a.iscale[k];
+            float r = is_f32<T>() ? v : v * a.iscale[k];
+            if (split) r += Stor<T>::ld(reinterpret_cast<const T*>(a.m0) + lidx) * a.iscale[a.lo0 + k - 1];
+            a.f[fi] = r;
         } else {
             const float v = is_f32<T>() ? a.f[fi] : a.f[fi] * a.scale[k];
             Stor<T>::st(reinterpret_cast<T*>(a.m0) + idx, v);
             Stor<T>::st(reinterpret_cast<T*>(a.m1) + idx, v);
+            if (split) {
+                const float lo = split_low(a.f[fi], a.scale[k]) * a.scale[a.lo0 + k - 1];
+                Stor<T>::st(reinterpret_cast<T*>(a.m0) + lidx, lo);
+                Stor<T>::st(reinterpret_cast<T*>(a.m1) + lidx, lo);
+            }
         }
     }
 }
@@ -201,6 +222,7 @@ struct RedArgs {
     int nx, ny, nz, pitch;
     long long plane, field;
     int nm;
+    int lo0;  // split velocity: stored word of the low part of 3u_x (-1: none)
     float rho0;
     float iscale[NM_MAX];
     double* partial;
@@ -229,6 +251,7 @@ __global__ void __launch_bounds__(RED_THREADS) reduce_kernel(const RedArgs a)
         for (int k = 0; k < 4; k++) {
             const float s = Stor<T>::ld(mp + mphys(k, idx, a.field));
             v[k] = is_f32<T>() ? s : s * a.iscale[k];
+            if (k >= 1 && a.lo0 >= 0) v[k] += Stor<T>::ld(mp + mphys(a.lo0 + k - 1, idx, a.field)) * a.iscale[a.lo0 + k - 1];
             finite = finite && isfinite(v[k]);
         }
         const double rho = (double)a.rho0 + (double)v[0];

@@ -45,7 +45,7 @@ namespace {
 template <int Q, typename T>
 mrlbm_status set_attr(size_t& smem)
 {
-    smem = ZSmem<Q, T, batch_tyi(Q), 6>::bytes;
+    smem = ZSmem<Q, T, batch_tyi(Q), batch_npm<T>()>::bytes;
     cudaError_t e = cudaFuncSetAttribute(batch_step<Q, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return fail(MRLBM_ECUDA, "batch attribute: %s", cudaGetErrorString(e));
     return MRLBM_OK;
@@ -96,6 +96,7 @@ int batch_flags(const mrlbm_domain* dom)
 
 bool flags_supported(int f)
 {
+    f &= ~F_SPLITU;  // every set below also with split-velocity storage
     return f == 0 || f == F_BC || f == (F_BC | F_FORCE) || f == (F_BC | F_FORCE | F_POWERLAW);
 }
 
@@ -227,8 +228,8 @@ extern "C" mrlbm_status mrlbm_batch_create(int lattice, int storage, mrlbm_batch
     if (!out) return fail(MRLBM_EINVAL, "null output handle");
     *out = nullptr;
     if (lattice != 19 && lattice != 27) return fail(MRLBM_EINVAL, "lattice must be 19 or 27");
-    if (storage != MRLBM_F32 && storage != MRLBM_F16)
-        return fail(MRLBM_EINVAL, "batches store moments in fp32 or fp16");
+    if (storage != MRLBM_F32 && storage != MRLBM_F16 && storage != MRLBM_F16U)
+        return fail(MRLBM_EINVAL, "batches store moments in fp32, fp16 or fp16 with split velocity");
     mrlbm_batch* b = new mrlbm_batch();
     b->lattice = lattice;
     b->storage = storage;

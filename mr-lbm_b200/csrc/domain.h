@@ -25,6 +25,7 @@ constexpr int GRAPH_STEPS = 16;  // launches per captured graph (even: parities 
 struct mrlbm_domain {
     mrlbm_desc d{};
     int q = 19, nm = 10;
+    int nms = 10;                    // stored words per node: nm, + 3 low words of 3u with split-velocity storage
     size_t esize = 4;
     int pitch = 0;
     long long plane = 0, field = 0;
@@ -66,7 +67,9 @@ mrlbm_status build_bc_class(int q, int mq, uint32_t word, const double uvel[4][3
 mrlbm_status classify_nodes(int q, int mq, const uint32_t* nt, long long n, const double uvel[4][3], double omega0,
                             std::vector<uint8_t>& cls, std::vector<BcClass>& table, bool& any_bc,
                             bool case_mode = false, const double* t_wall = nullptr);
-void storage_scales(int storage, float* scale, float* iscale);
+void storage_scales(int storage, int nm, float* scale, float* iscale);
+// storages kept as fp16 words (plain, or with split velocity)
+inline bool is_half_storage(int storage) { return storage == MRLBM_F16 || storage == MRLBM_F16U; }
 mrlbm_status domain_alloc(mrlbm_domain* dom);
 int choose_lz(const mrlbm_domain* dom, int tyi);
 void fill_step_args(const mrlbm_domain* dom, StepArgs& a, int parity, int& flags);

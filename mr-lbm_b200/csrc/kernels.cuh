@@ -58,6 +58,7 @@ enum : int {
     F_BINGHAM = 8,   // omega field, Bingham viscosity
     F_THERMAL = 16,  // thermal scalar C on D3G19 (4 more stored moments, Boussinesq force)
     F_OUTFLOW = 32,  // some wall class is an outflow (selects the OutflowBC policy at launch)
+    F_SPLITU = 64,   // 16-bit storage with each velocity component split in a high and a low word
 };
 
 // most stored moments per node: 10 flow moments + omega, or + C and its flux
@@ -794,8 +795,10 @@ __device__ __forceinline__ void gather_pops(float* g, const float4* e4t, const f
 }
 
 // a node's stored moments (unscaled to the FP32 stored form) from its element
-// pair of moments 0, 1 in a TMA stage (pair p is 2 box_x<T>() elements further)
-template <int NM, typename T>
+// pair of moments 0, 1 in a TMA stage (pair p is 2 box_x<T>() elements further);
+// with split velocity (SPLIT) the last three stored words are the low parts
+// of 3u, added to the high parts in moments 1-3
+template <int NM, typename T, bool SPLIT = false>
 __device__ __forceinline__ void stage_moments(const StepArgs& a, const T* sp, float* mc)
 {
 #pragma unroll
@@ -803,6 +806,24 @@ __device__ __forceinline__ void stage_moments(const StepArgs& a, const T* sp, fl
         const float2 v = Stor2<T>::lds(sp + p * 2 * box_x<T>());
         mc[2 * p] = scaled_storage<T>() ? v.x * a.iscale[2 * p] : v.x;
         if (2 * p + 1 < NM) mc[2 * p + 1] = scaled_storage<T>() ? v.y * a.iscale[2 * p + 1] : v.y;
+    }
+    if constexpr (SPLIT) {
+        mc[1] += mc[NM - 3];
+        mc[2] += mc[NM - 2];
+        mc[3] += mc[NM - 1];
+    }
+}
+
+// split velocity: the low words (moments NM-3 .. NM-1, FP32 before the
+// storage scaling) hold what the 16-bit high word of 3u (moments 1-3, stored
+// with scale[1..3]) rounds away
+template <int NM>
+__device__ __forceinline__ void split_velocity(const StepArgs& a, float* o)
+{
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const float hi = __half2float(__float2half_rn(o[1 + c] * a.scale[1 + c])) * a.iscale[1 + c];
+        o[NM - 3 + c] = o[1 + c] - hi;
     }
 }
 
@@ -834,13 +855,13 @@ __device__ __forceinline__ void thermal_pops(const StepArgs& a, const float* mc,
 // 31 take their inward c_x members from the edge buffer then).
 // sp: this thread's element pair of moments 0, 1 in the plane's TMA stage;
 // e4t / e1t: this thread's exchange slots in the buffer this production writes.
-template <int Q, int NM, typename T, int TYI, bool TH = false>
+template <int Q, int NM, typename T, int TYI, bool TH = false, bool SPLIT = false>
 __device__ __forceinline__ void prod_a(const StepArgs& a, const T* sp, float4* e4t, float* e1t, float (&gsh)[Q],
                                        float& om_node, float4* e4g = nullptr, float* e1g = nullptr,
                                        float* gshg = nullptr)
 {
     float mc[NM];
-    stage_moments<NM, T>(a, sp, mc);
+    stage_moments<NM, T, SPLIT>(a, sp, mc);
     float f[Q];
     reconstruct<Q>(mc, a.rho0, f);
     ex_write_all<Q, TYI>(f, e4t, e1t);
@@ -852,7 +873,7 @@ __device__ __forceinline__ void prod_a(const StepArgs& a, const T* sp, float4* e
             else gsh[i] = f[i];
         }
     });
-    om_node = mc[NM - 1];
+    om_node = mc[(SPLIT ? NM - 3 : NM) - 1];   // omega (moment 10) when the viscosity is per node
     if constexpr (TH) {
         float g[19];
         thermal_pops(a, mc, g);
@@ -877,7 +898,7 @@ __device__ __forceinline__ void prod_a(const StepArgs& a, const T* sp, float4* e
 // hp / ep: the halo-row and edge node's element pair of moments 0, 1 in the
 // stage; e4h / e1h and e4e / e1e: their exchange slots; edge: the edge buffer
 // of this side and parity (one float4 per exchange row).
-template <int Q, int NM, typename T, int TYI, int SIDE, bool TH = false>
+template <int Q, int NM, typename T, int TYI, int SIDE, bool TH = false, bool SPLIT = false>
 __device__ __forceinline__ void prod_helper(const StepArgs& a, int lane, const T* hp, const T* ep, float4* e4h,
                                             float* e1h, float4* e4e, float* e1e, float4* edge, float4* e4hg = nullptr,
                                             float* e1hg = nullptr, float4* e4eg = nullptr, float* e1eg = nullptr,
@@ -885,7 +906,7 @@ __device__ __forceinline__ void prod_helper(const StepArgs& a, int lane, const T
 {
     {
         float mc[NM], f[Q];
-        stage_moments<NM, T>(a, hp, mc);
+        stage_moments<NM, T, SPLIT>(a, hp, mc);
         reconstruct<Q>(mc, a.rho0, f);
         ex_write_sel<Q, TYI, 0, -SIDE>(f, e4h, e1h);
         if constexpr (TH) {
@@ -896,7 +917,7 @@ __device__ __forceinline__ void prod_helper(const StepArgs& a, int lane, const T
     }
     if (lane < TYI + 2) {
         float mc[NM], f[Q];
-        stage_moments<NM, T>(a, ep, mc);
+        stage_moments<NM, T, SPLIT>(a, ep, mc);
         reconstruct<Q>(mc, a.rho0, f);
         ex_write_sel<Q, TYI, -SIDE, 0>(f, e4e, e1e);
         edge[lane] = edge_pops<Q, -SIDE>(f);
@@ -1090,6 +1111,7 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
             o[10] = tC;
             o[11] = tq[0]; o[12] = tq[1]; o[13] = tq[2];
         }
+        if constexpr ((FLAGS & F_SPLITU) != 0) split_velocity<NM>(a, o);
         if constexpr (scaled_storage<T>()) {
 #pragma unroll
             for (int m = 0; m < NM; m++) o[m] = o[m] * a.scale[m];
@@ -1195,7 +1217,8 @@ struct ZSmem {
 // stored moments and moment pairs of a flag set
 __host__ __device__ constexpr int nmoments_of(int flags)
 {
-    return ((flags & (F_POWERLAW | F_BINGHAM)) ? 11 : 10) + ((flags & F_THERMAL) ? 4 : 0);
+    return ((flags & (F_POWERLAW | F_BINGHAM)) ? 11 : 10) + ((flags & F_THERMAL) ? 4 : 0) +
+           ((flags & F_SPLITU) ? 3 : 0);
 }
 __host__ __device__ constexpr int npairs_of(int flags) { return (nmoments_of(flags) + 1) / 2; }
 
@@ -1212,6 +1235,7 @@ struct ZMarch {
     static constexpr int NMID = lat_num_cz(Q, 0);
     static constexpr bool OMF = (FLAGS & (F_POWERLAW | F_BINGHAM)) != 0;
     static constexpr bool TH = (FLAGS & F_THERMAL) != 0;
+    static constexpr bool SPLIT = (FLAGS & F_SPLITU) != 0;
     static constexpr int NM = nmoments_of(FLAGS);
     static constexpr int NP = (NM + 1) / 2;  // moment pairs in a stage row
     static constexpr int ROW = NP * 2 * BX;  // elements of a stage row
@@ -1307,10 +1331,10 @@ struct ZMarch {
                 a, j - 1, z0 - 2 + j, it.e4t[PAR ^ 1], it.e1t[PAR ^ 1], it.eet[PAR ^ 1], it.xlo, it.xhi, it.interior,
                 it.x, it.y, gsh_old, up, mid, om_out, it.e4g[PAR ^ 1], it.e1g[PAR ^ 1], it.eetg[PAR ^ 1], sg_old, upg,
                 midg);
-            prod_a<Q, NM, T, TYI, TH>(a, stage_base() + it.toff, it.e4t[PAR], it.e1t[PAR], gsh_new, om_par,
+            prod_a<Q, NM, T, TYI, TH, SPLIT>(a, stage_base() + it.toff, it.e4t[PAR], it.e1t[PAR], gsh_new, om_par,
                                       it.e4g[PAR], it.e1g[PAR], sg_new);
         } else {
-            prod_a<Q, NM, T, TYI, TH>(a, stage_base() + it.toff, it.e4t[PAR], it.e1t[PAR], gsh_new, om_par,
+            prod_a<Q, NM, T, TYI, TH, SPLIT>(a, stage_base() + it.toff, it.e4t[PAR], it.e1t[PAR], gsh_new, om_par,
                                       it.e4g[PAR], it.e1g[PAR], sg_new);
             prod_b<Q, NM, NUP, NMID, T, FLAGS, TYI, BCP, LIGHT>(
                 a, j - 1, z0 - 2 + j, it.e4t[PAR ^ 1], it.e1t[PAR ^ 1], it.eet[PAR ^ 1], it.xlo, it.xhi, it.interior,
@@ -1358,7 +1382,7 @@ struct ZMarch {
         {
             // prologue: production 0 only (exchange buffer 0)
             const bool ok = mbar_wait(&sm.bars[cs], cph);
-            prod_a<Q, NM, T, TYI, TH>(a, stage_base() + it.toff, it.e4t[0], it.e1t[0], gA, omA, it.e4g[0], it.e1g[0],
+            prod_a<Q, NM, T, TYI, TH, SPLIT>(a, stage_base() + it.toff, it.e4t[0], it.e1t[0], gA, omA, it.e4g[0], it.e1g[0],
                                       sgA);
             if (!end_step(0, ok)) return 0;
         }
@@ -1415,7 +1439,7 @@ struct ZMarch {
             float* e1 = sm.ex1 + par * EX::buf1;
             float4* g4 = sm.exg4 + par * EXG::buf4;
             float* g1 = sm.exg1 + par * EXG::buf1;
-            prod_helper<Q, NM, T, TYI, SIDE, TH>(a, lane, st + hoff, st + eoff, e4 + sh, e1 + sh, e4 + se, e1 + se,
+            prod_helper<Q, NM, T, TYI, SIDE, TH, SPLIT>(a, lane, st + hoff, st + eoff, e4 + sh, e1 + sh, e4 + se, e1 + se,
                                                  sm.edge + (side * 2 + par) * NR, g4 + sh, g1 + sh, g4 + se, g1 + se,
                                                  sm.edgeg + (side * 2 + par) * NR);
             if (!end_step(j, ok)) return j;

@@ -194,10 +194,14 @@ mrlbm_status mrlbm::build_bc_class(int q, int mq, uint32_t word, const double uv
 
 // ------------------------------------------------------------ domain setup
 
+// moments a node carries (the reference's NUMBER_MOMENTS for the case) and
+// the words it stores: with split-velocity storage three more, the low
+// parts of 3u
 static int moments_of(const mrlbm_desc& d)
 {
     return (d.rheology != MRLBM_NEWTONIAN ? 11 : 10) + (d.thermal ? 4 : 0);
 }
+static int stored_moments_of(const mrlbm_desc& d) { return moments_of(d) + (d.storage == MRLBM_F16U ? 3 : 0); }
 
 // G_DIFF_FLUC_COEF from the thermal diffusivity with the reference's fixed
 // T_DIFF_REF = 1/6 and G_TAU = 3 T_DIFF_REF + 1/2
@@ -211,15 +215,20 @@ static double thermal_coef(double alpha)
 
 static size_t elem_size(int storage) { return storage == MRLBM_F32 ? 4 : 2; }
 
-void mrlbm::storage_scales(int storage, float* scale, float* iscale)
+void mrlbm::storage_scales(int storage, int nm, float* scale, float* iscale)
 {
     for (int k = 0; k < NM_MAX; k++) {
         float s = 1.0f;
-        if (storage == MRLBM_F16) {
+        if (is_half_storage(storage)) {
             // powers of two keep values of the shifted moments in the normal
             // range of fp16 (exact, no rounding from the scaling itself);
             // bf16 has fp32's exponent range and needs none
             s = k == 0 ? 256.0f : (k <= 3 ? 8.0f : (k <= 9 ? 64.0f : 1.0f));
+            // split velocity: the low words of 3u (stored after the nm
+            // moments) are what the high word rounds away, at most half an
+            // fp16 ulp of 8 * 3u, so 2^11 times the high word's scale keeps
+            // them in fp16's normal range
+            if (storage == MRLBM_F16U && k >= nm && k < nm + 3) s = 8.0f * 2048.0f;
         }
         scale[k] = s;
         iscale[k] = 1.0f / s;
@@ -232,7 +241,7 @@ static mrlbm_status validate(const mrlbm_desc* d)
     if (d->nx < 1 || d->ny < 1 || d->nz < 1 || d->nx > 8192 || d->ny > 8192 || d->nz > 8192)
         return fail(MRLBM_EINVAL, "bad grid %dx%dx%d", d->nx, d->ny, d->nz);
     if (d->lattice != 19 && d->lattice != 27) return fail(MRLBM_EINVAL, "lattice must be 19 or 27");
-    if (d->storage < 0 || d->storage > 2) return fail(MRLBM_EINVAL, "bad storage %d", d->storage);
+    if (d->storage < 0 || d->storage > 3) return fail(MRLBM_EINVAL, "bad storage %d", d->storage);
     if (!(d->tau > 0.5)) return fail(MRLBM_EINVAL, "tau must be > 0.5 (got %g)", d->tau);
     if (d->rheology < 0 || d->rheology > 2) return fail(MRLBM_EINVAL, "bad rheology");
     if (d->bc_matrix_q != 0 && d->bc_matrix_q != 19 && d->bc_matrix_q != d->lattice)
@@ -253,6 +262,7 @@ static mrlbm_status validate(const mrlbm_desc* d)
         // D3Q19 Newtonian
         if (d->lattice != 19 || d->storage != MRLBM_F32 || d->rheology != MRLBM_NEWTONIAN)
             return fail(MRLBM_EINVAL, "the thermal scalar needs D3Q19, FP32 storage and a Newtonian fluid");
+        if (d->storage == MRLBM_F16U) return fail(MRLBM_EINVAL, "split-velocity storage has no thermal scalar");
         if (!(d->t_diffusivity > 0.0) || !std::isfinite(thermal_coef(d->t_diffusivity)))
             return fail(MRLBM_EINVAL, "bad thermal diffusivity %g", d->t_diffusivity);
     }
@@ -266,7 +276,7 @@ extern "C" mrlbm_status mrlbm_domain_bytes(const mrlbm_desc* d, size_t* bytes)
     const size_t pitch = (size_t)((d->nx + XOFF + 1 + 7) / 8 * 8);
     const size_t field = pitch * (d->ny + 2) * (d->nz + 2);
     // two buffers of moment pairs (an odd count is padded to the next pair), node classes
-    *bytes = 2 * field * (2 * ((moments_of(*d) + 1) / 2)) * elem_size(d->storage) + field;
+    *bytes = 2 * field * (2 * ((stored_moments_of(*d) + 1) / 2)) * elem_size(d->storage) + field;
     return MRLBM_OK;
 }
 
@@ -275,6 +285,7 @@ mrlbm_status mrlbm::domain_alloc(mrlbm_domain* dom)
     const mrlbm_desc& d = dom->d;
     dom->q = d.lattice;
     dom->nm = moments_of(d);
+    dom->nms = stored_moments_of(d);
     dom->esize = elem_size(d.storage);
     dom->pitch = (d.nx + XOFF + 1 + 7) / 8 * 8;
     dom->plane = (long long)dom->pitch * (d.ny + 2);
@@ -285,9 +296,9 @@ mrlbm_status mrlbm::domain_alloc(mrlbm_domain* dom)
         return fail(MRLBM_EINVAL, "domain %d x %d x %d: %lld padded nodes per moment, the limit is 2^32", d.nx, d.ny,
                     d.nz, dom->field);
     dom->omega0 = 1.0 / d.tau;
-    storage_scales(d.storage, dom->scale, dom->iscale);
+    storage_scales(d.storage, dom->nm, dom->scale, dom->iscale);
     // moment pairs: moments 2p and 2p + 1 interleaved per node (an odd count is padded)
-    const size_t mbytes = (size_t)dom->field * (2 * ((dom->nm + 1) / 2)) * dom->esize;
+    const size_t mbytes = (size_t)dom->field * (2 * ((dom->nms + 1) / 2)) * dom->esize;
     CK(cudaMalloc(&dom->m[0], mbytes));
     CK(cudaMalloc(&dom->m[1], mbytes));
     CK(cudaMemset(dom->m[0], 0, mbytes));
@@ -310,6 +321,8 @@ mrlbm_status mrlbm::domain_alloc(mrlbm_domain* dom)
         // thermal: exterior C at the reference temperature, no flux
         if (d.thermal) ext[10] = (float)d.t_reference;
         else ext[10] = (float)dom->omega0;
+        // split velocity: the exterior is at rest, its low words are zero
+        for (int k = dom->nm; k < dom->nms; k++) ext[k] = 0.f;
     }
     memcpy(dom->ext, ext, sizeof(ext));
     CK(cudaStreamCreateWithFlags(&dom->stream, cudaStreamNonBlocking));
@@ -537,7 +550,7 @@ static void launch_init(mrlbm_domain* dom, InitArgs& a)
     int blocks = (int)std::min<long long>((n + threads - 1) / threads, 148LL * 32);
     if (dom->d.storage == MRLBM_F32)
         init_kernel<Q, float><<<blocks, threads, 0, dom->stream>>>(a);
-    else if (dom->d.storage == MRLBM_F16)
+    else if (is_half_storage(dom->d.storage))
         init_kernel<Q, __half><<<blocks, threads, 0, dom->stream>>>(a);
     else
         init_kernel<Q, __nv_bfloat16><<<blocks, threads, 0, dom->stream>>>(a);
@@ -550,7 +563,8 @@ static mrlbm_status run_init(mrlbm_domain* dom, InitArgs& a)
     a.m1 = dom->m[1];
     a.nx = d.nx; a.ny = d.ny; a.nz = d.nz; a.pitch = dom->pitch;
     a.plane = dom->plane; a.field = dom->field;
-    a.nm = dom->nm;
+    a.nm = dom->nms;
+    a.lo0 = dom->nms > dom->nm ? dom->nm : -1;
     a.qs = 19;  // the reference's D3Q19 second-moment sums (also on D3Q27)
     a.rho0 = (float)d.rho0;
     a.omega0 = (float)dom->omega0;
@@ -618,7 +632,7 @@ void mrlbm::fill_step_args(const mrlbm_domain* dom, StepArgs& a, int parity, int
     a.m_in = dom->m[parity];
     a.storage = d.storage;
     for (int p = 0; p < (NM_MAX + 1) / 2; p++)
-        a.out_p[p] = 2 * p < dom->nm ? static_cast<char*>(dom->m[parity ^ 1]) + (size_t)p * 2 * dom->field * dom->esize
+        a.out_p[p] = 2 * p < dom->nms ? static_cast<char*>(dom->m[parity ^ 1]) + (size_t)p * 2 * dom->field * dom->esize
                                      : nullptr;
     a.err = dom->err;
     a.cls = dom->cls;
@@ -646,6 +660,7 @@ void mrlbm::fill_step_args(const mrlbm_domain* dom, StepArgs& a, int parity, int
     if (flags & (F_POWERLAW | F_BINGHAM)) flags |= F_BC;  // nnf variants always read the class map
     if (d.thermal) flags |= F_THERMAL | F_FORCE;           // the Boussinesq force is per node
     if (dom->has_outflow) flags |= F_OUTFLOW;
+    if (d.storage == MRLBM_F16U) flags |= F_SPLITU;
     a.lz = dom->lz > 0 ? dom->lz : dom->lz_t[tile_kind(tile_rows(flags))];
 }
 
@@ -660,11 +675,11 @@ mrlbm_status mrlbm::enqueue_step(mrlbm_domain* dom, int parity, cudaStream_t s)
     const CUtensorMap* maps = dom->tmap[parity];
     if (q == 19) {
         if (stg == MRLBM_F32) st = dispatch_step<19, float>(maps, a, flags, s);
-        else if (stg == MRLBM_F16) st = dispatch_step<19, __half>(maps, a, flags, s);
+        else if (is_half_storage(stg)) st = dispatch_step<19, __half>(maps, a, flags, s);
         else st = dispatch_step<19, __nv_bfloat16>(maps, a, flags, s);
     } else {
         if (stg == MRLBM_F32) st = dispatch_step<27, float>(maps, a, flags, s);
-        else if (stg == MRLBM_F16) st = dispatch_step<27, __half>(maps, a, flags, s);
+        else if (is_half_storage(stg)) st = dispatch_step<27, __half>(maps, a, flags, s);
         else st = dispatch_step<27, __nv_bfloat16>(maps, a, flags, s);
     }
     return st;
@@ -843,13 +858,14 @@ static mrlbm_status convert(mrlbm_domain* dom, float* hbuf_out, const float* hbu
     a.nx = d.nx; a.ny = d.ny; a.nz = d.nz; a.pitch = dom->pitch;
     a.plane = dom->plane; a.field = dom->field;
     a.nm = dom->nm;
+    a.lo0 = dom->nms > dom->nm ? dom->nm : -1;
     a.mode = mode;
     memcpy(a.scale, dom->scale, sizeof(a.scale));
     memcpy(a.iscale, dom->iscale, sizeof(a.iscale));
     const int threads = 256;
     const int blocks = (int)std::min<size_t>((n + threads - 1) / threads, 148 * 64);
     if (d.storage == MRLBM_F32) convert_kernel<float><<<blocks, threads, 0, dom->stream>>>(a);
-    else if (d.storage == MRLBM_F16) convert_kernel<__half><<<blocks, threads, 0, dom->stream>>>(a);
+    else if (is_half_storage(d.storage)) convert_kernel<__half><<<blocks, threads, 0, dom->stream>>>(a);
     else convert_kernel<__nv_bfloat16><<<blocks, threads, 0, dom->stream>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess && (mode == 0 || mode == 2))
@@ -942,12 +958,12 @@ mrlbm_status mrlbm::make_tensor_maps(mrlbm_domain* dom)
     if (!enc) return fail(MRLBM_ECUDA, "cuTensorMapEncodeTiled unavailable");
     const mrlbm_desc& d = dom->d;
     const CUtensorMapDataType dt = d.storage == MRLBM_F32   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
-                                   : d.storage == MRLBM_F16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                   : is_half_storage(d.storage) ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
                                                             : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
     const cuuint64_t es = dom->esize;
     // x runs over the interleaved pair elements (2 per node), the second
     // dimension over moment pairs
-    const cuuint32_t npairs = (cuuint32_t)((dom->nm + 1) / 2);
+    const cuuint32_t npairs = (cuuint32_t)((dom->nms + 1) / 2);
     const cuuint64_t dims[4] = {(cuuint64_t)(2 * dom->pitch), npairs, (cuuint64_t)(d.ny + 2), (cuuint64_t)(d.nz + 2)};
     const cuuint64_t strides[3] = {(cuuint64_t)(2 * dom->field) * es, (cuuint64_t)(2 * dom->pitch) * es,
                                    (cuuint64_t)(2 * dom->plane) * es};
@@ -973,7 +989,7 @@ mrlbm_status mrlbm::fill_ghosts(mrlbm_domain* dom)
     g.m1 = dom->m[1];
     g.nx = d.nx; g.ny = d.ny; g.nz = d.nz; g.pitch = dom->pitch;
     g.plane = dom->plane; g.field = dom->field;
-    g.nm = dom->nm;
+    g.nm = dom->nms;
     g.periodic = (d.periodic[0] ? 1 : 0) | (d.periodic[1] ? 2 : 0) | (d.periodic[2] ? 4 : 0);
     memcpy(g.ext, dom->ext, sizeof(g.ext));
     memcpy(g.scale, dom->scale, sizeof(g.scale));
@@ -986,7 +1002,7 @@ mrlbm_status mrlbm::fill_ghosts(mrlbm_domain* dom)
         g.m1 = dom->m[0];
     }
     if (d.storage == MRLBM_F32) ghost_fill_kernel<float><<<blocks, threads, 0, dom->stream>>>(g);
-    else if (d.storage == MRLBM_F16) ghost_fill_kernel<__half><<<blocks, threads, 0, dom->stream>>>(g);
+    else if (is_half_storage(d.storage)) ghost_fill_kernel<__half><<<blocks, threads, 0, dom->stream>>>(g);
     else ghost_fill_kernel<__nv_bfloat16><<<blocks, threads, 0, dom->stream>>>(g);
     CK(cudaGetLastError());
     return MRLBM_OK;
@@ -1005,6 +1021,7 @@ mrlbm_status mrlbm::enqueue_reduce(mrlbm_domain* dom, double* partial, double* o
     a.nx = d.nx; a.ny = d.ny; a.nz = d.nz; a.pitch = dom->pitch;
     a.plane = dom->plane; a.field = dom->field;
     a.nm = dom->nm;
+    a.lo0 = dom->nms > dom->nm ? dom->nm : -1;
     a.rho0 = (float)d.rho0;
     memcpy(a.iscale, dom->iscale, sizeof(a.iscale));
     a.partial = partial;
@@ -1013,7 +1030,7 @@ mrlbm_status mrlbm::enqueue_reduce(mrlbm_domain* dom, double* partial, double* o
     a.usnap = dom->usnap;
     a.residual_mode = residual_mode;
     if (d.storage == MRLBM_F32) reduce_kernel<float><<<a.nblocks, RED_THREADS, 0, s>>>(a);
-    else if (d.storage == MRLBM_F16) reduce_kernel<__half><<<a.nblocks, RED_THREADS, 0, s>>>(a);
+    else if (is_half_storage(d.storage)) reduce_kernel<__half><<<a.nblocks, RED_THREADS, 0, s>>>(a);
     else reduce_kernel<__nv_bfloat16><<<a.nblocks, RED_THREADS, 0, s>>>(a);
     reduce_finish<<<1, 32, 0, s>>>(partial, a.nblocks, out);
     CK(cudaGetLastError());

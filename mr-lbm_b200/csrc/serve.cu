@@ -99,6 +99,22 @@ static mrlbm_status request_node_types(const mrlbm_request& r, std::vector<uint3
     return mrlbm_voxel_node_types(n, n, n, solid.data(), periodic, nt.data());
 }
 
+extern "C" mrlbm_status mrlbm_request_describe(const mrlbm_request* r, int storage, mrlbm_desc* desc,
+                                              uint32_t* node_types)
+{
+    if (!r || !desc) return fail(MRLBM_EINVAL, "null argument");
+    mrlbm_server tmp;
+    tmp.storage = storage;
+    mrlbm_status st = request_desc(&tmp, *r, desc);
+    if (st) return st;
+    if (node_types) {
+        std::vector<uint32_t> nt;
+        if ((st = request_node_types(*r, nt))) return st;
+        memcpy(node_types, nt.data(), nt.size() * sizeof(uint32_t));
+    }
+    return MRLBM_OK;
+}
+
 // A standalone domain for a request (same description, node types and
 // initial state as the server gives it), e.g. to solve it alone.
 extern "C" mrlbm_status mrlbm_request_domain(const mrlbm_request* r, int storage, mrlbm_domain** out)

@@ -48,6 +48,22 @@ mrlbm_status dispatch_step(const CUtensorMap* maps, const StepArgs& a, int flags
         case F_BC | F_FORCE | F_OUTFLOW: return launch_step_t<Q, T, F_BC | F_FORCE, OutflowBC>(maps, a, s);
         default: break;
     }
+    // split-velocity 16-bit storage (no thermal scalar, no outflow walls)
+    if constexpr (std::is_same<T, __half>::value) {
+        switch (flags) {
+            case F_SPLITU: return launch_step_t<Q, T, F_SPLITU>(maps, a, s);
+            case F_SPLITU | F_BC: return launch_step_t<Q, T, F_SPLITU | F_BC>(maps, a, s);
+            case F_SPLITU | F_FORCE: return launch_step_t<Q, T, F_SPLITU | F_FORCE>(maps, a, s);
+            case F_SPLITU | F_BC | F_FORCE: return launch_step_t<Q, T, F_SPLITU | F_BC | F_FORCE>(maps, a, s);
+            case F_SPLITU | F_BC | F_POWERLAW: return launch_step_t<Q, T, F_SPLITU | F_BC | F_POWERLAW>(maps, a, s);
+            case F_SPLITU | F_BC | F_FORCE | F_POWERLAW:
+                return launch_step_t<Q, T, F_SPLITU | F_BC | F_FORCE | F_POWERLAW>(maps, a, s);
+            case F_SPLITU | F_BC | F_BINGHAM: return launch_step_t<Q, T, F_SPLITU | F_BC | F_BINGHAM>(maps, a, s);
+            case F_SPLITU | F_BC | F_FORCE | F_BINGHAM:
+                return launch_step_t<Q, T, F_SPLITU | F_BC | F_FORCE | F_BINGHAM>(maps, a, s);
+            default: break;
+        }
+    }
     // thermal scalar: D3Q19 with FP32 storage only (its second row exchange
     // fits next to the D3Q19 flow's in shared memory)
     if constexpr (Q == 19 && is_f32<T>()) {

@@ -54,7 +54,7 @@ extern "C" mrlbm_status mrlbm_zslab_plane(mrlbm_domain* dom, int which, mrlbm_zp
     out->base = static_cast<char*>(dom->m[dom->cur]) + zp * dom->plane * 2 * es;
     out->pair_stride = dom->field * 2 * es;
     out->bytes = dom->plane * 2 * es;
-    out->npairs = (dom->nm + 1) / 2;
+    out->npairs = (dom->nms + 1) / 2;
     out->device = dom->device;
     return MRLBM_OK;
 }

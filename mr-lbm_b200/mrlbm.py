@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmrlbm.so")
 
 D3Q19, D3Q27 = 19, 27
-F32, F16, BF16 = 0, 1, 2
+F32, F16, BF16, F16U = 0, 1, 2, 3  # F16U: fp16 with split (two-word) velocity
 NEWTONIAN, POWERLAW, BINGHAM = 0, 1, 2
 
 NODE_BULK = 0x00
@@ -187,6 +187,7 @@ def lib():
             "mrlbm_server_inject_nan": [VP, C.c_int],
             "mrlbm_server_keep_results": [VP, C.c_int],
             "mrlbm_request_domain": [C.POINTER(Request), C.c_int, C.POINTER(VP)],
+            "mrlbm_request_describe": [C.POINTER(Request), C.c_int, C.POINTER(Desc), C.POINTER(C.c_uint32)],
             "mrlbm_reduce_fp64_ref_layout_noalloc": [VP, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, VP,
                                                      C.POINTER(Sums)],
             "mrlbm_selftest_bounded_wait": [C.c_uint, C.POINTER(C.c_double)],
@@ -554,6 +555,14 @@ def request_domain(req, storage=F16):
     nm = C.c_int()
     check(lib().mrlbm_num_moments(h, C.byref(nm)))
     return _Owned(h, req.n, nm.value)
+
+
+def request_describe(req, storage=F16):
+    """(Desc, node types (n, n, n) uint32 z-y-x) that the server builds for `req` (host only)."""
+    d = Desc()
+    nt = np.zeros((req.n, req.n, req.n), dtype=np.uint32)
+    check(lib().mrlbm_request_describe(C.byref(req), storage, C.byref(d), nt.ctypes.data_as(C.POINTER(C.c_uint32))))
+    return d, nt
 
 
 class Server:
