@@ -65,6 +65,9 @@ typedef enum { MRLBM_NEWTONIAN = 0, MRLBM_POWERLAW = 1, MRLBM_BINGHAM = 2 } mrlb
  * mountedCube / externalFlow cases do), bits 11-12 velocity index. */
 #define MRLBM_NODE_BULK 0x00u
 #define MRLBM_NODE_SOLID 0xFFu
+/* a voxel's neighbour whose type is still to be derived (the reference's
+ * MISSING_DEFINITION, src/nodeTypeMap.h) */
+#define MRLBM_NODE_UNRESOLVED 0xFFFFFFFFu
 #define MRLBM_BC_VELOCITY_WALL (1u << 8)
 #define MRLBM_BC_OUTFLOW (2u << 8)
 #define MRLBM_BC_VELOCITY_INDEX(k) (((uint32_t)(k) & 3u) << 11)
@@ -296,6 +299,12 @@ mrlbm_status mrlbm_save_vtk(mrlbm_domain* dom, const char* path_files, const cha
 /* <path>/<id>/<id>_info.txt (src/saveData.cu:469-613); case_name = BC type. */
 mrlbm_status mrlbm_save_info(mrlbm_domain* dom, const char* path_files, const char* id_sim,
                              const char* case_name, int nsteps, double mlups);
+/* The same text for a description alone, on the host (no device work; BY and
+ * BZ are the step geometry of the description without wall classes on a
+ * 148-SM B200): *len receives its length; buf (may be NULL to query) must hold
+ * len + 1 bytes. */
+mrlbm_status mrlbm_info_text(const mrlbm_desc* desc, const char* id_sim, const char* case_name, int nsteps,
+                             double mlups, char* buf, size_t cap, size_t* len);
 
 /* ------------------------------------------------------------------ batches
  * Many independent domains of uneven sizes advanced together by one
@@ -414,6 +423,17 @@ mrlbm_status mrlbm_request_describe(const mrlbm_request* req, int storage, mrlbm
  * define_voxel_bc (src/lbmInitialization.cu:1058-1227). */
 mrlbm_status mrlbm_voxel_node_types(int nx, int ny, int nz, const uint8_t* solid, const int periodic[3],
                                     uint32_t* node_type);
+/* Voxel files of the reference's obstacle cases (VOXEL_FILENAME, read by
+ * read_xyz_file, src/lbmInitialization.cu:978-1039, called at src/main.cuh:
+ * 996-1007): each "x,y,z" line marks that node MRLBM_NODE_SOLID and its 26
+ * neighbours (axes wrapped periodically) MRLBM_NODE_UNRESOLVED unless solid;
+ * lines outside the grid are skipped.  *voxels (may be NULL) receives the
+ * count of solid lines read.  node_types is x-fastest. */
+mrlbm_status mrlbm_voxel_mark_csv(const char* path, int nx, int ny, int nz, uint32_t* node_types, long long* voxels);
+/* The reference's define_voxel_bc / bc_id (src/lbmInitialization.cu:1058-1227):
+ * every MRLBM_NODE_UNRESOLVED node takes the octant mask of its solid
+ * neighbours, axes wrapped periodically (all eight octants is 0xFF, solid). */
+mrlbm_status mrlbm_voxel_resolve(int nx, int ny, int nz, uint32_t* node_types);
 /* The lid-driven cavity typing of src/cases/lidDrivenCavity_3D/bc_initialization.inc:
  * the whole y = ny-1 face (edges and corners included) is the lid, a velocity
  * wall with the given velocity index; other boundary nodes are no-slip walls. */

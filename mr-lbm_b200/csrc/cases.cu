@@ -2,6 +2,8 @@
 // (the reference does this in each case's bc_initialization.inc and, for voxel
 // geometries, in bc_id / define_voxel_bc).
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -101,5 +103,78 @@ extern "C" mrlbm_status mrlbm_bc_class_info(int lattice, int bc_matrix_q, uint32
     out[63] = c.s;
     memcpy(out + 64, c.u, 3 * sizeof(float));
     *known = c.known;
+    return MRLBM_OK;
+}
+
+// The reference's voxel-file loading (read_xyz_file, src/lbmInitialization.cu:
+// 978-1039): every line "x,y,z" of the CSV marks node (x, y, z) solid (0xFF)
+// and its 26 neighbours (each axis wrapped periodically) unresolved
+// (0xFFFFFFFF) unless they are solid already; lines outside the grid are
+// skipped.  node_types is x-fastest and keeps its other values.
+extern "C" mrlbm_status mrlbm_voxel_mark_csv(const char* path, int nx, int ny, int nz, uint32_t* node_types,
+                                             long long* voxels)
+{
+    if (!path || !node_types || nx < 1 || ny < 1 || nz < 1) return fail(MRLBM_EINVAL, "bad argument");
+    FILE* f = fopen(path, "r");
+    if (!f) return fail(MRLBM_EIO, "cannot open voxel file %s", path);
+    long long count = 0;
+    char line[256];
+    auto idx = [&](int x, int y, int z) { return (size_t)x + (size_t)nx * ((size_t)y + (size_t)ny * z); };
+    while (fgets(line, sizeof(line), f)) {
+        char* p = line;
+        char* e = nullptr;
+        long v[3];
+        bool ok = true;
+        for (int k = 0; k < 3 && ok; k++) {
+            v[k] = strtol(p, &e, 10);
+            if (e == p) ok = false;
+            p = e;
+            if (k < 2) {
+                if (*p != ',') ok = false;
+                else p++;
+            }
+        }
+        if (!ok) continue;   // blank or malformed line
+        if (v[0] < 0 || v[1] < 0 || v[2] < 0 || v[0] >= nx || v[1] >= ny || v[2] >= nz) continue;
+        const int x = (int)v[0], y = (int)v[1], z = (int)v[2];
+        const size_t c = idx(x, y, z);
+        node_types[c] = MRLBM_NODE_SOLID;
+        count++;
+        for (int dz = -1; dz <= 1; dz++)
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dx = -1; dx <= 1; dx++) {
+                    const size_t k = idx((x + dx + nx) % nx, (y + dy + ny) % ny, (z + dz + nz) % nz);
+                    if (k == c || node_types[k] == MRLBM_NODE_SOLID) continue;
+                    node_types[k] = MRLBM_NODE_UNRESOLVED;
+                }
+    }
+    fclose(f);
+    if (voxels) *voxels = count;
+    return MRLBM_OK;
+}
+
+// The reference's define_voxel_bc + bc_id (src/lbmInitialization.cu:1058-1227):
+// every unresolved node (0xFFFFFFFF) takes the octant mask of its solid
+// neighbours, each axis wrapped periodically (a mask of all eight octants is
+// the solid word 0xFF, as in the reference).
+extern "C" mrlbm_status mrlbm_voxel_resolve(int nx, int ny, int nz, uint32_t* node_types)
+{
+    if (!node_types || nx < 1 || ny < 1 || nz < 1) return fail(MRLBM_EINVAL, "bad argument");
+    auto idx = [&](int x, int y, int z) { return (size_t)x + (size_t)nx * ((size_t)y + (size_t)ny * z); };
+    for (int z = 0; z < nz; z++)
+        for (int y = 0; y < ny; y++)
+            for (int x = 0; x < nx; x++) {
+                const size_t c = idx(x, y, z);
+                if (node_types[c] != MRLBM_NODE_UNRESOLVED) continue;
+                uint32_t m = 0;
+                for (int dz = -1; dz <= 1; dz++)
+                    for (int dy = -1; dy <= 1; dy++)
+                        for (int dx = -1; dx <= 1; dx++) {
+                            if (!dx && !dy && !dz) continue;
+                            const size_t k = idx((x + dx + nx) % nx, (y + dy + ny) % ny, (z + dz + nz) % nz);
+                            if (node_types[k] == MRLBM_NODE_SOLID) m |= octants_of(dx, dy, dz);
+                        }
+                node_types[c] = m;
+            }
     return MRLBM_OK;
 }

@@ -3,7 +3,9 @@
 #include <sys/stat.h>
 #include <sys/types.h>
 
+#include <algorithm>
 #include <cerrno>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -307,64 +309,94 @@ extern "C" mrlbm_status mrlbm_save_vtk(mrlbm_domain* dom, const char* path_files
 }
 
 // Same keys and number formatting as getSimInfoString (src/saveData.cu:469-613),
-// which the reference's reader parses (post/fileTreat.py:61-150).
+// which the reference's reader parses (post/fileTreat.py:61-150).  by / bz:
+// the step's rows per CTA and z planes per CTA (the reference's BLOCK_NY / NZ).
+static std::string info_text(const mrlbm_desc& d, const char* id_sim, const char* case_name, int nsteps, double mlups,
+                             int by, int bz)
+{
+    std::string t;
+    char line[256];
+    auto put = [&](const char* fmt, auto... v) {
+        snprintf(line, sizeof(line), fmt, v...);
+        t += line;
+    };
+    put("---------------------------- SIMULATION INFORMATION ----------------------------\n");
+    put("      Simulation ID: %s\n", id_sim);
+    put("       Velocity set: D3Q%d\n", d.lattice);
+    put("          Precision: %s\n", d.storage == MRLBM_F32    ? "float"
+                                    : d.storage == MRLBM_F16  ? "half"
+                                    : d.storage == MRLBM_F16U ? "half-split-velocity"
+                                                              : "bfloat16");
+    put("                 NX: %d\n", d.nx);
+    put("                 NY: %d\n", d.ny);
+    put("                 NZ: %d\n", d.nz);
+    put("           NZ_TOTAL: %d\n", d.nz);
+    put("                Tau: %.6e\n", d.tau);
+    double umax = 0.0;
+    for (int k = 0; k < 4; k++)
+        for (int a = 0; a < 3; a++) umax = std::max(umax, std::fabs(d.bc_velocity[k][a]));
+    put("               Umax: %.6e\n", umax);
+    put("                 FX: %.6e\n", d.force[0]);
+    put("                 FY: %.6e\n", d.force[1]);
+    put("                 FZ: %.6e\n", d.force[2]);
+    put("         Save steps: %.6e\n", 0.0);
+    put("             Nsteps: %d\n", nsteps);
+    put("              MLUPS: %.6e\n", mlups);
+    put("                 BX: %d\n", TILE_X);
+    put("                 BY: %d\n", by);
+    put("                 BZ: %d\n", bz);
+    put("--------------------------------------------------------------------------------\n");
+    put("\n------------------------------ BOUNDARY CONDITIONS -----------------------------\n");
+    put("            BC mode: Moment Based \n");
+    put("            BC type: %s\n", case_name ? case_name : "runtime");
+    put("--------------------------------------------------------------------------------\n");
+    if (d.rheology != MRLBM_NEWTONIAN) {
+        put("\n------------------------------ NON NEWTONIAN FLUID -----------------------------\n");
+        if (d.rheology == MRLBM_POWERLAW) {
+            put("              Model: Power-Law\n");
+            put("        Power index: %.6e\n", d.nnf_n);
+            put(" Consistency factor: %.6e\n", d.nnf_k);
+            put("            Gamma 0: %.6e\n", 0.0);
+        } else {
+            put("              Model: Bingham\n");
+            put("  Plastic viscosity: %.6e\n", (1.0 / d.nnf_omega_p - 0.5) / 3.0);
+            put("       Yield stress: %.6e\n", d.nnf_yield);
+            put("      Plastic omega: %.6e\n", d.nnf_omega_p);
+        }
+        put("--------------------------------------------------------------------------------\n");
+    }
+    return t;
+}
+
 extern "C" mrlbm_status mrlbm_save_info(mrlbm_domain* dom, const char* path_files, const char* id_sim,
                                          const char* case_name, int nsteps, double mlups)
 {
     if (!dom || !path_files || !id_sim) return fail(MRLBM_EINVAL, "null argument");
-    const mrlbm_desc& d = dom->d;
     mrlbm_status st = mkdirs(std::string(path_files) + "/" + id_sim);
     if (st) return st;
-    const std::string name = std::string(path_files) + "/" + id_sim + "/" + id_sim + "_info.txt";
-    FILE* f = fopen(name.c_str(), "w");
-    if (!f) return fail(MRLBM_EIO, "cannot open '%s'", name.c_str());
-    fprintf(f, "---------------------------- SIMULATION INFORMATION ----------------------------\n");
-    fprintf(f, "      Simulation ID: %s\n", id_sim);
-    fprintf(f, "       Velocity set: D3Q%d\n", d.lattice);
-    fprintf(f, "          Precision: %s\n", d.storage == MRLBM_F32 ? "float" : d.storage == MRLBM_F16 ? "half" : "bfloat16");
-    fprintf(f, "                 NX: %d\n", d.nx);
-    fprintf(f, "                 NY: %d\n", d.ny);
-    fprintf(f, "                 NZ: %d\n", d.nz);
-    fprintf(f, "           NZ_TOTAL: %d\n", d.nz);
-    fprintf(f, "                Tau: %.6e\n", d.tau);
-    double umax = 0.0;
-    for (int k = 0; k < 4; k++)
-        for (int a = 0; a < 3; a++) umax = std::max(umax, std::fabs(d.bc_velocity[k][a]));
-    fprintf(f, "               Umax: %.6e\n", umax);
-    fprintf(f, "                 FX: %.6e\n", d.force[0]);
-    fprintf(f, "                 FY: %.6e\n", d.force[1]);
-    fprintf(f, "                 FZ: %.6e\n", d.force[2]);
-    fprintf(f, "         Save steps: %.6e\n", 0.0);
-    fprintf(f, "             Nsteps: %d\n", nsteps);
-    fprintf(f, "              MLUPS: %.6e\n", mlups);
-    fprintf(f, "                 BX: %d\n", TILE_X);
-    {
-        StepArgs sa;
-        int flags = 0;
-        fill_step_args(dom, sa, dom->cur, flags);
-        fprintf(f, "                 BY: %d\n", tile_rows(flags));
-        fprintf(f, "                 BZ: %d\n", sa.lz);
+    StepArgs sa;
+    int flags = 0;
+    fill_step_args(dom, sa, dom->cur, flags);
+    const std::string t = info_text(dom->d, id_sim, case_name, nsteps, mlups, tile_rows(flags), sa.lz);
+    return write_file(std::string(path_files) + "/" + id_sim + "/" + id_sim + "_info.txt", t.data(), t.size());
+}
+
+// The same text for a description alone, on the host (no device work): the
+// step's geometry is that of a domain without wall classes on a 148-SM B200.
+extern "C" mrlbm_status mrlbm_info_text(const mrlbm_desc* d, const char* id_sim, const char* case_name, int nsteps,
+                                        double mlups, char* buf, size_t cap, size_t* len)
+{
+    if (!d || !id_sim || !len) return fail(MRLBM_EINVAL, "null argument");
+    mrlbm_domain tmp;
+    tmp.d = *d;
+    tmp.nsm = 148;
+    const int flags = (d->rheology != MRLBM_NEWTONIAN ? F_POWERLAW | F_BC : 0) | (d->thermal ? F_THERMAL : 0);
+    const int by = tile_rows(flags);
+    const std::string t = info_text(*d, id_sim, case_name, nsteps, mlups, by, choose_lz(&tmp, by));
+    *len = t.size();
+    if (buf) {
+        if (cap < t.size() + 1) return fail(MRLBM_EINVAL, "buffer of %zu bytes, the text needs %zu", cap, t.size() + 1);
+        memcpy(buf, t.c_str(), t.size() + 1);
     }
-    fprintf(f, "--------------------------------------------------------------------------------\n");
-    fprintf(f, "\n------------------------------ BOUNDARY CONDITIONS -----------------------------\n");
-    fprintf(f, "            BC mode: Moment Based \n");
-    fprintf(f, "            BC type: %s\n", case_name ? case_name : "runtime");
-    fprintf(f, "--------------------------------------------------------------------------------\n");
-    if (d.rheology != MRLBM_NEWTONIAN) {
-        fprintf(f, "\n------------------------------ NON NEWTONIAN FLUID -----------------------------\n");
-        if (d.rheology == MRLBM_POWERLAW) {
-            fprintf(f, "              Model: Power-Law\n");
-            fprintf(f, "        Power index: %.6e\n", d.nnf_n);
-            fprintf(f, " Consistency factor: %.6e\n", d.nnf_k);
-            fprintf(f, "            Gamma 0: %.6e\n", 0.0);
-        } else {
-            fprintf(f, "              Model: Bingham\n");
-            fprintf(f, "  Plastic viscosity: %.6e\n", (1.0 / d.nnf_omega_p - 0.5) / 3.0);
-            fprintf(f, "       Yield stress: %.6e\n", d.nnf_yield);
-            fprintf(f, "      Plastic omega: %.6e\n", d.nnf_omega_p);
-        }
-        fprintf(f, "--------------------------------------------------------------------------------\n");
-    }
-    fclose(f);
     return MRLBM_OK;
 }

@@ -158,6 +158,11 @@ def lib():
             "mrlbm_save_macr_bin": [VP, C.c_char_p, C.c_char_p, C.c_int],
             "mrlbm_save_vtk": [VP, C.c_char_p, C.c_char_p, C.c_int],
             "mrlbm_save_info": [VP, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, C.c_double],
+            "mrlbm_info_text": [C.POINTER(Desc), C.c_char_p, C.c_char_p, C.c_int, C.c_double, C.c_char_p, C.c_size_t,
+                                C.POINTER(C.c_size_t)],
+            "mrlbm_voxel_mark_csv": [C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint32),
+                                     C.POINTER(C.c_longlong)],
+            "mrlbm_voxel_resolve": [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint32)],
             "mrlbm_voxel_node_types": [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint8), C.POINTER(C.c_int),
                                        C.POINTER(C.c_uint32)],
             "mrlbm_lid_cavity_node_types": [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint32)],
@@ -555,6 +560,17 @@ def request_domain(req, storage=F16):
     nm = C.c_int()
     check(lib().mrlbm_num_moments(h, C.byref(nm)))
     return _Owned(h, req.n, nm.value)
+
+
+def info_text(desc, sim_id, case_name=None, nsteps=0, mlups=0.0):
+    """The reference-format _info.txt text for a description (host only)."""
+    n = C.c_size_t()
+    cn = case_name.encode() if case_name else None
+    check(lib().mrlbm_info_text(C.byref(desc), sim_id.encode(), cn, int(nsteps), float(mlups), None, 0, C.byref(n)))
+    buf = C.create_string_buffer(n.value + 1)
+    check(lib().mrlbm_info_text(C.byref(desc), sim_id.encode(), cn, int(nsteps), float(mlups), buf, n.value + 1,
+                                C.byref(n)))
+    return buf.value.decode()
 
 
 def request_describe(req, storage=F16):

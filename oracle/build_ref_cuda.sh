@@ -19,7 +19,11 @@
 #   _ref/refsim_lid16_trace  16^3 lid cavity writing its fields after every step
 #   _ref/refsim_rb64         rayleighBenard_Periodic (thermal), 64 x 64 x 8, 1000 steps
 #   _ref/cases/*             the same cases compiled in this library's case mode
-# CASES_ONLY=1 rebuilds only the case-mode programs; THERMAL_ONLY=1 only refsim_rb64.
+#   _ref/refsim_voxel64      voxel (sphere.csv obstacle), D3Q19, 64^3, 500 steps
+#   _ref/refsim_lid64_ckpt   C1 (edges as walls), 1000 steps, checkpoint after step 500
+#   _ref/refsim_lid64_load   C1 (edges as walls) to step 1000 from a checkpoint
+# CASES_ONLY=1 rebuilds only the case-mode programs; THERMAL_ONLY=1 only refsim_rb64;
+# VOXEL_ONLY=1 only refsim_voxel64; CKPT_ONLY=1 only the two checkpoint programs.
 set -euo pipefail
 REF=${REF:?set REF to the reference checkout (its src/ folder is read)}
 HERE=$(cd "$(dirname "$0")" && pwd)
@@ -50,7 +54,7 @@ build_case() {
     echo "built $OUT/$name"
 }
 
-if [ -z "${CASES_ONLY:-}" ] && [ -z "${THERMAL_ONLY:-}" ]; then
+if [ -z "${CASES_ONLY:-}" ] && [ -z "${THERMAL_ONLY:-}" ] && [ -z "${VOXEL_ONLY:-}" ] && [ -z "${CKPT_ONLY:-}" ]; then
 # C1: lid-driven cavity 64^3, Re 100, lid velocity 0.05 (tau from Re, constants.inc:35-36)
 build_case refsim_lid64 lidDrivenCavity_3D D3Q19 2000 64 \
   'sed -i "s/^constexpr dfloat RE = .*/constexpr dfloat RE = 100;/; s/^constexpr dfloat U_MAX = .*/constexpr dfloat U_MAX = 0.05;/" "$c/constants.inc"; sed -i "s/^#define REPORT_SAVE .*/#define REPORT_SAVE (false)/" "$c/output.inc"'
@@ -81,7 +85,36 @@ build_case refsim_tgv256_q27 taylorGreen D3Q27 1000 256 \
 build_case refsim_bench256 benchmark D3Q19 1000 256 'true'
 fi
 
-if [ -z "${CASES_ONLY:-}" ] || [ -n "${THERMAL_ONLY:-}" ]; then
+if { [ -z "${CASES_ONLY:-}" ] && [ -z "${THERMAL_ONLY:-}" ] && [ -z "${CKPT_ONLY:-}" ]; } || [ -n "${VOXEL_ONLY:-}" ]; then
+# voxel obstacle case (VOXEL_FILENAME "sphere.csv", read from the working
+# directory), 64^3 periodic, 500 steps.  As shipped its U_MAX = 0 gives
+# TAU = 0.5 (no viscosity) and its fluid starts at rest with the body force
+# zeroed in the kernel (mlbm.cu:76-78), so nothing would move: U_MAX = 0.05
+# (TAU 0.519 at RE 500) and an initial uniform flow U_0_Z = 0.02 past the
+# obstacle make the run exercise the 254 voxel wall types.  Its FZ = 1e-6 is
+# set to 0 (the reference's kernel drops the force; this library applies it).
+build_case refsim_voxel64 voxel D3Q19 500 64 \
+  'sed -i "s/^constexpr dfloat U_MAX = .*/constexpr dfloat U_MAX = 0.05;/; s/^constexpr dfloat U_0_Z = .*/constexpr dfloat U_0_Z = 0.02;/; s/^constexpr dfloat FZ = .*/constexpr dfloat FZ = 0.0;/" "$c/constants.inc"; sed -i "s/^#define REPORT_SAVE .*/#define REPORT_SAVE (false)/" "$c/output.inc"'
+fi
+[ -n "${VOXEL_ONLY:-}" ] && exit 0
+
+if { [ -z "${CASES_ONLY:-}" ] && [ -z "${THERMAL_ONLY:-}" ] && [ -z "${VOXEL_ONLY:-}" ]; } || [ -n "${CKPT_ONLY:-}" ]; then
+# checkpoint interchange, on C1 with the lid's edges as walls, 1000 steps:
+# refsim_lid64_ckpt writes its checkpoint file set and its macroscopic fields
+# (.bin and legacy VTK) after step 500 (CHECKPOINT_SAVE, MACR_SAVE 500);
+# refsim_lid64_load starts from a checkpoint file set
+# (LOAD_CHECKPOINT true: the step from the last int of
+# ..\\bin\\TEST\\000\\checkpoint\\_curr_step.bin, a name the reference builds
+# with Windows separators, the arrays from TEST/000/checkpoint/_*.bin)
+LID_EDGES='sed -i "s/^constexpr dfloat RE = .*/constexpr dfloat RE = 100;/; s/^constexpr dfloat U_MAX = .*/constexpr dfloat U_MAX = 0.05;/" "$c/constants.inc"; sed -i "s/^#define REPORT_SAVE .*/#define REPORT_SAVE (false)/" "$c/output.inc"; printf "\nif (y == (NY - 1) && (x == 0 || x == (NX - 1) || z == 0 || z == (NZ_TOTAL - 1))) {\n    nodeType = NORTH | (x == 0 ? WEST : 0) | (x == (NX - 1) ? EAST : 0) | (z == 0 ? BACK : 0) | (z == (NZ_TOTAL - 1) ? FRONT : 0);\n}\n" >> "$c/bc_initialization.inc"'
+build_case refsim_lid64_ckpt lidDrivenCavity_3D D3Q19 1000 64 \
+  "$LID_EDGES"'; sed -i "s/^#define CHECKPOINT_SAVE .*/#define CHECKPOINT_SAVE 500/" "$c/constants.inc"; sed -i "s/^#define MACR_SAVE .*/#define MACR_SAVE (500)/; s/^#define VTK_SAVE .*/#define VTK_SAVE (true)/; s/^#define ONLY_FINAL_MACRO .*/#define ONLY_FINAL_MACRO (false)/" "$c/output.inc"'
+build_case refsim_lid64_load lidDrivenCavity_3D D3Q19 1000 64 \
+  "$LID_EDGES"'; sed -i "s/^#define LOAD_CHECKPOINT .*/#define LOAD_CHECKPOINT true/" "$c/constants.inc"'
+fi
+[ -n "${CKPT_ONLY:-}" ] && exit 0
+
+if { [ -z "${CASES_ONLY:-}" ] && [ -z "${VOXEL_ONLY:-}" ] && [ -z "${CKPT_ONLY:-}" ]; } || [ -n "${THERMAL_ONLY:-}" ]; then
 # thermal: rayleighBenard_Periodic (D3Q19 flow + D3G19 scalar, THERMAL_MODEL),
 # 64 x 64 x 8, Pr 10, Ra 1e5, hot WEST / cold EAST walls, gravity along x,
 # 1000 steps; final rho, u and C as .bin.  The case ships NZ = 4, which is
@@ -114,6 +147,9 @@ $PY "$CB" "$REF/src/cases/lidDrivenCavity_3D" -o "$OUT/cases/lid64" --set N=64 -
 $PY "$CB" "$REF/src/cases/taylorGreen" -o "$OUT/cases/tgv256_q27" --lattice 27 --set N=256 --set RE=1600 \
     --set U_MAX=0.04 --set N_STEPS=1000 --set "REPORT_SAVE=(100)" --set "SAVEDATA=(true)" $common_out
 $PY "$CB" "$REF/src/cases/benchmark" -o "$OUT/cases/bench256" --set N_STEPS=1000 $common_out
+# voxel obstacle case as refsim_voxel64 runs it
+$PY "$CB" "$REF/src/cases/voxel" -o "$OUT/cases/voxel64" --set N=64 --set N_STEPS=500 --set U_MAX=0.05 \
+    --set U_0_Z=0.02 --set FZ=0.0 --set "REPORT_SAVE=(false)" $common_out
 # thermal: rayleighBenard_Periodic as refsim_rb64 runs it (NZ = 8, 1000 steps)
 $PY "$CB" "$REF/src/cases/rayleighBenard_Periodic" -o "$OUT/cases/rb64" --set NZ=8 --set N_STEPS=1000 \
     --set "REPORT_SAVE=(false)" $common_out

@@ -92,6 +92,54 @@ def test_voxel_typing_matches_bc_id():
                     assert t[z, y, x] == (0xFE if want == 0xFF else want)
 
 
+def test_voxel_file_loading_matches_read_xyz_file_and_define_voxel_bc(tmp_path):
+    """mrlbm_voxel_mark_csv + mrlbm_voxel_resolve against a restatement of the
+    reference's read_xyz_file (src/lbmInitialization.cu:978-1039: solid
+    voxels, their 26 neighbours marked MISSING_DEFINITION with every axis
+    wrapped, out-of-grid lines skipped) and define_voxel_bc / bc_id (wrapped
+    octant masks; a mask of all eight octants is the solid word)."""
+    mrlbm = _lib()
+    L = mrlbm.lib()
+    nx, ny, nz = 9, 8, 7
+    rng = np.random.default_rng(11)
+    pts = [tuple(int(v) for v in p) for p in rng.integers(0, [nx, ny, nz], size=(25, 3))]
+    pts += [(0, 0, 0), (nx - 1, 3, 2), (4, ny - 1, nz - 1), (nx + 3, 1, 1), (2, 2, nz)]   # wrap + out of grid
+    csv = tmp_path / "vox.csv"
+    csv.write_text("".join("%d,%d,%d\n" % p for p in pts))
+    nt = np.zeros((nz, ny, nx), dtype=np.uint32)
+    count = C.c_longlong()
+    rc = L.mrlbm_voxel_mark_csv(str(csv).encode(), nx, ny, nz, nt.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                C.byref(count))
+    assert rc == 0
+    # restatement of read_xyz_file
+    want = np.zeros((nz, ny, nx), dtype=np.int64)
+    n_in = 0
+    for x, y, z in pts:
+        if x >= nx or y >= ny or z >= nz:
+            continue
+        n_in += 1
+        want[z, y, x] = 0xFF
+        for dz in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dx in (-1, 0, 1):
+                    k = ((z + dz) % nz, (y + dy) % ny, (x + dx) % nx)
+                    if k == (z, y, x) or want[k] == 0xFF:
+                        continue
+                    want[k] = 0xFFFFFFFF
+    assert count.value == n_in
+    assert np.array_equal(nt.astype(np.int64), want)
+    rc = L.mrlbm_voxel_resolve(nx, ny, nz, nt.ctypes.data_as(C.POINTER(C.c_uint32)))
+    assert rc == 0
+    solid = (want == 0xFF).astype(np.uint8)
+    for z in range(nz):
+        for y in range(ny):
+            for x in range(nx):
+                if want[z, y, x] == 0xFFFFFFFF:
+                    assert nt[z, y, x] == bc_id_restated(solid, x, y, z), (x, y, z)
+                else:
+                    assert nt[z, y, x] == want[z, y, x]
+
+
 def test_voxel_typing_walls_on_nonperiodic_axes():
     mrlbm = _lib()
     solid = np.zeros((6, 5, 4), dtype=np.uint8)

@@ -10,6 +10,10 @@ same inputs.
   kinetic-energy reports (every 100 steps) must agree.
 * lidDrivenCavity_3D 64^3: the case's own bc_definition.inc running inside the
   z-march kernel must agree with the library's generic moment-BC solver.
+* voxel (an obstacle case whose VOXEL_FILENAME names a CSV of solid nodes),
+  64^3, 500 steps, with a sphere and a blob that wraps across the periodic
+  faces: the case's voxel file, its 254-mask bc_definition.inc and the
+  reference program's own run must agree to FP32 operation order.
 """
 import os
 import re
@@ -81,6 +85,36 @@ def test_taylor_green_d3q27_case_matches_reference_program(tmp_path):
     worst = max(abs(ko[s] - kr[s]) / kr[s] for s in kr)
     print("TGV 256^3 D3Q27: reference %.0f MLUPS, case mode %.0f MLUPS; KE worst rel diff %.2e" % (ml_ref, ml_ours, worst))
     assert worst < 2e-5
+
+
+def write_voxels(path, n):
+    """A sphere of radius 9 at the centre and a small blob across the corner of
+    the periodic box (its neighbours wrap), as "x,y,z" lines."""
+    c = (n - 1) / 2.0
+    pts = []
+    for z in range(n):
+        for y in range(n):
+            for x in range(n):
+                if (x - c) ** 2 + (y - c) ** 2 + (z - c) ** 2 <= 81.0:
+                    pts.append((x, y, z))
+    pts += [(0, 0, 0), (n - 1, 0, 0), (0, n - 1, 1), (1, 1, n - 1)]
+    with open(path, "w") as f:
+        f.write("".join("%d,%d,%d\n" % p for p in pts))
+
+
+def test_voxel_case_matches_reference_program(tmp_path):
+    n = 64
+    for who in ("ref", "ours"):
+        os.makedirs(tmp_path / who, exist_ok=True)
+        write_voxels(tmp_path / who / "sphere.csv", n)
+    ml_ref = run(os.path.join(REF, "refsim_voxel64"), tmp_path / "ref")
+    ml_ours = run(os.path.join(REF, "cases", "voxel64"), tmp_path / "ours")
+    a, b = fields(tmp_path / "ours", n, 500), fields(tmp_path / "ref", n, 500)
+    e = u_err(a, b)
+    drho = float(np.max(np.abs(a["rho"] - b["rho"])))
+    print("voxel 64^3: reference %.0f MLUPS, case mode %.0f MLUPS; u rel L2 %.2e, max |drho| %.2e"
+          % (ml_ref or 0, ml_ours or 0, e, drho))
+    assert e < 1e-4 and drho < 1e-5
 
 
 def test_lid_case_bc_snippet_equals_generic_solver(tmp_path):

@@ -7,6 +7,12 @@
   (rho and u: relative L2 5e-5, Linf 5e-4; second moments 3e-4 / 2e-3) or
   twice the error of the oracle's own FP32 build, whichever is larger (a
   driven flow accumulates FP32 round-off over its 2000 steps).
+* Periodic Taylor-Green vortex 256^3, D3Q27, Re 1600, u0 0.04, 1000 steps
+  (src/cases/taylorGreen/constants.inc:14-16): the kinetic energy every 100
+  steps and every stored moment on z planes 0 and 96 (every 4th node in x and
+  y) against the FP64 oracle's values in tests/golden/tgv256_fp64.npz (made by
+  tests/golden/make_tgv_fixtures.py), with the per-moment bounds of
+  test_gpu_parity.py.
 * FP16 batch members: three uneven FP16 lid cavities advanced together by the
   batched kernel, each against the FP64 oracle.
 * An FP16 power-law duct request (voxel obstacles, body force) solved by the
@@ -16,6 +22,8 @@
 16-bit storage rounds every stored moment each step, so its bounds are the
 measured 16-bit error level with a margin, stated next to each assertion.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -23,6 +31,7 @@ import mrlbm
 import parity_util as pu
 
 pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 def per_moment_bounds(res, yard, l2=2e-5, linf=2e-4, l2_2=3e-4, linf_2=2e-3):
@@ -59,6 +68,34 @@ def test_lid_cavity_64_full_run_matches_fp64_oracle():
         print("C1 moment %d: GPU rel L2 %.2e Linf %.2e | FP32 oracle %.2e %.2e" % (k, *res[k], *yard[k]))
     assert pu.velocity_rel_l2(g, o) < 1e-4
     bad = per_moment_bounds(res, yard, l2=5e-5, linf=5e-4)
+    assert not bad, "; ".join(bad)
+
+
+def test_taylor_green_256_d3q27_matches_fp64_fixture():
+    ref = np.load(os.path.join(HERE, "golden", "tgv256_fp64.npz"))
+    n, steps, re = int(ref["n"]), int(ref["steps"]), float(ref["re"])
+    L = n / (2 * np.pi)
+    tau = 0.5 + 3.0 * 0.04 * L / re
+    assert abs(tau - float(ref["tau"])) < 1e-12
+    d = mrlbm.make_desc(n, n, n, lattice=27, tau=tau)
+    dom = mrlbm.Domain(d)
+    dom.init_taylor_green(0.04, L)
+    ke = [dom.sums()["kinetic_energy"]]
+    for _ in range(steps // 100):
+        dom.step(100)
+        ke.append(dom.sums()["kinetic_energy"])
+    m = dom.moments()
+    dom.close()
+    ke_ref = ref["ke"][:, 1]
+    ke_err = np.abs(np.array(ke) - ke_ref) / ke_ref
+    print("TGV 256^3 D3Q27: KE worst relative difference vs FP64 %.2e" % ke_err.max())
+    assert ke_err.max() < 1e-5
+    planes, st = [int(p) for p in ref["planes"]], int(ref["stride"])
+    g = m[:, planes][:, :, ::st, ::st]
+    res = pu.compare(g, ref["moments"].astype(np.float64))
+    for k in range(10):
+        print("C2 moment %d: rel L2 %.2e Linf %.2e" % (k, *res[k]))
+    bad = per_moment_bounds(res, {k: (0.0, 0.0) for k in res})
     assert not bad, "; ".join(bad)
 
 
