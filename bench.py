@@ -275,7 +275,7 @@ def run_gpu_arm(args):
             dom.synchronize()
             if len(reps) == 1:
                 first = max_over_ranks(pg, reps[0])
-                nrep = max(1, min(MAX_REGIONS, int(np.ceil(MIN_TIMED_S * 1e3 / max(first, 1e-6)))))
+                nrep = max(1, min(MAX_REGIONS, int(np.ceil(args.min_timed_s * 1e3 / max(first, 1e-6)))))
             if len(reps) >= nrep:
                 break
     barrier(pg)
@@ -702,6 +702,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--min-timed-s", type=float, default=MIN_TIMED_S,
+                    help="repeat the K-step timed region until this much device time has run (0: one region)")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="reference arm: skip the side run of the reference's own CUDA program")
     ap.add_argument("--cpu-budget", type=float, default=15.0)

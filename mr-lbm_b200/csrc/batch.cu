@@ -389,6 +389,11 @@ extern "C" mrlbm_status mrlbm_batch_chunk_for(mrlbm_batch* b, int nx, int ny, in
 // Coordinate search over the z-chunk length of each size class present, timing
 // the whole batch: the chunk trades z-halo work (2 planes per chunk) against
 // the number of work items available for load balance.
+// Chunk autotuner.  It times candidate chunks on the members themselves, so it
+// first copies every member's current moment buffer (ghost shell included)
+// aside and afterwards copies it back and restores the step counters: the
+// timed steps (an even number, so the buffer parities come back) leave no
+// trace in any solve.
 extern "C" mrlbm_status mrlbm_batch_autotune(mrlbm_batch* b)
 {
     if (!b) return fail(MRLBM_EINVAL, "null batch");
@@ -398,6 +403,26 @@ extern "C" mrlbm_status mrlbm_batch_autotune(mrlbm_batch* b)
             const int c = size_class(d->d.nx, d->d.ny, d->d.nz);
             if (std::find(classes.begin(), classes.end(), c) == classes.end()) classes.push_back(c);
         }
+    // snapshot
+    struct Saved {
+        mrlbm_domain* dom;
+        size_t bytes, off;
+        int cur, step;
+    };
+    std::vector<Saved> saved;
+    size_t total = 0;
+    for (mrlbm_domain* d : b->members)
+        if (d) {
+            const size_t bytes = (size_t)d->field * (2 * ((d->nms + 1) / 2)) * d->esize;
+            saved.push_back({d, bytes, total, d->cur, d->step});
+            total += (bytes + 255) / 256 * 256;
+        }
+    const long long step0 = b->step;
+    char* snap = nullptr;
+    if (total) CK(cudaMalloc(&snap, total));
+    for (const Saved& s : saved)
+        CK(cudaMemcpyAsync(snap + s.off, s.dom->m[s.cur], s.bytes, cudaMemcpyDeviceToDevice, b->stream));
+
     static const int cand[] = {8, 16, 24, 32, 48, 64, 96};
     auto timed = [&](float* ms) -> mrlbm_status {
         mrlbm_status st = refresh(b);
@@ -412,20 +437,37 @@ extern "C" mrlbm_status mrlbm_batch_autotune(mrlbm_batch* b)
         CK(cudaEventElapsedTime(ms, b->ev0, b->ev1));
         return MRLBM_OK;
     };
+    mrlbm_status st = MRLBM_OK;
     for (int c : classes) {
         float best = 1e30f;
         int best_lz = 32;
         for (int lz : cand) {
             b->lz_by_class[c] = lz;
             float ms = 0.f;
-            mrlbm_status st = timed(&ms);
-            if (st) return st;
+            if ((st = timed(&ms))) break;
             if (ms < best * 0.98f) {
                 best = ms;
                 best_lz = lz;
             }
         }
         b->lz_by_class[c] = best_lz;
+        if (st) break;
     }
+    // restore the members and the step counters (the device counter too)
+    cudaStreamSynchronize(b->stream);
+    for (const Saved& s : saved) {
+        cudaMemcpyAsync(s.dom->m[s.cur], snap + s.off, s.bytes, cudaMemcpyDeviceToDevice, b->stream);
+        s.dom->cur = s.cur;
+        s.dom->step = s.step;
+    }
+    b->step = step0;
+    {
+        const int dstep = (int)step0;
+        cudaMemcpyAsync(&b->d_ctl->step, &dstep, sizeof(int), cudaMemcpyHostToDevice, b->stream);
+    }
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    cudaFree(snap);
+    if (st) return st;
+    if (e != cudaSuccess) return fail(MRLBM_ECUDA, "autotune restore: %s", cudaGetErrorString(e));
     return refresh(b);
 }

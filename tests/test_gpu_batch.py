@@ -104,10 +104,14 @@ def test_batch_autotune_keeps_results():
         m.set_node_types(nt)
         m.init_uniform()
         mem.append(m)
-    b.autotune()                   # runs timed steps on the members
-    steps_done = mem[0].step_count
+    b.step(6)
+    before = [(m.step_count, m.moments()) for m in mem]
+    b.autotune()                   # times candidate chunks on the members, then restores them
+    for (steps, mom), m in zip(before, mem):
+        assert m.step_count == steps == 6
+        np.testing.assert_array_equal(m.moments(), mom)
     b.step(10)
     for (d, nt), m in zip(cases, mem):
-        np.testing.assert_array_equal(m.moments(), run_alone(d, nt, steps_done + 10))
+        np.testing.assert_array_equal(m.moments(), run_alone(d, nt, 16))
         assert 1 <= b.chunk_for(d.nx, d.ny, d.nz) <= d.nz
     b.close()
