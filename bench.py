@@ -416,19 +416,13 @@ def run_batch_workload(args):
     return 0
 
 
-def run_serve_workload(args):
-    """Poisson arrivals (mean 200/s) of D3Q19 solves, 50/50 lid cavities and
-    power-law ducts with 5 % voxel obstacles, edges U{32..192}, FP16 storage,
-    each until residual <= 1e-6 or 20k steps, HBM budget 150 GB; then the same
-    requests solved one at a time with plain single-domain launches (each
-    request's time includes building its domain, as it does in the server)."""
+def serve_requests(rng, count, rate):
+    """`count` requests with Poisson arrivals (mean `rate`/s), 50/50 lid
+    cavities (Re U[50, 1000]) and power-law ducts (n U[0.6, 1.2], 5 % voxel
+    obstacles), edges U{32..192}."""
     import mrlbm
 
-    mrlbm.set_device(0)
-    rng = np.random.default_rng(20261203)
-    count = args.requests
-    gaps = rng.exponential(1.0 / args.rate, size=count)
-    arrivals = np.cumsum(gaps)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=count))
     reqs = []
     for k in range(count):
         n = int(rng.integers(32, 193))
@@ -437,8 +431,18 @@ def run_serve_workload(args):
         else:
             reqs.append(mrlbm.make_request(mrlbm.REQ_DUCT, n, nnf_n=float(rng.uniform(0.6, 1.2)), solid_fraction=0.05,
                                            seed=int(rng.integers(1 << 62))))
-    srv = mrlbm.Server(storage=mrlbm.F16, hbm_budget=150e9, max_active=args.max_active, steps_per_tick=100,
-                       residual_tol=1e-6, max_steps=args.max_steps)
+    return reqs, arrivals
+
+
+def serve_phase(args, reqs, arrivals, storage):
+    """The requests through the continuous-batching server, then one at a
+    time with plain single-domain launches (a request's latency includes
+    building its domain in both); returns the phase's record and the served
+    results (steps, final moments)."""
+    import mrlbm
+
+    srv = mrlbm.Server(storage=storage, hbm_budget=150e9, max_active=args.max_active, steps_per_tick=100,
+                       residual_tol=1e-6, max_steps=args.max_steps, keep_results=True)
     t0 = srv.now()
     ids = []
     for r, a in zip(reqs, arrivals):
@@ -454,20 +458,20 @@ def run_serve_workload(args):
             time.sleep(0.001)  # waiting for the next arrival
     wall = time.perf_counter() - wall0
     stats = srv.stats()
-    steps_done = [srv.result(i)["steps"] for i in ids]
+    served = []
+    for i, r in zip(ids, reqs):
+        res = srv.result(i)
+        nm = 11 if r.kind == mrlbm.REQ_DUCT else 10
+        served.append((res, srv.moments(i, r.n, nm) if res["status"] == 0 else None))
+        srv.release(i)
     srv.close()
-    # one at a time, plain launches, same convergence rule
     t_alone = 0.0
     lat_alone = []
     clock = 0.0
-    setup = []
     for r, a in zip(reqs, arrivals):
-        # a request's latency includes building its domain, as in the server
         t1 = time.perf_counter()
-        dom = mrlbm.request_domain(r, mrlbm.F16)
+        dom = mrlbm.request_domain(r, storage)
         dom.residual()
-        dom.synchronize()
-        setup.append(time.perf_counter() - t1)
         steps = 0
         while steps < args.max_steps:
             dom.step(100)
@@ -480,21 +484,75 @@ def run_serve_workload(args):
         t_alone += dt
         clock = max(clock, float(a)) + dt
         lat_alone.append(clock - float(a))
-    line = {"metric": "serving solves/s and latency (continuous batching)", "value": round(stats["solves_per_s"], 4),
-            "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f16 storage, f32 arithmetic",
-            "data": "synthetic (seed 20261203)",
-            "config": {"workload": "serving_poisson_d3q19", "rate_per_s": args.rate, "requests": count,
-                       "edges": "U{32..192}", "mix": "50/50 lid cavity / power-law duct (5% obstacles)",
-                       "residual_tol": 1e-6, "max_steps": args.max_steps, "hbm_budget_gb": 150},
-            "p50_latency_s": stats["p50_latency"], "p99_latency_s": stats["p99_latency"],
-            "mean_latency_s": stats["mean_latency"], "done": stats["done"], "failed": stats["failed"],
-            "wall_s": round(wall, 3), "lattice_updates": stats["lattice_updates"],
-            "mlups": stats["lattice_updates"] / wall / 1e6,
-            "alone": {"solves_per_s": count / t_alone, "p50_latency_s": float(np.percentile(lat_alone, 50)),
-                      "p99_latency_s": float(np.percentile(lat_alone, 99)),
-                      "setup_s_mean": float(np.mean(setup)), "setup_s_max": float(np.max(setup))},
-            "speedup_vs_alone": (stats["solves_per_s"] / (count / t_alone)) if t_alone > 0 else None,
-            "steps_per_request": {"min": int(min(steps_done)), "max": int(max(steps_done))}}
+    steps_done = [res["steps"] for res, _ in served]
+    resid = [res["residual"] for res, _ in served]
+    rec = {"rate_per_s": None, "requests": len(reqs), "solves_per_s": round(stats["solves_per_s"], 4),
+           "p50_latency_s": stats["p50_latency"], "p99_latency_s": stats["p99_latency"],
+           "mean_latency_s": stats["mean_latency"], "done": stats["done"], "failed": stats["failed"],
+           "wall_s": round(wall, 3), "mlups": stats["lattice_updates"] / wall / 1e6,
+           "alone": {"solves_per_s": len(reqs) / t_alone, "p50_latency_s": float(np.percentile(lat_alone, 50)),
+                     "p99_latency_s": float(np.percentile(lat_alone, 99))},
+           "speedup_vs_alone": (stats["solves_per_s"] / (len(reqs) / t_alone)) if t_alone > 0 else None,
+           "steps_per_request": {"min": int(min(steps_done)), "max": int(max(steps_done))},
+           "final_residual": {"min": float(min(resid)), "max": float(max(resid))},
+           "retired_on_residual": int(sum(1 for s in steps_done if s < args.max_steps))}
+    return rec, served
+
+
+def serve_errors(reqs, served, sample):
+    """Relative L2 error of each sampled served velocity field against an FP32
+    solve of the same request for the same number of steps (fluid nodes)."""
+    import mrlbm
+
+    out = {"lid_cavity": [], "duct": []}
+    for k, (r, (res, m)) in enumerate(zip(reqs, served)):
+        if m is None or k >= sample:
+            continue
+        ref = mrlbm.request_domain(r, mrlbm.F32)
+        ref.step(res["steps"])
+        mr = ref.moments()
+        ref.close()
+        _, nt = mrlbm.request_describe(r, mrlbm.F32)
+        fluid = nt != mrlbm.NODE_SOLID
+        du = (m[1:4] - mr[1:4])[:, fluid].astype(np.float64)
+        e = float(np.sqrt(np.sum(du * du) / np.sum(mr[1:4][:, fluid].astype(np.float64) ** 2)))
+        out["lid_cavity" if r.kind == mrlbm.REQ_LID_CAVITY else "duct"].append(e)
+    return {t: {"sampled": len(v), "u_rel_l2_max": max(v) if v else None, "u_rel_l2_mean": float(np.mean(v)) if v else None}
+            for t, v in out.items()}
+
+
+def run_serve_workload(args):
+    """Serving (continuous batching) of D3Q19 solves: Poisson arrivals,
+    50/50 lid cavities and power-law ducts with 5 % voxel obstacles, edges
+    U{32..192}, each until residual <= 1e-6 or --max-steps, HBM budget 150 GB,
+    at two loads: the saturating rate (--rate, 200/s by default: offered work
+    far above what one GPU does) and a rate below capacity (--rate-low), each
+    against the same requests solved one at a time with plain single-domain
+    launches.  Storage --serve-storage (split-velocity fp16 by default); the
+    accuracy columns compare sampled served velocity fields with FP32 solves
+    of the same requests for the same step counts."""
+    import mrlbm
+
+    mrlbm.set_device(0)
+    storage = {"f16": mrlbm.F16, "f16u": mrlbm.F16U, "f32": mrlbm.F32}[args.serve_storage]
+    phases = {}
+    for name, rate, count in (("saturated", args.rate, args.requests), ("below_capacity", args.rate_low,
+                                                                        args.requests_low)):
+        rng = np.random.default_rng(20261203)
+        reqs, arrivals = serve_requests(rng, count, rate)
+        rec, served = serve_phase(args, reqs, arrivals, storage)
+        rec["rate_per_s"] = rate
+        rec["accuracy_vs_fp32"] = serve_errors(reqs, served, args.error_sample)
+        phases[name] = rec
+        del served
+    sat = phases["saturated"]
+    line = {"metric": "serving solves/s and latency (continuous batching)", "value": sat["solves_per_s"],
+            "unit": "solves/s", "n_gpus": 1, "higher_is_better": True,
+            "dtype": "%s storage, f32 arithmetic" % args.serve_storage, "data": "synthetic (seed 20261203)",
+            "config": {"workload": "serving_poisson_d3q19", "edges": "U{32..192}",
+                       "mix": "50/50 lid cavity / power-law duct (5% obstacles)", "residual_tol": 1e-6,
+                       "max_steps": args.max_steps, "hbm_budget_gb": 150, "storage": args.serve_storage},
+            "phases": phases}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -722,6 +780,10 @@ def main():
     ap.add_argument("--alone-steps", type=int, default=200)
     ap.add_argument("--requests", type=int, default=32)
     ap.add_argument("--rate", type=float, default=200.0)
+    ap.add_argument("--rate-low", type=float, default=0.1, help="serving: the below-capacity arrival rate")
+    ap.add_argument("--requests-low", type=int, default=12)
+    ap.add_argument("--serve-storage", default="f16u", choices=["f16", "f16u", "f32"])
+    ap.add_argument("--error-sample", type=int, default=8, help="serving: requests compared with an FP32 solve")
     ap.add_argument("--max-active", type=int, default=512)
     ap.add_argument("--max-steps", type=int, default=20000)
     args = ap.parse_args()

@@ -44,7 +44,8 @@ typedef enum {
     MRLBM_ETIMEDOUT = 6,  /* a bounded device wait gave up */
     MRLBM_ENOTFOUND = 7,  /* unknown request / handle */
     MRLBM_EBUSY = 8,      /* no free slot / request still queued or running */
-    MRLBM_ECANCELED = 9   /* request cancelled */
+    MRLBM_ECANCELED = 9,  /* request cancelled */
+    MRLBM_EBOUNDS = 10    /* bounds-check build: a step kernel skipped an out-of-range access */
 } mrlbm_status;
 
 typedef enum { MRLBM_D3Q19 = 19, MRLBM_D3Q27 = 27 } mrlbm_lattice;
@@ -239,6 +240,21 @@ mrlbm_status mrlbm_zslab_plane(mrlbm_domain* dom, int which, mrlbm_zplane* out);
  * the work queued on both domains' streams and before dst's later work.  The
  * two domains must have the same nx, ny, lattice, storage and moments. */
 mrlbm_status mrlbm_zslab_copy(mrlbm_domain* src, int src_which, mrlbm_domain* dst, int dst_which);
+/* The exchange across processes (one slab per rank), for C/C++ callers: NCCL
+ * point-to-point operations of all moment pairs' planes, in place, in one NCCL
+ * group queued on the domain's stream after its steps (no host wait).  The
+ * library opens libnccl.so.2 itself.  mrlbm_nccl_unique_id writes a
+ * 128-byte id that the caller hands to every rank (its own transport);
+ * mrlbm_nccl_comm_init makes this rank's communicator on the current device;
+ * rank_below / rank_above are the ranks of the neighbouring slabs in that
+ * communicator, -1 at a non-periodic end, the own rank for a single periodic
+ * slab.  Every rank lists the upward plane before the downward one, so sends
+ * and receives pair up in NCCL's per-peer order.  No reference counterpart
+ * (the reference is single-GPU, README.md:38). */
+mrlbm_status mrlbm_nccl_unique_id(void* id);
+mrlbm_status mrlbm_nccl_comm_init(int nranks, const void* id, int rank, void** comm);
+mrlbm_status mrlbm_nccl_comm_destroy(void* comm);
+mrlbm_status mrlbm_zslab_exchange_nccl(mrlbm_domain* dom, void* comm, int rank_below, int rank_above);
 
 /* Moments in the reference's idxMom layout (fMom, host float buffer of
  * nx*ny*nz*num_moments).  Used by checkpoints and drop-in callers. */

@@ -48,7 +48,8 @@ struct InitArgs {
     float tg_u0, tg_L;
     int thermal;  // moments 10..13 are C and its flux: C = c0, no flux
     float c0;     // (the thermal cases' flow_initialization.inc: cVar = T_REFERENCE, q = 0)
-    int lo0;      // split velocity: stored word of the low part of 3u_x (-1: none)
+    int lo0;      // split storage: stored word of the low part of 3u_x (-1: none)
+    int lom;      // split storage: stored word of the low part of omega (-1: none)
     float scale[NM_MAX];
 };
 
@@ -92,6 +93,7 @@ __global__ void init_kernel(const InitArgs a)
         }
         if (a.lo0 >= 0)
             for (int c = 0; c < 3; c++) m[a.lo0 + c] = split_low(m[1 + c], a.scale[1 + c]);
+        if (a.lom >= 0) m[a.lom] = split_low(m[10], a.scale[10]);
         const long long idx = pidx(x, y, z, a.pitch, a.plane);
         T* p0 = reinterpret_cast<T*>(a.m0);
         T* p1 = reinterpret_cast<T*>(a.m1);
@@ -113,7 +115,8 @@ struct ConvArgs {
     int nx, ny, nz, pitch;
     long long plane, field;
     int nm, mode;
-    int lo0;  // split velocity: stored word of the low part of 3u_x (-1: none)
+    int lo0;  // split storage: stored word of the low part of 3u_x (-1: none)
+    int lom;  // split storage: stored word of the low part of omega (-1: none)
     float scale[NM_MAX], iscale[NM_MAX];
 };
 
@@ -138,20 +141,21 @@ __global__ void convert_kernel(const ConvArgs a)
             const long long blk = (x >> 3) + (long long)nbx * ((y >> 3) + (long long)nby * (z >> 3));
             fi = (x & 7) + 8 * ((y & 7) + 8 * ((z & 7) + 8 * (k + (long long)a.nm * blk)));
         }
-        // split velocity: 3u = high word + low word (stored word lo0 + k - 1)
-        const bool split = a.lo0 >= 0 && k >= 1 && k <= 3;
-        const long long lidx = split ? mphys(a.lo0 + k - 1, pidx(x, y, z, a.pitch, a.plane), a.field) : 0;
+        // split storage: 3u (and omega) = high word + low word
+        const int lw = (a.lo0 >= 0 && k >= 1 && k <= 3) ? a.lo0 + k - 1 : (a.lom >= 0 && k == 10 ? a.lom : -1);
+        const bool split = lw >= 0;
+        const long long lidx = split ? mphys(lw, pidx(x, y, z, a.pitch, a.plane), a.field) : 0;
         if (a.mode == 0 || a.mode == 2) {
             const float v = Stor<T>::ld(reinterpret_cast<const T*>(a.m0) + idx);
             float r = is_f32<T>() ? v : v * a.iscale[k];
-            if (split) r += Stor<T>::ld(reinterpret_cast<const T*>(a.m0) + lidx) * a.iscale[a.lo0 + k - 1];
+            if (split) r += Stor<T>::ld(reinterpret_cast<const T*>(a.m0) + lidx) * a.iscale[lw];
             a.f[fi] = r;
         } else {
             const float v = is_f32<T>() ? a.f[fi] : a.f[fi] * a.scale[k];
             Stor<T>::st(reinterpret_cast<T*>(a.m0) + idx, v);
             Stor<T>::st(reinterpret_cast<T*>(a.m1) + idx, v);
             if (split) {
-                const float lo = split_low(a.f[fi], a.scale[k]) * a.scale[a.lo0 + k - 1];
+                const float lo = split_low(a.f[fi], a.scale[k]) * a.scale[lw];
                 Stor<T>::st(reinterpret_cast<T*>(a.m0) + lidx, lo);
                 Stor<T>::st(reinterpret_cast<T*>(a.m1) + lidx, lo);
             }

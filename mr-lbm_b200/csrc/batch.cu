@@ -42,27 +42,31 @@ struct mrlbm_batch {
 
 namespace {
 
-template <int Q, typename T>
+template <int Q, typename T, int S = 0>
 mrlbm_status set_attr(size_t& smem)
 {
-    smem = ZSmem<Q, T, batch_tyi(Q), batch_npm<T>()>::bytes;
-    cudaError_t e = cudaFuncSetAttribute(batch_step<Q, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    smem = ZSmem<Q, T, batch_tyi(Q), batch_npm<T, S>()>::bytes;
+    cudaError_t e = cudaFuncSetAttribute(batch_step<Q, T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return fail(MRLBM_ECUDA, "batch attribute: %s", cudaGetErrorString(e));
     return MRLBM_OK;
 }
 
-template <int Q, typename T>
+template <int Q, typename T, int S = 0>
 void launch(mrlbm_batch* b)
 {
-    batch_step<Q, T><<<b->grid, 32 * (batch_tyi(Q) + 2), b->smem, b->stream>>>(b->d_doms, b->d_items, b->d_ctl);
+    batch_step<Q, T, S><<<b->grid, 32 * (batch_tyi(Q) + 2), b->smem, b->stream>>>(b->d_doms, b->d_items, b->d_ctl);
 }
 
 void launch_any(mrlbm_batch* b)
 {
     if (b->lattice == 19) {
-        if (b->storage == MRLBM_F32) launch<19, float>(b); else launch<19, __half>(b);
+        if (b->storage == MRLBM_F32) launch<19, float>(b);
+        else if (b->storage == MRLBM_F16U) launch<19, __half, F_SPLITU>(b);
+        else launch<19, __half>(b);
     } else {
-        if (b->storage == MRLBM_F32) launch<27, float>(b); else launch<27, __half>(b);
+        if (b->storage == MRLBM_F32) launch<27, float>(b);
+        else if (b->storage == MRLBM_F16U) launch<27, __half, F_SPLITU>(b);
+        else launch<27, __half>(b);
     }
 }
 
@@ -234,18 +238,27 @@ extern "C" mrlbm_status mrlbm_batch_create(int lattice, int storage, mrlbm_batch
     b->lattice = lattice;
     b->storage = storage;
     mrlbm_status st;
-    if (lattice == 19) st = storage == MRLBM_F32 ? set_attr<19, float>(b->smem) : set_attr<19, __half>(b->smem);
-    else st = storage == MRLBM_F32 ? set_attr<27, float>(b->smem) : set_attr<27, __half>(b->smem);
+    if (lattice == 19)
+        st = storage == MRLBM_F32    ? set_attr<19, float>(b->smem)
+             : storage == MRLBM_F16U ? set_attr<19, __half, F_SPLITU>(b->smem)
+                                     : set_attr<19, __half>(b->smem);
+    else
+        st = storage == MRLBM_F32    ? set_attr<27, float>(b->smem)
+             : storage == MRLBM_F16U ? set_attr<27, __half, F_SPLITU>(b->smem)
+                                     : set_attr<27, __half>(b->smem);
     if (st) { delete b; return st; }
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (lattice == 19)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, storage == MRLBM_F32 ? batch_step<19, float> : batch_step<19, __half>,
-                                                      32 * (batch_tyi(lattice) + 2), b->smem);
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, storage == MRLBM_F32 ? batch_step<27, float> : batch_step<27, __half>,
-                                                      32 * (batch_tyi(lattice) + 2), b->smem);
+    {
+        const void* k = lattice == 19 ? (storage == MRLBM_F32    ? (const void*)batch_step<19, float>
+                                         : storage == MRLBM_F16U ? (const void*)batch_step<19, __half, F_SPLITU>
+                                                                 : (const void*)batch_step<19, __half>)
+                                      : (storage == MRLBM_F32    ? (const void*)batch_step<27, float>
+                                         : storage == MRLBM_F16U ? (const void*)batch_step<27, __half, F_SPLITU>
+                                                                 : (const void*)batch_step<27, __half>);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 32 * (batch_tyi(lattice) + 2), b->smem);
+    }
     b->grid = sms * std::max(per_sm, 1);
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||

@@ -13,12 +13,12 @@ namespace mrlbm {
 // rows per CTA: the single-domain kernel's for wall domains (members share
 // its tensor maps; the batch's flag sets include walls)
 __host__ __device__ constexpr int batch_tyi(int q) { return TYI_WALL; }
-// moment pairs a ring slot holds: the largest flag set's (power law, + the
-// low words of 3u with split-velocity fp16 storage)
-template <typename T>
+// moment pairs a ring slot holds: the largest flag set's (power law, with
+// the split storage's low words when S = F_SPLITU)
+template <typename T, int S>
 __host__ __device__ constexpr int batch_npm()
 {
-    return sizeof(T) == 2 ? npairs_of(F_BC | F_POWERLAW | F_SPLITU) : npairs_of(F_BC | F_POWERLAW);
+    return npairs_of(F_BC | F_POWERLAW | S);
 }
 
 // Per-domain data the batched kernel needs; both parities are precomputed so
@@ -46,19 +46,23 @@ struct BatchCtl {
 
 template <int Q, typename T, int FLAGS>
 __device__ __forceinline__ bool batch_column(const StepArgs& a, const CUtensorMap* map, const BatchItem& it,
-                                             const ZSmem<Q, T, batch_tyi(Q), batch_npm<T>()>& sm, unsigned& g0)
+                                             const ZSmem<Q, T, batch_tyi(Q), batch_npm<T, FLAGS & F_SPLITU>()>& sm,
+                                             unsigned& g0)
 {
     return zmarch_column<Q, T, FLAGS, batch_tyi(Q)>(a, map, it.X0, it.Y0, it.z0, min(it.z0 + a.lz, a.nz), sm, g0);
 }
 
-template <int Q, typename T>
+// S = F_SPLITU for split-storage fp16 batches (their members' flag sets carry
+// it), else 0: one kernel per storage kind keeps each kernel's code and
+// register demand to the flag sets it can meet.
+template <int Q, typename T, int S = 0>
 __global__ void __launch_bounds__(32 * (batch_tyi(Q) + 2), 1)
     batch_step(const BatchDomain* __restrict__ doms, const BatchItem* __restrict__ items, BatchCtl* ctl)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ int s_item;
     __shared__ __align__(16) StepArgs s_args;
-    const ZSmem<Q, T, batch_tyi(Q), batch_npm<T>()> sm(smem);  // ring slots for the largest flag set
+    const ZSmem<Q, T, batch_tyi(Q), batch_npm<T, S>()> sm(smem);  // ring slots for the largest flag set
     zmarch_init_barriers(sm);
     const int step = *((volatile int*)&ctl->step);
     const int nitems = *((volatile int*)&ctl->nitems);
@@ -77,31 +81,13 @@ __global__ void __launch_bounds__(32 * (batch_tyi(Q) + 2), 1)
         __syncthreads();
         bool ok = true;
         switch (D.flags) {
-            case 0: ok = batch_column<Q, T, 0>(s_args, &D.map[par], item, sm, g0); break;
-            case F_BC: ok = batch_column<Q, T, F_BC>(s_args, &D.map[par], item, sm, g0); break;
-            case F_BC | F_FORCE: ok = batch_column<Q, T, F_BC | F_FORCE>(s_args, &D.map[par], item, sm, g0); break;
-            case F_BC | F_FORCE | F_POWERLAW:
-                ok = batch_column<Q, T, F_BC | F_FORCE | F_POWERLAW>(s_args, &D.map[par], item, sm, g0);
+            case S: ok = batch_column<Q, T, S>(s_args, &D.map[par], item, sm, g0); break;
+            case S | F_BC: ok = batch_column<Q, T, S | F_BC>(s_args, &D.map[par], item, sm, g0); break;
+            case S | F_BC | F_FORCE: ok = batch_column<Q, T, S | F_BC | F_FORCE>(s_args, &D.map[par], item, sm, g0); break;
+            case S | F_BC | F_FORCE | F_POWERLAW:
+                ok = batch_column<Q, T, S | F_BC | F_FORCE | F_POWERLAW>(s_args, &D.map[par], item, sm, g0);
                 break;
-            default:
-                // split-velocity fp16 members (rejected on the host for other storages)
-                if constexpr (sizeof(T) == 2) {
-                    switch (D.flags) {
-                        case F_SPLITU: ok = batch_column<Q, T, F_SPLITU>(s_args, &D.map[par], item, sm, g0); break;
-                        case F_SPLITU | F_BC:
-                            ok = batch_column<Q, T, F_SPLITU | F_BC>(s_args, &D.map[par], item, sm, g0);
-                            break;
-                        case F_SPLITU | F_BC | F_FORCE:
-                            ok = batch_column<Q, T, F_SPLITU | F_BC | F_FORCE>(s_args, &D.map[par], item, sm, g0);
-                            break;
-                        case F_SPLITU | F_BC | F_FORCE | F_POWERLAW:
-                            ok = batch_column<Q, T, F_SPLITU | F_BC | F_FORCE | F_POWERLAW>(s_args, &D.map[par], item,
-                                                                                          sm, g0);
-                            break;
-                        default: break;
-                    }
-                }
-                break;
+            default: break;  // rejected on the host when the domain joins
         }
         if (!ok) break;
     }

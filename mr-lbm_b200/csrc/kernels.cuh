@@ -62,7 +62,8 @@ enum : int {
 };
 
 // most stored moments per node: 10 flow moments + omega, or + C and its flux
-constexpr int NM_MAX = 14;
+// (split-velocity fp16 storage of a non-Newtonian flow: 11 moments + 4 low words)
+constexpr int NM_MAX = 15;
 
 // CTA geometry: 32 x TYI interior nodes of an (x, y) column (warp w < TYI is
 // row y = Y0 + w, lane l is x = X0 + l) plus two helper warps that produce
@@ -98,12 +99,56 @@ __host__ __device__ constexpr size_t smem_budget(int tyi)
 {
     return ctas_per_sm(tyi) == 1 ? 232448 : 233472 / ctas_per_sm(tyi) - 1024;
 }
+// stored moments and moment pairs of a flag set
+__host__ __device__ constexpr int nmoments_of(int flags)
+{
+    return ((flags & (F_POWERLAW | F_BINGHAM)) ? 11 : 10) + ((flags & F_THERMAL) ? 4 : 0) +
+           ((flags & F_SPLITU) ? ((flags & (F_POWERLAW | F_BINGHAM)) ? 4 : 3) : 0);
+}
+__host__ __device__ constexpr int npairs_of(int flags) { return (nmoments_of(flags) + 1) / 2; }
 // index of a tile height among the domain's tensor maps and z chunks
 __host__ __device__ constexpr int tile_kind(int tyi) { return tyi == TYI_BULK ? 0 : 1; }
 __host__ __device__ constexpr int tile_rows_of_kind(int kind) { return kind == 0 ? TYI_BULK : TYI_WALL; }
 constexpr uint8_t CLS_BULK = 0;
 constexpr uint8_t CLS_SOLID = 255;
 constexpr unsigned WAIT_LIMIT = 1u << 26;  // mbarrier polls before giving up (~seconds)
+
+// Bounds-check build (-DMRLBM_BOUNDS_CHECK, libmrlbm_check.so): every
+// shared-memory access of the step kernels is checked against the CTA's
+// regions (TMA ring, row exchanges, edge buffers), every global store and
+// node-class load against the padded field, before it happens; a bad access
+// is skipped and sets bit 1 of the device error word (bits 8-15: which kind
+// of access).  The exchange and edge buffers are also refilled with NaN after
+// every consumption (and at the start of a column), so a slot that a
+// consumption reads but the production before it did not write shows up as
+// NaN in the moments.  The default build has none of it.
+enum : int { BCK_STAGE = 1, BCK_EXCHANGE = 2, BCK_EDGE = 4, BCK_STORE = 8, BCK_CLASS = 16 };
+#ifdef MRLBM_BOUNDS_CHECK
+struct SmemBounds {
+    unsigned stage_lo, stage_hi, ex_lo, ex_hi, edge_lo, edge_hi;
+    int* err;
+};
+__shared__ SmemBounds g_bounds;
+__device__ __forceinline__ bool bounds_fail(int kind, int* err)
+{
+    atomicOr(err, 2 | (kind << 8));
+    return false;
+}
+__device__ __forceinline__ bool smem_ok(const void* p, int bytes, int kind)
+{
+    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    unsigned lo, hi;
+    if (kind == BCK_STAGE) { lo = g_bounds.stage_lo; hi = g_bounds.stage_hi; }
+    else if (kind == BCK_EXCHANGE) { lo = g_bounds.ex_lo; hi = g_bounds.ex_hi; }
+    else { lo = g_bounds.edge_lo; hi = g_bounds.edge_hi; }
+    return (a >= lo && a + (unsigned)bytes <= hi) ? true : bounds_fail(kind, g_bounds.err);
+}
+#define MRLBM_SMEM_OK(p, bytes, kind) smem_ok((p), (bytes), (kind))
+#define MRLBM_GLOBAL_OK(cond, kind, err) ((cond) ? true : bounds_fail((kind), (err)))
+#else
+#define MRLBM_SMEM_OK(p, bytes, kind) true
+#define MRLBM_GLOBAL_OK(cond, kind, err) true
+#endif
 
 // Moment-space wall BC data of one node class (octant mask + velocity index).
 // The BC is the linear system
@@ -694,7 +739,8 @@ __device__ __forceinline__ void ex_write(const float* f, float4* e4t)
                 else v.z = f[i];
             }
         });
-        e4t[ex_slot4(Q, G) * Exchange<Q, TYI>::plane] = v;
+        float4* d = e4t + ex_slot4(Q, G) * Exchange<Q, TYI>::plane;
+        if (MRLBM_SMEM_OK(d, 16, BCK_EXCHANGE)) *d = v;
     }
 }
 
@@ -712,7 +758,10 @@ __device__ __forceinline__ void ex_write_all(const float* f, float4* e4t, float*
     if constexpr (Q == 19) {
         static_for<1, Q>([&](auto I) {
             constexpr int i = I;
-            if constexpr (lat_cy(i) != 0 && !ex_packed(Q, i)) e1t[ex_scalar_slot(i) * Exchange<Q, TYI>::plane] = f[i];
+            if constexpr (lat_cy(i) != 0 && !ex_packed(Q, i)) {
+                float* d = e1t + ex_scalar_slot(i) * Exchange<Q, TYI>::plane;
+                if (MRLBM_SMEM_OK(d, 4, BCK_EXCHANGE)) *d = f[i];
+            }
         });
     }
 }
@@ -734,7 +783,10 @@ __device__ __forceinline__ void ex_write_sel(const float* f, float4* e4t, float*
             constexpr int i = I;
             if constexpr (lat_cy(i) != 0 && !ex_packed(Q, i) && (CX == 0 || lat_cx(i) == CX) &&
                           (CY == 0 || lat_cy(i) == CY))
-                e1t[ex_scalar_slot(i) * Exchange<Q, TYI>::plane] = f[i];
+            {
+                float* d = e1t + ex_scalar_slot(i) * Exchange<Q, TYI>::plane;
+                if (MRLBM_SMEM_OK(d, 4, BCK_EXCHANGE)) *d = f[i];
+            }
         });
     }
 }
@@ -753,7 +805,8 @@ __device__ __forceinline__ void ex_read(float* g, const float4* e4t)
 {
     if constexpr (ex_group_used<Q, G>()) {
         constexpr int cx = (G % 3) - 1, cy = G >= 3 ? 1 : -1;
-        const float4 v = e4t[ex_slot4(Q, G) * Exchange<Q, TYI>::plane - cy * EX_COLS - cx];
+        const float4* sp = e4t + ex_slot4(Q, G) * Exchange<Q, TYI>::plane - cy * EX_COLS - cx;
+        const float4 v = MRLBM_SMEM_OK(sp, 16, BCK_EXCHANGE) ? *sp : make_float4(0.f, 0.f, 0.f, 0.f);
         static_for<1, Q>([&](auto I) {
             constexpr int i = I;
             if constexpr (lat_cy(i) != 0 && ex_group(i) == G && ex_packed(Q, i))
@@ -779,7 +832,10 @@ __device__ __forceinline__ void gather_pops(float* g, const float4* e4t, const f
         static_for<1, Q>([&](auto I) {
             constexpr int i = I;
             if constexpr (lat_cy(i) != 0 && !ex_packed(Q, i))
-                g[i] = e1t[ex_scalar_slot(i) * Exchange<Q, TYI>::plane - lat_cy(i) * EX_COLS - lat_cx(i)];
+            {
+                const float* sp = e1t + ex_scalar_slot(i) * Exchange<Q, TYI>::plane - lat_cy(i) * EX_COLS - lat_cx(i);
+                g[i] = MRLBM_SMEM_OK(sp, 4, BCK_EXCHANGE) ? *sp : 0.f;
+            }
         });
     }
     static_for<0, Q>([&](auto I) {
@@ -796,34 +852,41 @@ __device__ __forceinline__ void gather_pops(float* g, const float4* e4t, const f
 
 // a node's stored moments (unscaled to the FP32 stored form) from its element
 // pair of moments 0, 1 in a TMA stage (pair p is 2 box_x<T>() elements further);
-// with split velocity (SPLIT) the last three stored words are the low parts
-// of 3u, added to the high parts in moments 1-3
-template <int NM, typename T, bool SPLIT = false>
+// with split storage (NML < NM) the stored words after the NML moments are the
+// low parts of 3u (and of omega, moment 10, when NM - NML = 4), added to the
+// high parts
+template <int NM, typename T, int NML = NM>
 __device__ __forceinline__ void stage_moments(const StepArgs& a, const T* sp, float* mc)
 {
 #pragma unroll
     for (int p = 0; p < (NM + 1) / 2; p++) {
-        const float2 v = Stor2<T>::lds(sp + p * 2 * box_x<T>());
+        const T* q = sp + p * 2 * box_x<T>();
+        const float2 v = MRLBM_SMEM_OK(q, 2 * (int)sizeof(T), BCK_STAGE) ? Stor2<T>::lds(q) : make_float2(0.f, 0.f);
         mc[2 * p] = scaled_storage<T>() ? v.x * a.iscale[2 * p] : v.x;
         if (2 * p + 1 < NM) mc[2 * p + 1] = scaled_storage<T>() ? v.y * a.iscale[2 * p + 1] : v.y;
     }
-    if constexpr (SPLIT) {
-        mc[1] += mc[NM - 3];
-        mc[2] += mc[NM - 2];
-        mc[3] += mc[NM - 1];
+    if constexpr (NML < NM) {
+        mc[1] += mc[NML];
+        mc[2] += mc[NML + 1];
+        mc[3] += mc[NML + 2];
+        if constexpr (NM - NML == 4) mc[10] += mc[NML + 3];
     }
 }
 
-// split velocity: the low words (moments NM-3 .. NM-1, FP32 before the
-// storage scaling) hold what the 16-bit high word of 3u (moments 1-3, stored
-// with scale[1..3]) rounds away
-template <int NM>
-__device__ __forceinline__ void split_velocity(const StepArgs& a, float* o)
+// split storage: the low words (stored words NML.., FP32 before the storage
+// scaling) hold what the 16-bit high words of 3u (moments 1-3, stored with
+// scale[1..3]) and of omega (moment 10, when NM - NML = 4) round away
+template <int NM, int NML>
+__device__ __forceinline__ void split_words(const StepArgs& a, float* o)
 {
 #pragma unroll
     for (int c = 0; c < 3; c++) {
         const float hi = __half2float(__float2half_rn(o[1 + c] * a.scale[1 + c])) * a.iscale[1 + c];
-        o[NM - 3 + c] = o[1 + c] - hi;
+        o[NML + c] = o[1 + c] - hi;
+    }
+    if constexpr (NM - NML == 4) {
+        const float hi = __half2float(__float2half_rn(o[10] * a.scale[10])) * a.iscale[10];
+        o[NML + 3] = o[10] - hi;
     }
 }
 
@@ -855,13 +918,13 @@ __device__ __forceinline__ void thermal_pops(const StepArgs& a, const float* mc,
 // 31 take their inward c_x members from the edge buffer then).
 // sp: this thread's element pair of moments 0, 1 in the plane's TMA stage;
 // e4t / e1t: this thread's exchange slots in the buffer this production writes.
-template <int Q, int NM, typename T, int TYI, bool TH = false, bool SPLIT = false>
+template <int Q, int NM, typename T, int TYI, bool TH = false, int NML = NM>
 __device__ __forceinline__ void prod_a(const StepArgs& a, const T* sp, float4* e4t, float* e1t, float (&gsh)[Q],
                                        float& om_node, float4* e4g = nullptr, float* e1g = nullptr,
                                        float* gshg = nullptr)
 {
     float mc[NM];
-    stage_moments<NM, T, SPLIT>(a, sp, mc);
+    stage_moments<NM, T, NML>(a, sp, mc);
     float f[Q];
     reconstruct<Q>(mc, a.rho0, f);
     ex_write_all<Q, TYI>(f, e4t, e1t);
@@ -873,7 +936,7 @@ __device__ __forceinline__ void prod_a(const StepArgs& a, const T* sp, float4* e
             else gsh[i] = f[i];
         }
     });
-    om_node = mc[(SPLIT ? NM - 3 : NM) - 1];   // omega (moment 10) when the viscosity is per node
+    om_node = mc[NML - 1];   // omega (moment 10) when the viscosity is per node
     if constexpr (TH) {
         float g[19];
         thermal_pops(a, mc, g);
@@ -898,7 +961,7 @@ __device__ __forceinline__ void prod_a(const StepArgs& a, const T* sp, float4* e
 // hp / ep: the halo-row and edge node's element pair of moments 0, 1 in the
 // stage; e4h / e1h and e4e / e1e: their exchange slots; edge: the edge buffer
 // of this side and parity (one float4 per exchange row).
-template <int Q, int NM, typename T, int TYI, int SIDE, bool TH = false, bool SPLIT = false>
+template <int Q, int NM, typename T, int TYI, int SIDE, bool TH = false, int NML = NM>
 __device__ __forceinline__ void prod_helper(const StepArgs& a, int lane, const T* hp, const T* ep, float4* e4h,
                                             float* e1h, float4* e4e, float* e1e, float4* edge, float4* e4hg = nullptr,
                                             float* e1hg = nullptr, float4* e4eg = nullptr, float* e1eg = nullptr,
@@ -906,7 +969,7 @@ __device__ __forceinline__ void prod_helper(const StepArgs& a, int lane, const T
 {
     {
         float mc[NM], f[Q];
-        stage_moments<NM, T, SPLIT>(a, hp, mc);
+        stage_moments<NM, T, NML>(a, hp, mc);
         reconstruct<Q>(mc, a.rho0, f);
         ex_write_sel<Q, TYI, 0, -SIDE>(f, e4h, e1h);
         if constexpr (TH) {
@@ -917,15 +980,15 @@ __device__ __forceinline__ void prod_helper(const StepArgs& a, int lane, const T
     }
     if (lane < TYI + 2) {
         float mc[NM], f[Q];
-        stage_moments<NM, T, SPLIT>(a, ep, mc);
+        stage_moments<NM, T, NML>(a, ep, mc);
         reconstruct<Q>(mc, a.rho0, f);
         ex_write_sel<Q, TYI, -SIDE, 0>(f, e4e, e1e);
-        edge[lane] = edge_pops<Q, -SIDE>(f);
+        if (MRLBM_SMEM_OK(edge + lane, 16, BCK_EDGE)) edge[lane] = edge_pops<Q, -SIDE>(f);
         if constexpr (TH) {
             float g[19];
             thermal_pops(a, mc, g);
             ex_write_sel<19, TYI, -SIDE, 0>(g, e4eg, e1eg);
-            edgeg[lane] = edge_pops<19, -SIDE>(g);
+            if (MRLBM_SMEM_OK(edgeg + lane, 16, BCK_EDGE)) edgeg[lane] = edge_pops<19, -SIDE>(g);
         }
     }
 }
@@ -992,6 +1055,7 @@ __device__ __forceinline__ void thermal_wall(const StepArgs& a, const BcClass* _
 template <typename T, int NM>
 __device__ __forceinline__ void store_node32(const StepArgs& a, unsigned idx, const float* o)
 {
+    if (!MRLBM_GLOBAL_OK((long long)idx < a.field, BCK_STORE, a.err)) return;
 #pragma unroll
     for (int p = 0; p < NM / 2; p++) Stor2<T>::st(reinterpret_cast<T*>(a.out_p[p]) + 2 * (size_t)idx, o[2 * p], o[2 * p + 1]);
     if constexpr (NM % 2 != 0) Stor<T>::st(reinterpret_cast<T*>(a.out_p[NM / 2]) + 2 * (size_t)idx, o[NM - 1]);
@@ -1000,6 +1064,7 @@ __device__ __forceinline__ void store_node32(const StepArgs& a, unsigned idx, co
 template <typename T, int NM>
 __device__ __forceinline__ void store_node(const StepArgs& a, long long idx, const float* o)
 {
+    if (!MRLBM_GLOBAL_OK(idx >= 0 && idx < a.field, BCK_STORE, a.err)) return;
     T* outp = reinterpret_cast<T*>(a.m_out);
 #pragma unroll
     for (int m = 0; m < NM; m++) Stor<T>::st(outp + mphys(m, idx, a.field), o[m]);
@@ -1026,7 +1091,8 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
     if constexpr (TH) {
         float gshg19[19];
         static_for<0, 19>([&](auto I) { gshg19[I] = gshg[I]; });
-        gather_pops<19, TYI>(gg, e4g, e1g, gshg19, *eetg, xlo, xhi);
+        const float4 eeg = MRLBM_SMEM_OK(eetg, 16, BCK_EDGE) ? *eetg : make_float4(0.f, 0.f, 0.f, 0.f);
+        gather_pops<19, TYI>(gg, e4g, e1g, gshg19, eeg, xlo, xhi);
         static_for<0, 19>([&](auto I) {
             constexpr int i = I;
             constexpr int slot = lat_cz_slot(19, i);
@@ -1036,7 +1102,8 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
         });
     }
     float g[Q];
-    gather_pops<Q, TYI>(g, e4t, e1t, gsh, *eet, xlo, xhi);
+    const float4 ee = MRLBM_SMEM_OK(eet, 16, BCK_EDGE) ? *eet : make_float4(0.f, 0.f, 0.f, 0.f);
+    gather_pops<Q, TYI>(g, e4t, e1t, gsh, ee, xlo, xhi);
 
     if constexpr (!LIGHT) {
         // consumptions 0 and 1 complete no plane: the column runs them LIGHT
@@ -1055,7 +1122,8 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
         const float omega = OMF ? om_out : a.omega0;
         const unsigned oidx = (unsigned)(zd + 1) * (unsigned)a.plane + (unsigned)((y + 1) * a.pitch + x + XOFF);
         uint8_t cls = CLS_BULK;
-        if constexpr ((FLAGS & F_BC) != 0) cls = live ? __ldg(a.cls + oidx) : CLS_SOLID;
+        if constexpr ((FLAGS & F_BC) != 0)
+            cls = (live && MRLBM_GLOBAL_OK((long long)oidx < a.field, BCK_CLASS, a.err)) ? __ldg(a.cls + oidx) : CLS_SOLID;
         float o[NM_MAX];
         float r, j[3], P[6];
         lattice_sums<Q>(p, r, j, P);
@@ -1111,7 +1179,7 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
             o[10] = tC;
             o[11] = tq[0]; o[12] = tq[1]; o[13] = tq[2];
         }
-        if constexpr ((FLAGS & F_SPLITU) != 0) split_velocity<NM>(a, o);
+        if constexpr ((FLAGS & F_SPLITU) != 0) split_words<NM, nmoments_of(FLAGS & ~F_SPLITU)>(a, o);
         if constexpr (scaled_storage<T>()) {
 #pragma unroll
             for (int m = 0; m < NM; m++) o[m] = o[m] * a.scale[m];
@@ -1214,13 +1282,7 @@ struct ZSmem {
     }
 };
 
-// stored moments and moment pairs of a flag set
-__host__ __device__ constexpr int nmoments_of(int flags)
-{
-    return ((flags & (F_POWERLAW | F_BINGHAM)) ? 11 : 10) + ((flags & F_THERMAL) ? 4 : 0) +
-           ((flags & F_SPLITU) ? 3 : 0);
-}
-__host__ __device__ constexpr int npairs_of(int flags) { return (nmoments_of(flags) + 1) / 2; }
+
 
 // Per-CTA pipeline state of the z-march over one column.  The TMA ring is
 // indexed by a running production count `g0 + k` so a persistent CTA can
@@ -1235,8 +1297,8 @@ struct ZMarch {
     static constexpr int NMID = lat_num_cz(Q, 0);
     static constexpr bool OMF = (FLAGS & (F_POWERLAW | F_BINGHAM)) != 0;
     static constexpr bool TH = (FLAGS & F_THERMAL) != 0;
-    static constexpr bool SPLIT = (FLAGS & F_SPLITU) != 0;
     static constexpr int NM = nmoments_of(FLAGS);
+    static constexpr int NML = nmoments_of(FLAGS & ~F_SPLITU);  // moments before the split storage's low words
     static constexpr int NP = (NM + 1) / 2;  // moment pairs in a stage row
     static constexpr int ROW = NP * 2 * BX;  // elements of a stage row
     static constexpr size_t stage_bytes = (size_t)NR * ROW * sizeof(T);
@@ -1292,9 +1354,33 @@ struct ZMarch {
         if (!ok) raise_timeout();
         __syncthreads();
         if (timed_out()) return false;
+#ifdef MRLBM_BOUNDS_CHECK
+        // the buffers consumption k-1 read are free until production k+1
+        // writes them: NaN in every slot first
+        poison((k + 1) & 1);
+        __syncthreads();
+#endif
         advance(k);
         return true;
     }
+#ifdef MRLBM_BOUNDS_CHECK
+    __device__ void poison(int par) const
+    {
+        const float nan = __int_as_float(0x7fc00000);
+        const float4 n4 = make_float4(nan, nan, nan, nan);
+        for (int i = threadIdx.x; i < EX::buf4; i += blockDim.x) sm.ex4[par * EX::buf4 + i] = n4;
+        for (int i = threadIdx.x; i < EX::buf1; i += blockDim.x) sm.ex1[par * EX::buf1 + i] = nan;
+        if constexpr (TH) {
+            for (int i = threadIdx.x; i < EXG::buf4; i += blockDim.x) sm.exg4[par * EXG::buf4 + i] = n4;
+            for (int i = threadIdx.x; i < EXG::buf1; i += blockDim.x) sm.exg1[par * EXG::buf1 + i] = nan;
+        }
+        for (int i = threadIdx.x; i < 2 * NR; i += blockDim.x) {
+            const int side = i / NR, er = i % NR;
+            sm.edge[(side * 2 + par) * NR + er] = n4;
+            if constexpr (TH) sm.edgeg[(side * 2 + par) * NR + er] = n4;
+        }
+    }
+#endif
 
     // ---- interior warps: row w, lane l = node (X0 + l, Y0 + w)
     struct Interior {
@@ -1331,10 +1417,10 @@ struct ZMarch {
                 a, j - 1, z0 - 2 + j, it.e4t[PAR ^ 1], it.e1t[PAR ^ 1], it.eet[PAR ^ 1], it.xlo, it.xhi, it.interior,
                 it.x, it.y, gsh_old, up, mid, om_out, it.e4g[PAR ^ 1], it.e1g[PAR ^ 1], it.eetg[PAR ^ 1], sg_old, upg,
                 midg);
-            prod_a<Q, NM, T, TYI, TH, SPLIT>(a, stage_base() + it.toff, it.e4t[PAR], it.e1t[PAR], gsh_new, om_par,
+            prod_a<Q, NM, T, TYI, TH, NML>(a, stage_base() + it.toff, it.e4t[PAR], it.e1t[PAR], gsh_new, om_par,
                                       it.e4g[PAR], it.e1g[PAR], sg_new);
         } else {
-            prod_a<Q, NM, T, TYI, TH, SPLIT>(a, stage_base() + it.toff, it.e4t[PAR], it.e1t[PAR], gsh_new, om_par,
+            prod_a<Q, NM, T, TYI, TH, NML>(a, stage_base() + it.toff, it.e4t[PAR], it.e1t[PAR], gsh_new, om_par,
                                       it.e4g[PAR], it.e1g[PAR], sg_new);
             prod_b<Q, NM, NUP, NMID, T, FLAGS, TYI, BCP, LIGHT>(
                 a, j - 1, z0 - 2 + j, it.e4t[PAR ^ 1], it.e1t[PAR ^ 1], it.eet[PAR ^ 1], it.xlo, it.xhi, it.interior,
@@ -1382,7 +1468,7 @@ struct ZMarch {
         {
             // prologue: production 0 only (exchange buffer 0)
             const bool ok = mbar_wait(&sm.bars[cs], cph);
-            prod_a<Q, NM, T, TYI, TH, SPLIT>(a, stage_base() + it.toff, it.e4t[0], it.e1t[0], gA, omA, it.e4g[0], it.e1g[0],
+            prod_a<Q, NM, T, TYI, TH, NML>(a, stage_base() + it.toff, it.e4t[0], it.e1t[0], gA, omA, it.e4g[0], it.e1g[0],
                                       sgA);
             if (!end_step(0, ok)) return 0;
         }
@@ -1439,7 +1525,7 @@ struct ZMarch {
             float* e1 = sm.ex1 + par * EX::buf1;
             float4* g4 = sm.exg4 + par * EXG::buf4;
             float* g1 = sm.exg1 + par * EXG::buf1;
-            prod_helper<Q, NM, T, TYI, SIDE, TH, SPLIT>(a, lane, st + hoff, st + eoff, e4 + sh, e1 + sh, e4 + se, e1 + se,
+            prod_helper<Q, NM, T, TYI, SIDE, TH, NML>(a, lane, st + hoff, st + eoff, e4 + sh, e1 + sh, e4 + se, e1 + se,
                                                  sm.edge + (side * 2 + par) * NR, g4 + sh, g1 + sh, g4 + se, g1 + se,
                                                  sm.edgeg + (side * 2 + par) * NR);
             if (!end_step(j, ok)) return j;
@@ -1465,6 +1551,23 @@ __device__ __forceinline__ bool zmarch_column(const StepArgs& a, const CUtensorM
     ZM zm{a, map, sm, g0, X0, Y0, z0, p0, zend - z0 + 2 /* planes z0-1 .. zend */, 0, 0u};
     zm.cs = zm.slot(0);
     zm.cph = zm.phase(0);
+#ifdef MRLBM_BOUNDS_CHECK
+    if (threadIdx.x == 0) {
+        using SMT = ZSmem<Q, T, TYI, NPM, (FLAGS & F_THERMAL) != 0>;
+        g_bounds.stage_lo = smem_u32(sm.stages);
+        g_bounds.stage_hi = smem_u32(sm.stages) + (unsigned)(SMT::NS * SMT::stage_max);
+        g_bounds.ex_lo = smem_u32(sm.ex4);
+        g_bounds.ex_hi = smem_u32(sm.edge);
+        g_bounds.edge_lo = smem_u32(sm.edge);
+        g_bounds.edge_hi = smem_u32(sm.edge) + (unsigned)SMT::edge_bytes;
+        g_bounds.err = a.err;
+    }
+    // no TMA load may land in the ring before the CTA's poison writes are done
+    __syncthreads();
+    zm.poison(0);
+    zm.poison(1);
+    __syncthreads();
+#endif
 
     if (threadIdx.x == ZM::TMA_THREAD) {
         // the ring was last read through the generic proxy (previous column)

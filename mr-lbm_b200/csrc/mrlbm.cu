@@ -201,7 +201,10 @@ static int moments_of(const mrlbm_desc& d)
 {
     return (d.rheology != MRLBM_NEWTONIAN ? 11 : 10) + (d.thermal ? 4 : 0);
 }
-static int stored_moments_of(const mrlbm_desc& d) { return moments_of(d) + (d.storage == MRLBM_F16U ? 3 : 0); }
+static int stored_moments_of(const mrlbm_desc& d)
+{
+    return moments_of(d) + (d.storage == MRLBM_F16U ? (d.rheology != MRLBM_NEWTONIAN ? 4 : 3) : 0);
+}
 
 // G_DIFF_FLUC_COEF from the thermal diffusivity with the reference's fixed
 // T_DIFF_REF = 1/6 and G_TAU = 3 T_DIFF_REF + 1/2
@@ -224,11 +227,12 @@ void mrlbm::storage_scales(int storage, int nm, float* scale, float* iscale)
             // range of fp16 (exact, no rounding from the scaling itself);
             // bf16 has fp32's exponent range and needs none
             s = k == 0 ? 256.0f : (k <= 3 ? 8.0f : (k <= 9 ? 64.0f : 1.0f));
-            // split velocity: the low words of 3u (stored after the nm
-            // moments) are what the high word rounds away, at most half an
-            // fp16 ulp of 8 * 3u, so 2^11 times the high word's scale keeps
-            // them in fp16's normal range
+            // split storage: the low words of 3u and omega (stored after the
+            // nm moments) are what the high word rounds away, at most half
+            // an fp16 ulp of the scaled value, so 2^11 times the high word's
+            // scale keeps them in fp16's normal range
             if (storage == MRLBM_F16U && k >= nm && k < nm + 3) s = 8.0f * 2048.0f;
+            if (storage == MRLBM_F16U && nm == 11 && k == nm + 3) s = 2048.0f;
         }
         scale[k] = s;
         iscale[k] = 1.0f / s;
@@ -565,6 +569,7 @@ static mrlbm_status run_init(mrlbm_domain* dom, InitArgs& a)
     a.plane = dom->plane; a.field = dom->field;
     a.nm = dom->nms;
     a.lo0 = dom->nms > dom->nm ? dom->nm : -1;
+    a.lom = dom->nms - dom->nm == 4 ? dom->nm + 3 : -1;
     a.qs = 19;  // the reference's D3Q19 second-moment sums (also on D3Q27)
     a.rho0 = (float)d.rho0;
     a.omega0 = (float)dom->omega0;
@@ -753,6 +758,9 @@ mrlbm_status mrlbm::check_device_error(mrlbm_domain* dom)
     CK(cudaStreamSynchronize(dom->stream));
     if (h) {
         CK(cudaMemsetAsync(dom->err, 0, sizeof(int), dom->stream));
+        if (h & 2)
+            return fail(MRLBM_EBOUNDS, "a step kernel skipped an out-of-range access (flag 0x%x: kinds 0x%x)", h,
+                        (h >> 8) & 0xff);
         return fail(MRLBM_ETIMEDOUT, "a step kernel gave up waiting for its tile loads (flag 0x%x)", h);
     }
     return MRLBM_OK;
@@ -859,6 +867,7 @@ static mrlbm_status convert(mrlbm_domain* dom, float* hbuf_out, const float* hbu
     a.plane = dom->plane; a.field = dom->field;
     a.nm = dom->nm;
     a.lo0 = dom->nms > dom->nm ? dom->nm : -1;
+    a.lom = dom->nms - dom->nm == 4 ? dom->nm + 3 : -1;
     a.mode = mode;
     memcpy(a.scale, dom->scale, sizeof(a.scale));
     memcpy(a.iscale, dom->iscale, sizeof(a.iscale));

@@ -13,7 +13,9 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libmrlbm.so")
+# MRLBM_LIBRARY may name another build of the library (the bounds-check
+# build libmrlbm_check.so); default: the in-tree libmrlbm.so
+LIB_PATH = os.environ.get("MRLBM_LIBRARY") or os.path.join(HERE, "libmrlbm.so")
 
 D3Q19, D3Q27 = 19, 27
 F32, F16, BF16, F16U = 0, 1, 2, 3  # F16U: fp16 with split (two-word) velocity
@@ -45,7 +47,7 @@ def THERMAL_INDEX(k):
 WEST, EAST, SOUTH, NORTH, BACK, FRONT = 0x55, 0xAA, 0x33, 0xCC, 0x0F, 0xF0
 
 STATUS = {0: "OK", 1: "EINVAL", 2: "ENOMEM", 3: "ECUDA", 4: "EIO", 5: "EDIVERGED", 6: "ETIMEDOUT",
-          7: "ENOTFOUND", 8: "EBUSY"}
+          7: "ENOTFOUND", 8: "EBUSY", 9: "ECANCELED", 10: "EBOUNDS"}
 
 
 class MrlbmError(RuntimeError):
@@ -198,6 +200,10 @@ def lib():
             "mrlbm_selftest_bounded_wait": [C.c_uint, C.POINTER(C.c_double)],
             "mrlbm_set_stream": [VP, VP],
             "mrlbm_set_z_chunk": [VP, C.c_int],
+            "mrlbm_nccl_unique_id": [VP],
+            "mrlbm_nccl_comm_init": [C.c_int, VP, C.c_int, C.POINTER(VP)],
+            "mrlbm_nccl_comm_destroy": [VP],
+            "mrlbm_zslab_exchange_nccl": [VP, VP, C.c_int, C.c_int],
             "mrlbm_get_z_chunk": [VP, C.POINTER(C.c_int)],
             "mrlbm_get_stream": [VP, C.POINTER(VP)],
             "mrlbm_zslab_plane": [VP, C.c_int, C.POINTER(ZPlane)],
@@ -579,6 +585,27 @@ def request_describe(req, storage=F16):
     nt = np.zeros((req.n, req.n, req.n), dtype=np.uint32)
     check(lib().mrlbm_request_describe(C.byref(req), storage, C.byref(d), nt.ctypes.data_as(C.POINTER(C.c_uint32))))
     return d, nt
+
+
+def nccl_unique_id():
+    """A 128-byte NCCL unique id (bytes) for mrlbm_nccl_comm_init on every rank."""
+    b = C.create_string_buffer(128)
+    check(lib().mrlbm_nccl_unique_id(C.cast(b, VP)))
+    return b.raw
+
+
+class NcclComm:
+    """A communicator of the library's NCCL (mrlbm_nccl_comm_init) on the current device."""
+
+    def __init__(self, nranks, uid, rank):
+        self.h = VP()
+        buf = C.create_string_buffer(bytes(uid), 128)
+        check(lib().mrlbm_nccl_comm_init(int(nranks), C.cast(buf, VP), int(rank), C.byref(self.h)))
+
+    def close(self):
+        if self.h:
+            check(lib().mrlbm_nccl_comm_destroy(self.h))
+            self.h = VP()
 
 
 class Server:

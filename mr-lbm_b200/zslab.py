@@ -17,10 +17,13 @@ Two drivers share the plan of the exchange:
   moves planes with device copies (``mrlbm_zslab_copy``), each slab on its own
   stream with event ordering;
 * ``ZSlabDomain.distributed(desc)`` owns the slab of this rank of
-  torch.distributed (one process per GPU, NCCL over NVLink): the planes are
-  sent and received in place, as views of the library's device buffers, in one
-  batch of point-to-point operations per step, queued on the stream the domain
-  launches on, so nothing waits on the host between steps.
+  torch.distributed (one process per GPU, NCCL over NVLink).  With an NCCL
+  process group the exchange is the library's own (mrlbm_zslab_exchange_nccl:
+  NCCL point-to-point operations in place, one group per step, queued on the
+  domain's stream, so nothing waits on the host between steps and no PyTorch
+  is on the data path; torch.distributed only hands the NCCL unique id to the
+  ranks).  ``exchange="torch"`` (and any non-NCCL group, e.g. gloo) sends the
+  planes as torch tensors viewing the library's buffers instead.
 
 Arrays are numpy, x fastest, global shapes (nz, ny, nx) and (nm, nz, ny, nx)
 as in ``mrlbm``.
@@ -181,12 +184,14 @@ class ZSlabDomain:
         return cls(desc, slabs, 0, parts, None, True)
 
     @classmethod
-    def distributed(cls, desc, group=None):
+    def distributed(cls, desc, group=None, exchange="library"):
         """The slab of this rank of torch.distributed (initialised by the
-        caller; one process per GPU with the device already selected).  The
-        domain launches on a torch stream of its own (`.stream`) and the
-        exchange's NCCL operations are queued on that stream, so steps and
-        exchanges are ordered on the device without host waits."""
+        caller; one process per GPU with the device already selected).
+        exchange="library" (NCCL groups): the library's NCCL driver on the
+        domain's own stream, its communicator made from a unique id that rank
+        0 broadcasts over the group.  exchange="torch" (and non-NCCL groups):
+        the domain launches on a torch stream of its own (`.stream`) and the
+        planes go as torch point-to-point operations queued on that stream."""
         import torch
         import torch.distributed as dist
 
@@ -194,10 +199,19 @@ class ZSlabDomain:
         parts = dist.get_world_size(group)
         z0, z1 = slab_bounds(desc.nz, parts)[rank]
         s = GpuSlab(desc, z0, z1)
-        stream = torch.cuda.Stream()
-        s.dom.set_stream(stream.cuda_stream)
         obj = cls(desc, [s], rank, parts, group, False)
-        obj.stream = stream
+        obj.comm = None
+        if exchange == "library" and dist.get_backend(group) == "nccl":
+            box = [mrlbm.nccl_unique_id() if rank == 0 else None]
+            dist.broadcast_object_list(box, src=dist.get_global_rank(group, 0) if group is not None else 0,
+                                       group=group)
+            obj.comm = mrlbm.NcclComm(parts, box[0], rank)
+            below, above = neighbours(rank, parts, obj.periodic_z)
+            obj.nccl_peers = (-1 if below is None else below, -1 if above is None else above)
+        else:
+            stream = torch.cuda.Stream()
+            s.dom.set_stream(stream.cuda_stream)
+            obj.stream = stream
         return obj
 
     # -- setup (global arrays; each slab takes its planes)
@@ -231,6 +245,9 @@ class ZSlabDomain:
                     if op in ("send", "copy"):
                         dst = self.slabs[peer] if op == "send" else s
                         mrlbm.check(mrlbm.lib().mrlbm_zslab_copy(s.dom.h, which, dst.dom.h, GHOST_OF[direction]))
+        elif self.comm is not None:
+            below, above = self.nccl_peers
+            mrlbm.check(mrlbm.lib().mrlbm_zslab_exchange_nccl(self.slabs[0].dom.h, self.comm.h, below, above))
         else:
             import torch
 
@@ -278,6 +295,10 @@ class ZSlabDomain:
     def close(self):
         for s in self.slabs:
             if not self.local_mode:
+                s.dom.synchronize()
                 s.dom.set_stream(None)
             s.close()
         self.slabs = []
+        if getattr(self, "comm", None) is not None:
+            self.comm.close()
+            self.comm = None

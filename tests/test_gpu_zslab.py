@@ -158,7 +158,7 @@ def test_one_nccl_rank_on_torch_stream():
         mono.step(16)
         want, ws = mono.moments(), mono.sums()
         mono.close()
-        zs = zslab.ZSlabDomain.distributed(d)
+        zs = zslab.ZSlabDomain.distributed(d, exchange="torch")
         assert zs.slabs[0].dom.get_stream() == zs.stream.cuda_stream != 0
         zs.init_flow(rho, *u)
         zs.step(16)
@@ -171,6 +171,61 @@ def test_one_nccl_rank_on_torch_stream():
     finally:
         dist.destroy_process_group()
 
+
+
+def test_one_rank_library_nccl_exchange():
+    """The library's own NCCL driver (mrlbm_zslab_exchange_nccl), one rank:
+    a single periodic slab is its own neighbour below and above, so each
+    step's exchange is an NCCL send/receive to itself of both boundary
+    planes; the result equals the undivided periodic domain bit for bit.
+    Bootstrapped through torch.distributed (unique id broadcast) and, second,
+    with no torch at all (mrlbm_nccl_unique_id / mrlbm_nccl_comm_init)."""
+    import datetime
+    import socket
+
+    import torch
+    import torch.distributed as dist
+
+    d = mrlbm.make_desc(48, 32, 24, lattice=mrlbm.D3Q27, tau=0.57)
+    rho, u = _random_flow((24, 32, 48), 13)
+    mono = mrlbm.Domain(d)
+    mono.init_flow(rho, *u)
+    mono.step(12)
+    want = mono.moments()
+    mono.close()
+
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % port, rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        zs = zslab.ZSlabDomain.distributed(d)
+        assert zs.comm is not None and zs.nccl_peers == (0, 0)
+        zs.init_flow(rho, *u)
+        zs.step(12)
+        got = zs.moments()
+        zs.close()
+        assert np.array_equal(got, want)
+    finally:
+        dist.destroy_process_group()
+
+    # no torch on any path: the id and the communicator from the library
+    comm = mrlbm.NcclComm(1, mrlbm.nccl_unique_id(), 0)
+    slab = mrlbm.Domain(zslab.slab_desc(d, 0, 24))
+    slab.init_flow(rho, *u)
+    L = mrlbm.lib()
+    mrlbm.check(L.mrlbm_zslab_exchange_nccl(slab.h, comm.h, 0, 0))
+    for _ in range(12):
+        slab.step(1)
+        mrlbm.check(L.mrlbm_zslab_exchange_nccl(slab.h, comm.h, 0, 0))
+    got2 = slab.moments()
+    slab.synchronize()
+    slab.close()
+    comm.close()
+    assert np.array_equal(got2, want)
 
 
 def test_outflow_channel_with_a_one_plane_top_slab():
