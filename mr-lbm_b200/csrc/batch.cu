@@ -42,10 +42,16 @@ struct mrlbm_batch {
 
 namespace {
 
+// the batch kernel's rows per CTA for the batch's lattice and storage
+int batch_rows(const mrlbm_batch* b)
+{
+    return batch_tyi(b->lattice, b->storage == MRLBM_F16U ? F_SPLITU : 0);
+}
+
 template <int Q, typename T, int S = 0>
 mrlbm_status set_attr(size_t& smem)
 {
-    smem = ZSmem<Q, T, batch_tyi(Q), batch_npm<T, S>()>::bytes;
+    smem = ZSmem<Q, T, batch_tyi(Q, S), batch_npm<T, S>(), false, BATCH_STATIC_SMEM>::bytes;
     cudaError_t e = cudaFuncSetAttribute(batch_step<Q, T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return fail(MRLBM_ECUDA, "batch attribute: %s", cudaGetErrorString(e));
     return MRLBM_OK;
@@ -54,7 +60,7 @@ mrlbm_status set_attr(size_t& smem)
 template <int Q, typename T, int S = 0>
 void launch(mrlbm_batch* b)
 {
-    batch_step<Q, T, S><<<b->grid, 32 * (batch_tyi(Q) + 2), b->smem, b->stream>>>(b->d_doms, b->d_items, b->d_ctl);
+    batch_step<Q, T, S><<<b->grid, 32 * (batch_tyi(Q, S) + 2), b->smem, b->stream>>>(b->d_doms, b->d_items, b->d_ctl);
 }
 
 void launch_any(mrlbm_batch* b)
@@ -133,10 +139,10 @@ mrlbm_status refresh(mrlbm_batch* b)
             return fail(MRLBM_EINVAL, "batch member %d: physics flag set %d not supported in batches", id, hd[id].flags);
         if (dom->has_outflow)
             return fail(MRLBM_EINVAL, "batch member %d: outflow walls are not supported in batches", id);
-        hd[id].map[0] = dom->tmap[0][tile_kind(batch_tyi(dom->q))];
-        hd[id].map[1] = dom->tmap[1][tile_kind(batch_tyi(dom->q))];
+        const int ty = batch_rows(b);
+        hd[id].map[0] = dom->tmap[0][tile_kind(ty)];
+        hd[id].map[1] = dom->tmap[1][tile_kind(ty)];
         hd[id].parity_offset = b->offsets[id];
-        const int ty = batch_tyi(dom->q);
         const int gx = (dom->d.nx + TILE_X - 1) / TILE_X, gy = (dom->d.ny + ty - 1) / ty;
         for (int z0 = 0; z0 < dom->d.nz; z0 += dom->lz)
             for (int by = 0; by < gy; by++)
@@ -257,7 +263,7 @@ extern "C" mrlbm_status mrlbm_batch_create(int lattice, int storage, mrlbm_batch
                                       : (storage == MRLBM_F32    ? (const void*)batch_step<27, float>
                                          : storage == MRLBM_F16U ? (const void*)batch_step<27, __half, F_SPLITU>
                                                                  : (const void*)batch_step<27, __half>);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 32 * (batch_tyi(lattice) + 2), b->smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 32 * (batch_rows(b) + 2), b->smem);
     }
     b->grid = sms * std::max(per_sm, 1);
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||

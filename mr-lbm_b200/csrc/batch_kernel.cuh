@@ -10,9 +10,13 @@
 
 namespace mrlbm {
 
-// rows per CTA: the single-domain kernel's for wall domains (members share
-// its tensor maps; the batch's flag sets include walls)
-__host__ __device__ constexpr int batch_tyi(int q) { return TYI_WALL; }
+// rows per CTA (members share the single-domain kernel's tensor maps of that
+// height): 8, two CTAs per SM, except D3Q27 split-velocity fp16 batches (S =
+// F_SPLITU), whose 15 stored words of a power-law member spill at 8 rows
+__host__ __device__ constexpr int batch_tyi(int q, int s) { return (q == 27 && s != 0) ? TYI_WALL : TYI_BULK; }
+// static shared memory of the batch kernel (the work item and its step
+// arguments), kept out of the ring's share
+constexpr int BATCH_STATIC_SMEM = 512;
 // moment pairs a ring slot holds: the largest flag set's (power law, with
 // the split storage's low words when S = F_SPLITU)
 template <typename T, int S>
@@ -45,24 +49,28 @@ struct BatchCtl {
 };
 
 template <int Q, typename T, int FLAGS>
-__device__ __forceinline__ bool batch_column(const StepArgs& a, const CUtensorMap* map, const BatchItem& it,
-                                             const ZSmem<Q, T, batch_tyi(Q), batch_npm<T, FLAGS & F_SPLITU>()>& sm,
-                                             unsigned& g0)
+__device__ __forceinline__ bool batch_column(
+    const StepArgs& a, const CUtensorMap* map, const BatchItem& it,
+    const ZSmem<Q, T, batch_tyi(Q, FLAGS & F_SPLITU), batch_npm<T, FLAGS & F_SPLITU>(), false, BATCH_STATIC_SMEM>& sm,
+    unsigned& g0)
 {
-    return zmarch_column<Q, T, FLAGS, batch_tyi(Q)>(a, map, it.X0, it.Y0, it.z0, min(it.z0 + a.lz, a.nz), sm, g0);
+    return zmarch_column<Q, T, FLAGS, batch_tyi(Q, FLAGS & F_SPLITU)>(a, map, it.X0, it.Y0, it.z0,
+                                                                      min(it.z0 + a.lz, a.nz), sm, g0);
 }
 
 // S = F_SPLITU for split-storage fp16 batches (their members' flag sets carry
 // it), else 0: one kernel per storage kind keeps each kernel's code and
 // register demand to the flag sets it can meet.
 template <int Q, typename T, int S = 0>
-__global__ void __launch_bounds__(32 * (batch_tyi(Q) + 2), 1)
+__global__ void __launch_bounds__(32 * (batch_tyi(Q, S) + 2), ctas_per_sm(batch_tyi(Q, S)))
     batch_step(const BatchDomain* __restrict__ doms, const BatchItem* __restrict__ items, BatchCtl* ctl)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ int s_item;
     __shared__ __align__(16) StepArgs s_args;
-    const ZSmem<Q, T, batch_tyi(Q), batch_npm<T, S>()> sm(smem);  // ring slots for the largest flag set
+    static_assert(sizeof(StepArgs) + 16 <= BATCH_STATIC_SMEM, "batch static shared memory");
+    // ring slots for the largest flag set
+    const ZSmem<Q, T, batch_tyi(Q, S), batch_npm<T, S>(), false, BATCH_STATIC_SMEM> sm(smem);
     zmarch_init_barriers(sm);
     const int step = *((volatile int*)&ctl->step);
     const int nitems = *((volatile int*)&ctl->nitems);

@@ -82,12 +82,13 @@ __host__ __device__ constexpr int box_x_nodes(int esize) { return esize == 4 ? 3
 // memory (4 measured 1-3 % faster than 3), else 3 (or 2)
 constexpr int NSTAGE_MAX = 4;
 // interior rows per CTA: 8 (two CTAs of 10 warps per SM, up to 102 registers
-// a thread) for the bulk-only flag sets, 14 (one CTA of 16 warps, up to 128
-// registers) for the heavier wall, non-Newtonian and thermal sets
+// a thread) for every flow-only set, walls and non-Newtonian viscosity
+// included; 14 (one CTA of 16 warps, up to 128 registers) for the thermal
+// sets, whose second population pipeline needs them
 constexpr int TYI_BULK = 8, TYI_WALL = 14;
 __host__ __device__ constexpr int tile_rows(int flags)
 {
-    return (flags & (F_BC | F_POWERLAW | F_BINGHAM | F_THERMAL)) ? TYI_WALL : TYI_BULK;
+    return (flags & F_THERMAL) ? TYI_WALL : TYI_BULK;
 }
 // CTAs resident per SM: two for short columns (their per-plane barriers
 // interleave, which measured 2-3 % faster for 8 rows than one CTA of 16), else one
@@ -407,68 +408,38 @@ __device__ __forceinline__ void bc_known_sums(uint32_t known, const float* p, fl
 // mac = rho, u (unscaled), Pi_hat (unscaled xx,xy,xz,yy,yz,zz) from the
 // known-set moment system of class c (the wall-node closed forms of the
 // reference's bc_definition.inc, e.g. src/cases/lidDrivenCavity_3D/
-// bc_definition.inc:637-663, solved generically).
+// bc_definition.inc:637-663, solved generically).  The class words are read
+// one at a time: read as 16-byte vectors they all issue up front and spill at
+// the 102 registers a thread of the two-CTA wall kernels may use.
 template <int Q>
 __device__ __forceinline__ void bc_moments(const BcClass* __restrict__ c, const float* p, float omega,
                                            float omega0, float* mac)
 {
-    float b[7], X[7], u[3];
-    float dot = 0.f;
+    float b[7], X[7];
+    bc_known_sums<Q>(__ldg(&c->known), p, b);
+#pragma unroll
+    for (int r = 0; r < 7; r++) {
+        float acc = 0.f;
+#pragma unroll
+        for (int k = 0; k < 7; k++) acc = fmaf(__ldg(&c->ainv[r * 7 + k]), b[k], acc);
+        X[r] = acc;
+    }
+    // per-node omega (non-Newtonian): Sherman-Morrison update of A(omega0)^-1;
+    // a Newtonian domain (omega == omega0) reads none of its words
     const float dw = omega - omega0;
-    if constexpr (Q == 19) {
-        // the class's words (ainv 0-48, v 49-55, qa 56-62, s 63, u 64-66,
-        // known 67) in 17 vector loads streamed into the solve (measured 13 %
-        // faster on a 128^3 cavity); the D3Q27 kernels keep scalar loads,
-        // whose lower register need avoids spills there
-        const float4* c4 = reinterpret_cast<const float4*>(c);
-        const float4 tail = __ldg(c4 + 16);
-        bc_known_sums<Q>(__float_as_uint(tail.w), p, b);
-        u[0] = tail.x; u[1] = tail.y; u[2] = tail.z;
+    if (dw != 0.f) {
+        float dot = 0.f;
 #pragma unroll
-        for (int r = 0; r < 7; r++) X[r] = 0.f;
-        float V[7], sv = 0.f;
-        auto use = [&](auto E, float val) {
-            constexpr int e = E;
-            if constexpr (e < 49) X[e / 7] = fmaf(val, b[e % 7], X[e / 7]);
-            else if constexpr (e < 56) V[e - 49] = val;
-            else if constexpr (e < 63) dot = fmaf(val, b[e - 56], dot);
-            else sv = val;
-        };
-        static_for<0, 16>([&](auto K) {
-            constexpr int k = K;
-            const float4 t = __ldg(c4 + k);
-            use(std::integral_constant<int, 4 * k>{}, t.x);
-            use(std::integral_constant<int, 4 * k + 1>{}, t.y);
-            use(std::integral_constant<int, 4 * k + 2>{}, t.z);
-            use(std::integral_constant<int, 4 * k + 3>{}, t.w);
-        });
-        if (dw != 0.f) {
-            const float corr = dw * dot / (1.0f + dw * sv);
+        for (int r = 0; r < 7; r++) dot = fmaf(__ldg(&c->qa[r]), b[r], dot);
+        const float corr = dw * dot / (1.0f + dw * __ldg(&c->s));
 #pragma unroll
-            for (int r = 0; r < 7; r++) X[r] = fmaf(-corr, V[r], X[r]);
-        }
-    } else {
-        bc_known_sums<Q>(__ldg(&c->known), p, b);
-#pragma unroll
-        for (int r = 0; r < 7; r++) {
-            float acc = 0.f;
-#pragma unroll
-            for (int k = 0; k < 7; k++) acc = fmaf(__ldg(&c->ainv[r * 7 + k]), b[k], acc);
-            X[r] = acc;
-            dot = fmaf(__ldg(&c->qa[r]), b[r], dot);
-        }
-        if (dw != 0.f) {
-            const float corr = dw * dot / (1.0f + dw * __ldg(&c->s));
-#pragma unroll
-            for (int r = 0; r < 7; r++) X[r] = fmaf(-corr, __ldg(&c->v[r]), X[r]);
-        }
-        u[0] = __ldg(&c->u[0]); u[1] = __ldg(&c->u[1]); u[2] = __ldg(&c->u[2]);
+        for (int r = 0; r < 7; r++) X[r] = fmaf(-corr, __ldg(&c->v[r]), X[r]);
     }
     const float rho = X[0], ir = 1.0f / rho;
     mac[0] = rho;
-    mac[1] = u[0];
-    mac[2] = u[1];
-    mac[3] = u[2];
+    mac[1] = __ldg(&c->u[0]);
+    mac[2] = __ldg(&c->u[1]);
+    mac[3] = __ldg(&c->u[2]);
 #pragma unroll
     for (int k = 0; k < 6; k++) mac[4 + k] = X[1 + k] * ir;
 }
@@ -557,14 +528,27 @@ __device__ __forceinline__ float nnf_powerlaw(float omega_old, float smag, float
 {
     if (smag < 1e-6f) return 0.f;
     float omega = omega_old;
-    const float a = K * powf(smag / (rho0 * (1.0f / 3.0f)), n);
+    // powers of positive bases on the special-function unit (__powf:
+    // 2^(y log2 x)), with omega^(n-1) as omega^n / omega: one power an
+    // iteration instead of two full powf.  omega = 0 (a node the cut-off
+    // stopped in an earlier step) keeps powf's limits: 0^(n-1) is +inf for
+    // n < 1, so the step vanishes and omega stays 0, as in the reference.
+    const float a = K * __powf(smag / (rho0 * (1.0f / 3.0f)), n);
     const float b = 0.5f * smag, c = -smag;
     for (int it = 0; it < 7; it++) {
-        const float on = powf(omega, n);
-        const float fx = a * on + b * omega + c;
-        const float dfx = a * n * powf(omega, n - 1.0f) + b;
-        if (fabsf(fx / dfx) < 1e-6f) break;
-        omega = omega - fx / dfx;
+        float on, on1;
+        if (omega > 0.f) {
+            on = __powf(omega, n);
+            on1 = on / omega;
+        } else {
+            on = powf(omega, n);
+            on1 = powf(omega, n - 1.0f);
+        }
+        const float fx = fmaf(a, on, fmaf(b, omega, c));
+        const float dfx = fmaf(a * n, on1, b);
+        const float dx = fx / dfx;
+        if (fabsf(dx) < 1e-6f) break;
+        omega = omega - dx;
     }
     return omega;
 }
@@ -578,27 +562,29 @@ __device__ __forceinline__ void collide_scaled(const StepArgs& a, float rho, flo
                                                float mxy, float mxz, float myy, float myz, float mzz, float omega,
                                                float* out, float Fx, float Fy, float Fz)
 {
+    // every multiply-add is written as fmaf: the same bits wherever the
+    // collision is inlined, whichever product the compiler would otherwise fuse
     const float t_om = 1.0f - omega, om_d2 = 0.5f * omega;
     if constexpr ((FLAGS & F_FORCE) != 0) {
         const float ir = 1.0f / rho;
         const float tt_om = 1.0f - 0.5f * omega;
-        ux += 3.0f * ir * Fx;
-        uy += 3.0f * ir * Fy;
-        uz += 3.0f * ir * Fz;
+        ux = fmaf(3.0f * ir, Fx, ux);
+        uy = fmaf(3.0f * ir, Fy, uy);
+        uz = fmaf(3.0f * ir, Fz, uz);
         const float c15 = 1.5f * ir * tt_om, c3 = 3.0f * tt_om * ir;
-        mxx = t_om * mxx + om_d2 * ux * ux + c15 * (2.0f * Fx * ux);
-        myy = t_om * myy + om_d2 * uy * uy + c15 * (2.0f * Fy * uy);
-        mzz = t_om * mzz + om_d2 * uz * uz + c15 * (2.0f * Fz * uz);
-        mxy = t_om * mxy + omega * ux * uy + c3 * (Fx * uy + Fy * ux);
-        mxz = t_om * mxz + omega * ux * uz + c3 * (Fx * uz + Fz * ux);
-        myz = t_om * myz + omega * uy * uz + c3 * (Fy * uz + Fz * uy);
+        mxx = fmaf(c15, 2.0f * Fx * ux, fmaf(t_om, mxx, om_d2 * ux * ux));
+        myy = fmaf(c15, 2.0f * Fy * uy, fmaf(t_om, myy, om_d2 * uy * uy));
+        mzz = fmaf(c15, 2.0f * Fz * uz, fmaf(t_om, mzz, om_d2 * uz * uz));
+        mxy = fmaf(c3, fmaf(Fx, uy, Fy * ux), fmaf(t_om, mxy, omega * ux * uy));
+        mxz = fmaf(c3, fmaf(Fx, uz, Fz * ux), fmaf(t_om, mxz, omega * ux * uz));
+        myz = fmaf(c3, fmaf(Fy, uz, Fz * uy), fmaf(t_om, myz, omega * uy * uz));
     } else {
-        mxx = t_om * mxx + om_d2 * ux * ux;
-        myy = t_om * myy + om_d2 * uy * uy;
-        mzz = t_om * mzz + om_d2 * uz * uz;
-        mxy = t_om * mxy + omega * ux * uy;
-        mxz = t_om * mxz + omega * ux * uz;
-        myz = t_om * myz + omega * uy * uz;
+        mxx = fmaf(t_om, mxx, om_d2 * ux * ux);
+        myy = fmaf(t_om, myy, om_d2 * uy * uy);
+        mzz = fmaf(t_om, mzz, om_d2 * uz * uz);
+        mxy = fmaf(t_om, mxy, omega * ux * uy);
+        mxz = fmaf(t_om, mxz, omega * ux * uz);
+        myz = fmaf(t_om, myz, omega * uy * uz);
     }
     out[0] = rho - a.rho0;
     out[1] = ux; out[2] = uy; out[3] = uz;
@@ -1243,7 +1229,7 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
 // (kernels that switch between flag sets at run time size them for the
 // largest set), and the ring has NSTAGE_MAX stages when they fit next to the
 // exchange buffers, else fewer.
-template <int Q, typename T, int TYI, int NPM, bool TH = false>
+template <int Q, typename T, int TYI, int NPM, bool TH = false, int RESERVE = 0>
 struct ZSmem {
     static constexpr int NR = TYI + 2;  // stage rows = exchange rows
     static constexpr size_t stage_max = ((size_t)NR * NPM * 2 * box_x<T>() * sizeof(T) + 127) / 128 * 128;
@@ -1255,7 +1241,8 @@ struct ZSmem {
     static constexpr int edge_n = 2 * 2 * NR;
     static constexpr size_t edge_bytes = (size_t)(TH ? 2 : 1) * edge_n * 16;
     static constexpr size_t fixed = 128 + ex_bytes + edge_bytes;
-    static constexpr size_t budget = smem_budget(TYI);
+    // RESERVE: the kernel's static shared memory, which the CTA's share holds too
+    static constexpr size_t budget = smem_budget(TYI) - RESERVE;
     static constexpr int NS = fixed + NSTAGE_MAX * stage_max <= budget         ? NSTAGE_MAX
                               : fixed + (NSTAGE_MAX - 1) * stage_max <= budget ? NSTAGE_MAX - 1
                                                                                : NSTAGE_MAX - 2;
@@ -1289,7 +1276,7 @@ struct ZSmem {
 // chain columns without re-initialising its mbarriers.  Warps 0 .. TYI-1 run
 // the interior pipeline (interior_loop), warps TYI and TYI+1 the helper one
 // (helper_loop); both take the same barriers in the same order.
-template <int Q, typename T, int FLAGS, int TYI, typename BCP, int NPM>
+template <int Q, typename T, int FLAGS, int TYI, typename BCP, int NPM, int RES = 0>
 struct ZMarch {
     static constexpr int NR = TYI + 2;
     static constexpr int BX = box_x<T>();
@@ -1304,7 +1291,7 @@ struct ZMarch {
     static constexpr size_t stage_bytes = (size_t)NR * ROW * sizeof(T);
     using EX = Exchange<Q, TYI>;
     using EXG = Exchange<19, TYI>;
-    using SM = ZSmem<Q, T, TYI, NPM, TH>;
+    using SM = ZSmem<Q, T, TYI, NPM, TH, RES>;
     static constexpr int NS = SM::NS;
     static constexpr int TMA_THREAD = 32 * TYI;  // lane 0 of the bottom helper
     static_assert(NP <= NPM, "ring slots sized for fewer moment pairs");
@@ -1537,12 +1524,12 @@ struct ZMarch {
 // One column (X0, Y0) x planes [z0, zend) of one domain.  g0 is the CTA's
 // running production count (advanced by the column's productions).  Returns
 // false when a bounded wait timed out (the CTA must stop).
-template <int Q, typename T, int FLAGS, int TYI, typename BCP = TableBC, int NPM>
+template <int Q, typename T, int FLAGS, int TYI, typename BCP = TableBC, int NPM, int RES>
 __device__ __forceinline__ bool zmarch_column(const StepArgs& a, const CUtensorMap* map, int X0, int Y0, int z0,
-                                              int zend, const ZSmem<Q, T, TYI, NPM, (FLAGS & F_THERMAL) != 0>& sm,
+                                              int zend, const ZSmem<Q, T, TYI, NPM, (FLAGS & F_THERMAL) != 0, RES>& sm,
                                               unsigned& g0)
 {
-    using ZM = ZMarch<Q, T, FLAGS, TYI, BCP, NPM>;
+    using ZM = ZMarch<Q, T, FLAGS, TYI, BCP, NPM, RES>;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     // aligned box start (padded column): the TMA x coordinate, 2 elements a
     // node, must be a multiple of 16 bytes
@@ -1553,7 +1540,7 @@ __device__ __forceinline__ bool zmarch_column(const StepArgs& a, const CUtensorM
     zm.cph = zm.phase(0);
 #ifdef MRLBM_BOUNDS_CHECK
     if (threadIdx.x == 0) {
-        using SMT = ZSmem<Q, T, TYI, NPM, (FLAGS & F_THERMAL) != 0>;
+        using SMT = ZSmem<Q, T, TYI, NPM, (FLAGS & F_THERMAL) != 0, RES>;
         g_bounds.stage_lo = smem_u32(sm.stages);
         g_bounds.stage_hi = smem_u32(sm.stages) + (unsigned)(SMT::NS * SMT::stage_max);
         g_bounds.ex_lo = smem_u32(sm.ex4);
@@ -1594,12 +1581,12 @@ __device__ __forceinline__ bool zmarch_column(const StepArgs& a, const CUtensorM
     return true;
 }
 
-template <int Q, typename T, int TYI, int NPM, bool TH>
-__device__ __forceinline__ void zmarch_init_barriers(const ZSmem<Q, T, TYI, NPM, TH>& sm)
+template <int Q, typename T, int TYI, int NPM, bool TH, int RES>
+__device__ __forceinline__ void zmarch_init_barriers(const ZSmem<Q, T, TYI, NPM, TH, RES>& sm)
 {
     if (threadIdx.x == 0) {
         *reinterpret_cast<int*>(sm.bars + NSTAGE_MAX) = 0;  // the timeout flag
-        for (int s = 0; s < ZSmem<Q, T, TYI, NPM, TH>::NS; s++) mbar_init(&sm.bars[s], 1);
+        for (int s = 0; s < ZSmem<Q, T, TYI, NPM, TH, RES>::NS; s++) mbar_init(&sm.bars[s], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();

@@ -47,7 +47,8 @@ def cases():
         nx, ny, nz = shape
         out["bulk_%dx%dx%d_q%d_s%d" % (nx, ny, nz, q, st)] = lambda nx=nx, ny=ny, nz=nz, q=q, st=st: _run(
             mrlbm.make_desc(nx, ny, nz, lattice=q, storage=st, tau=0.7))
-    for shape, q, st in [((33, 15, 7), 19, mrlbm.F32), ((32, 14, 9), 27, mrlbm.F32), ((29, 13, 6), 19, mrlbm.F16U)]:
+    for shape, q, st in [((33, 15, 7), 19, mrlbm.F32), ((32, 14, 9), 27, mrlbm.F32), ((29, 13, 6), 19, mrlbm.F16U),
+                         ((34, 8, 5), 27, mrlbm.F32), ((31, 17, 3), 19, mrlbm.BF16)]:
         nx, ny, nz = shape
 
         def cav(nx=nx, ny=ny, nz=nz, q=q, st=st):
