@@ -624,6 +624,38 @@ def run_thermal_workload(args):
     return 0
 
 
+def run_cavity_workload(args):
+    """Walled domain: the lid-driven cavity of src/cases/lidDrivenCavity_3D
+    (wall classes on all six faces, the lid moving at 0.05, Re 100) at
+    --cavity-n^3, D3Q19 by default (--cavity-lattice), FP32, device-timed like
+    the step benchmark from the rest state."""
+    import mrlbm
+
+    mrlbm.set_device(0)
+    n, q = args.cavity_n, args.cavity_lattice
+    d = mrlbm.lid_cavity_desc(n, re=100.0, lid_u=0.05, lattice=q)
+    dom = mrlbm.Domain(d)
+    dom.set_node_types(mrlbm.lid_cavity_node_types(n, n, n, 1))
+    dom.init_uniform()
+    dom.step(max(args.warmup, 3))
+    dom.synchronize()
+    with ClockSampler(0) as clk:
+        ms = dom.time_steps(args.steps)
+    sums = dom.sums()
+    dom.close()
+    mlups = args.steps * n ** 3 / (ms * 1e-3) / 1e6
+    b_alg = 2 * 10 * 4 + 1  # moments read and written, node class read
+    line = {"metric": "MLUPS (fused step, walled domain)", "value": round(mlups, 1), "unit": "MLUPS", "n_gpus": 1,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": round(ms / args.steps, 5),
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic (rest state, moving lid)",
+            "config": {"workload": "lid_cavity_%d^3_d3q%d_fp32" % (n, q), "re": 100.0, "lid_u": 0.05,
+                       "bytes_per_lup_algorithmic": b_alg},
+            "hbm_gbs_algorithmic": round(mlups * 1e6 * b_alg / 1e9, 1), "clocks": clk.summary(),
+            "finite": bool(sums["nonfinite"] == 0)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_zslab_workload(args):
     """Z-slab decomposition on one GPU: the benchmark vortex (D3Q27, 256^3,
     FP32) cut into 2 and 4 slabs, each a library domain on its own stream with
@@ -765,16 +797,19 @@ def main():
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="reference arm: skip the side run of the reference's own CUDA program")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
-    ap.add_argument("--workload", default="tgv", choices=["tgv", "batch", "serve", "precision", "thermal", "zslab"],
-                    help="tgv: the headline step benchmark (default); batch / serve / precision / thermal / zslab: "
-                         "the batched-cavity, serving, storage-precision, thermal-scalar and z-slab workloads (run "
-                         "on their own)")
+    ap.add_argument("--workload", default="tgv",
+                    choices=["tgv", "batch", "serve", "precision", "thermal", "zslab", "cavity"],
+                    help="tgv: the headline step benchmark (default); batch / serve / precision / thermal / zslab / "
+                         "cavity: the batched-cavity, serving, storage-precision, thermal-scalar, z-slab and "
+                         "walled-cavity workloads (run on their own)")
     ap.add_argument("--lattice", type=int, default=27, choices=[19, 27],
                     help="tgv workload: velocity set (D3Q27 is the benchmark's; D3Q19 for comparison)")
     ap.add_argument("--n", type=int, default=512, help="precision workload: grid edge")
     ap.add_argument("--precision-steps", type=int, default=1000)
     ap.add_argument("--precision-re", type=float, default=RE)
     ap.add_argument("--reference", default=None, help="precision workload: FP64 planes from oracle/tgv_reference.py")
+    ap.add_argument("--cavity-n", type=int, default=128, help="cavity workload: grid edge")
+    ap.add_argument("--cavity-lattice", type=int, default=19, choices=[19, 27])
     ap.add_argument("--domains", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=5000)
     ap.add_argument("--alone-steps", type=int, default=200)
@@ -801,6 +836,8 @@ def main():
         return run_thermal_workload(args)
     if args.workload == "zslab":
         return run_zslab_workload(args)
+    if args.workload == "cavity":
+        return run_cavity_workload(args)
     return run_gpu_arm(args)
 
 
