@@ -442,7 +442,8 @@ def serve_phase(args, reqs, arrivals, storage):
     import mrlbm
 
     srv = mrlbm.Server(storage=storage, hbm_budget=150e9, max_active=args.max_active, steps_per_tick=100,
-                       residual_tol=1e-6, max_steps=args.max_steps, keep_results=True)
+                       residual_tol=1e-6, max_steps=args.max_steps, keep_results=True,
+                       capacity_nodes=args.serve_capacity)
     t0 = srv.now()
     ids = []
     for r, a in zip(reqs, arrivals):
@@ -528,7 +529,10 @@ def run_serve_workload(args):
     at two loads: the saturating rate (--rate, 200/s by default: offered work
     far above what one GPU does) and a rate below capacity (--rate-low), each
     against the same requests solved one at a time with plain single-domain
-    launches.  Storage --serve-storage (split-velocity fp16 by default); the
+    launches.  --serve-capacity limits the nodes running together (0, the
+    default: none; 8e6, about one 200^3 domain: large solves run in arrival
+    order, small ones share a batch).  Storage --serve-storage
+    (split-velocity fp16 by default); the
     accuracy columns compare sampled served velocity fields with FP32 solves
     of the same requests for the same step counts."""
     import mrlbm
@@ -551,7 +555,8 @@ def run_serve_workload(args):
             "dtype": "%s storage, f32 arithmetic" % args.serve_storage, "data": "synthetic (seed 20261203)",
             "config": {"workload": "serving_poisson_d3q19", "edges": "U{32..192}",
                        "mix": "50/50 lid cavity / power-law duct (5% obstacles)", "residual_tol": 1e-6,
-                       "max_steps": args.max_steps, "hbm_budget_gb": 150, "storage": args.serve_storage},
+                       "max_steps": args.max_steps, "hbm_budget_gb": 150, "storage": args.serve_storage,
+                       "capacity_nodes": args.serve_capacity},
             "phases": phases}
     print(json.dumps(line), flush=True)
     return 0
@@ -819,6 +824,9 @@ def main():
     ap.add_argument("--requests-low", type=int, default=12)
     ap.add_argument("--serve-storage", default="f16u", choices=["f16", "f16u", "f32"])
     ap.add_argument("--error-sample", type=int, default=8, help="serving: requests compared with an FP32 solve")
+    ap.add_argument("--serve-capacity", type=float, default=0.0,
+                    help="serving: lattice nodes the running solves may hold together (0, the default: every "
+                         "arrived request shares the GPU; 8e6: large solves in arrival order)")
     ap.add_argument("--max-active", type=int, default=512)
     ap.add_argument("--max-steps", type=int, default=20000)
     args = ap.parse_args()

@@ -419,6 +419,15 @@ mrlbm_status mrlbm_server_now(mrlbm_server* srv, double* t);
 /* Test hook: replace one node's moments of an admitted request with NaN
  * (host-side fault injection; the divergence watch must retire it). */
 mrlbm_status mrlbm_server_inject_nan(mrlbm_server* srv, int rid);
+/* Compute limit of admission (0, the default: none).  A queued request
+ * joins the running solves only while their lattice nodes together, its own
+ * included, stay within `nodes`; with nothing running it always starts.
+ * Admission stays in arrival order, so with a limit of about what fills the
+ * GPU (a few million nodes on a B200) large solves run one or two at a time
+ * in arrival order and small ones still share a batch: the same throughput
+ * as sharing the GPU among every arrived request, and earlier completions
+ * for the early arrivals.  No counterpart in the reference. */
+mrlbm_status mrlbm_server_set_capacity(mrlbm_server* srv, double nodes);
 /* Keep each finished request's final moments on the host for
  * mrlbm_server_moments (off by default: large requests are hundreds of MB). */
 mrlbm_status mrlbm_server_keep_results(mrlbm_server* srv, int on);

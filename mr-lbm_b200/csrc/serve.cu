@@ -43,6 +43,8 @@ struct mrlbm_server {
     std::map<int, Request> reqs;
     std::vector<int> active;
     double used = 0;
+    double capacity = 0;  // lattice nodes the active solves may hold together (0: no limit)
+    double active_nodes = 0;
     double lups = 0;
     int next_id = 0;
     std::chrono::steady_clock::time_point t0;
@@ -169,6 +171,14 @@ extern "C" mrlbm_status mrlbm_server_destroy(mrlbm_server* s)
     return MRLBM_OK;
 }
 
+extern "C" mrlbm_status mrlbm_server_set_capacity(mrlbm_server* s, double nodes)
+{
+    if (!s) return fail(MRLBM_EINVAL, "null server");
+    if (!(nodes >= 0)) return fail(MRLBM_EINVAL, "capacity %g nodes", nodes);
+    s->capacity = nodes;
+    return MRLBM_OK;
+}
+
 extern "C" mrlbm_status mrlbm_server_keep_results(mrlbm_server* s, int on)
 {
     if (!s) return fail(MRLBM_EINVAL, "null server");
@@ -241,6 +251,7 @@ static mrlbm_status admit(mrlbm_server* s, int rid)
     q.member = mid;
     q.admitted = now_s(s);
     s->used += (double)q.bytes;
+    s->active_nodes += (double)q.nodes;
     s->active.push_back(rid);
     return MRLBM_OK;
 }
@@ -262,6 +273,7 @@ static mrlbm_status retire(mrlbm_server* s, int rid, int status)
     q.status = status;
     q.finished = now_s(s);
     s->used -= (double)q.bytes;
+    s->active_nodes -= (double)q.nodes;
     s->active.erase(std::find(s->active.begin(), s->active.end(), rid));
     return MRLBM_OK;
 }
@@ -280,6 +292,9 @@ extern "C" mrlbm_status mrlbm_server_tick(mrlbm_server* s, int* active_out)
         Request& q = s->reqs[rid];
         if (q.arrival > t) break;
         if (s->used + (double)q.bytes > s->budget) break;
+        // the compute limit: a solve joins the running ones only while their
+        // nodes together still fit it; with nothing running it always starts
+        if (s->capacity > 0 && !s->active.empty() && s->active_nodes + (double)q.nodes > s->capacity) break;
         s->queue.pop_front();
         if ((st = admit(s, rid))) {
             q.status = st;

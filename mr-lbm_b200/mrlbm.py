@@ -193,6 +193,7 @@ def lib():
             "mrlbm_server_now": [VP, C.POINTER(C.c_double)],
             "mrlbm_server_inject_nan": [VP, C.c_int],
             "mrlbm_server_keep_results": [VP, C.c_int],
+            "mrlbm_server_set_capacity": [VP, C.c_double],
             "mrlbm_request_domain": [C.POINTER(Request), C.c_int, C.POINTER(VP)],
             "mrlbm_request_describe": [C.POINTER(Request), C.c_int, C.POINTER(Desc), C.POINTER(C.c_uint32)],
             "mrlbm_reduce_fp64_ref_layout_noalloc": [VP, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, VP,
@@ -612,7 +613,7 @@ class Server:
     """Continuous-batching solve server (mrlbm_server_* in include/mrlbm.h)."""
 
     def __init__(self, storage=F16, hbm_budget=150e9, max_active=512, steps_per_tick=100, residual_tol=1e-6,
-                 max_steps=20000, keep_results=False):
+                 max_steps=20000, keep_results=False, capacity_nodes=0):
         self.L = lib()
         h = VP()
         check(self.L.mrlbm_server_create(storage, float(hbm_budget), int(max_active), int(steps_per_tick),
@@ -620,6 +621,8 @@ class Server:
         self.h = h
         if keep_results:
             check(self.L.mrlbm_server_keep_results(self.h, 1))
+        if capacity_nodes:
+            check(self.L.mrlbm_server_set_capacity(self.h, float(capacity_nodes)))
 
     def close(self):
         if getattr(self, "h", None):

@@ -18,9 +18,9 @@ def mix():
             mrlbm.make_request(mrlbm.REQ_LID_CAVITY, 30, re=900.0)]
 
 
-def run_server(reqs, max_steps=300, tick=50, budget=150e9, max_active=64, inject=None):
+def run_server(reqs, max_steps=300, tick=50, budget=150e9, max_active=64, inject=None, capacity=0):
     srv = mrlbm.Server(storage=mrlbm.F16, hbm_budget=budget, max_active=max_active, steps_per_tick=tick,
-                       residual_tol=1e-12, max_steps=max_steps, keep_results=True)
+                       residual_tol=1e-12, max_steps=max_steps, keep_results=True, capacity_nodes=capacity)
     ids = [srv.submit(r) for r in reqs]
     first = True
     while True:
@@ -95,4 +95,33 @@ def test_cancel_running_request():
     srv.tick()
     assert srv.result(rid)["status"] == 9
     assert srv.stats()["active"] == 0
+    srv.close()
+
+
+def test_capacity_admits_in_arrival_order_within_the_node_limit():
+    """With a compute limit of 60,000 nodes: the 24^3 and 28^3 requests
+    (13,824 + 21,952 nodes) run together, the 36^3 one (46,656) waits until
+    they leave, and every result is still the one the request gets alone."""
+    reqs = mix()
+    srv = mrlbm.Server(storage=mrlbm.F16, hbm_budget=150e9, max_active=64, steps_per_tick=50,
+                       residual_tol=1e-12, max_steps=300, keep_results=True, capacity_nodes=60000)
+    ids = [srv.submit(r) for r in reqs]
+    srv.tick()
+    st = srv.stats()
+    assert st["active"] == 2 and st["queued"] == 3
+    while True:
+        active = srv.tick()
+        if active == 0 and srv.stats()["queued"] == 0:
+            break
+    res = [srv.result(i) for i in ids]
+    assert all(r["status"] == 0 and r["steps"] == 300 for r in res)
+    # later arrivals start no earlier than the requests before them
+    admitted = [r["admitted"] for r in res]
+    assert admitted == sorted(admitted) and admitted[2] >= max(res[0]["finished"], res[1]["finished"]) - 1e-9
+    with pytest.raises(mrlbm.MrlbmError):
+        mrlbm.check(srv.L.mrlbm_server_set_capacity(srv.h, -1.0))
+    _, ref, _ = run_server(reqs)
+    for rid, k in zip(ids, range(len(reqs))):
+        np.testing.assert_array_equal(srv.moments(rid, reqs[k].n, 11 if reqs[k].kind == mrlbm.REQ_DUCT else 10),
+                                      list(ref.values())[k][1])
     srv.close()
