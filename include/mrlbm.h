@@ -351,10 +351,18 @@ mrlbm_status mrlbm_batch_synchronize(mrlbm_batch* batch);
 mrlbm_status mrlbm_batch_time_steps(mrlbm_batch* batch, int nsteps, float* ms);
 /* Work items (columns) in the current list, lattice nodes of all members. */
 mrlbm_status mrlbm_batch_info(mrlbm_batch* batch, int* members, int* items, long long* nodes);
-/* Autotuner: measures the z-chunk length per domain-size class on this GPU
- * (a few timed steps per candidate on a scratch domain) and uses the winner
- * for every member of that class.  Without it a size rule is used. */
+/* Autotuner, for each of the kernel's two tile heights (8 rows, two CTAs an
+ * SM; 14 rows, one): measures the z-chunk length per domain-size class (a few
+ * timed steps of the whole batch per candidate), then times the batch with
+ * those chunks; keeps the faster height (the starting one unless the other
+ * is 2 % faster) and its chunks.  It times on the members themselves and
+ * restores their moments and step counts afterwards.  Without it: 8 rows
+ * (14 for D3Q27 split-velocity fp16 batches) and 32-plane chunks. */
 mrlbm_status mrlbm_batch_autotune(mrlbm_batch* batch);
+/* The batch kernel's tile height: 8 or 14 interior rows per CTA (results do
+ * not depend on it; no counterpart in the reference). */
+mrlbm_status mrlbm_batch_set_rows(mrlbm_batch* batch, int rows);
+mrlbm_status mrlbm_batch_get_rows(mrlbm_batch* batch, int* rows);
 /* The z-chunk length the batch uses for a domain of this size. */
 mrlbm_status mrlbm_batch_chunk_for(mrlbm_batch* batch, int nx, int ny, int nz, int* lz);
 

@@ -35,32 +35,49 @@ struct mrlbm_batch {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaGraphExec_t graph = nullptr;
-    int grid = 148;
-    size_t smem = 0;
+    int rows = TYI_BULK;   // rows per CTA of the batch kernel (TYI_BULK or TYI_WALL)
+    int grid[2] = {148, 148};   // persistent grid per tile kind (tile_kind(rows))
+    size_t smem[2] = {0, 0};
     std::map<int, int> lz_by_class;  // autotuned z-chunk per size class
 };
 
 namespace {
 
-// the batch kernel's rows per CTA for the batch's lattice and storage
-int batch_rows(const mrlbm_batch* b)
+// the batch kernel's rows per CTA
+int batch_rows(const mrlbm_batch* b) { return b->rows; }
+
+// shared memory and persistent grid of the batch kernel of each tile height
+template <int Q, typename T, int S, int TYI>
+mrlbm_status set_shape(mrlbm_batch* b, int sms)
 {
-    return batch_tyi(b->lattice, b->storage == MRLBM_F16U ? F_SPLITU : 0);
+    const int k = tile_kind(TYI);
+    b->smem[k] = ZSmem<Q, T, TYI, batch_npm<T, S>(), false, BATCH_STATIC_SMEM>::bytes;
+    cudaError_t e =
+        cudaFuncSetAttribute(batch_step<Q, T, S, TYI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem[k]);
+    if (e != cudaSuccess) return fail(MRLBM_ECUDA, "batch attribute: %s", cudaGetErrorString(e));
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_step<Q, T, S, TYI>, 32 * (TYI + 2), b->smem[k]);
+    b->grid[k] = sms * std::max(per_sm, 1);
+    return MRLBM_OK;
 }
 
 template <int Q, typename T, int S = 0>
-mrlbm_status set_attr(size_t& smem)
+mrlbm_status set_shapes(mrlbm_batch* b, int sms)
 {
-    smem = ZSmem<Q, T, batch_tyi(Q, S), batch_npm<T, S>(), false, BATCH_STATIC_SMEM>::bytes;
-    cudaError_t e = cudaFuncSetAttribute(batch_step<Q, T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return fail(MRLBM_ECUDA, "batch attribute: %s", cudaGetErrorString(e));
-    return MRLBM_OK;
+    mrlbm_status st = set_shape<Q, T, S, TYI_BULK>(b, sms);
+    return st ? st : set_shape<Q, T, S, TYI_WALL>(b, sms);
 }
 
 template <int Q, typename T, int S = 0>
 void launch(mrlbm_batch* b)
 {
-    batch_step<Q, T, S><<<b->grid, 32 * (batch_tyi(Q, S) + 2), b->smem, b->stream>>>(b->d_doms, b->d_items, b->d_ctl);
+    const int k = tile_kind(b->rows);
+    if (b->rows == TYI_BULK)
+        batch_step<Q, T, S, TYI_BULK>
+            <<<b->grid[k], 32 * (TYI_BULK + 2), b->smem[k], b->stream>>>(b->d_doms, b->d_items, b->d_ctl);
+    else
+        batch_step<Q, T, S, TYI_WALL>
+            <<<b->grid[k], 32 * (TYI_WALL + 2), b->smem[k], b->stream>>>(b->d_doms, b->d_items, b->d_ctl);
 }
 
 void launch_any(mrlbm_batch* b)
@@ -86,6 +103,18 @@ int size_class(int nx, int ny, int nz)
     if (e < 128) return 4;
     if (e < 192) return 5;
     return 6;
+}
+
+// switch the batch kernel's tile height (the captured graph holds the old
+// launch shape; the next refresh rebuilds the work list for the new height)
+void set_rows(mrlbm_batch* b, int rows)
+{
+    if (rows == b->rows) return;
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    b->rows = rows;
 }
 
 int chunk_for(const mrlbm_batch* b, int nx, int ny, int nz)
@@ -243,29 +272,20 @@ extern "C" mrlbm_status mrlbm_batch_create(int lattice, int storage, mrlbm_batch
     mrlbm_batch* b = new mrlbm_batch();
     b->lattice = lattice;
     b->storage = storage;
-    mrlbm_status st;
-    if (lattice == 19)
-        st = storage == MRLBM_F32    ? set_attr<19, float>(b->smem)
-             : storage == MRLBM_F16U ? set_attr<19, __half, F_SPLITU>(b->smem)
-                                     : set_attr<19, __half>(b->smem);
-    else
-        st = storage == MRLBM_F32    ? set_attr<27, float>(b->smem)
-             : storage == MRLBM_F16U ? set_attr<27, __half, F_SPLITU>(b->smem)
-                                     : set_attr<27, __half>(b->smem);
-    if (st) { delete b; return st; }
-    int dev = 0, sms = 148, per_sm = 1;
+    b->rows = batch_tyi(lattice, storage == MRLBM_F16U ? F_SPLITU : 0);
+    int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    {
-        const void* k = lattice == 19 ? (storage == MRLBM_F32    ? (const void*)batch_step<19, float>
-                                         : storage == MRLBM_F16U ? (const void*)batch_step<19, __half, F_SPLITU>
-                                                                 : (const void*)batch_step<19, __half>)
-                                      : (storage == MRLBM_F32    ? (const void*)batch_step<27, float>
-                                         : storage == MRLBM_F16U ? (const void*)batch_step<27, __half, F_SPLITU>
-                                                                 : (const void*)batch_step<27, __half>);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 32 * (batch_rows(b) + 2), b->smem);
-    }
-    b->grid = sms * std::max(per_sm, 1);
+    mrlbm_status st;
+    if (lattice == 19)
+        st = storage == MRLBM_F32    ? set_shapes<19, float>(b, sms)
+             : storage == MRLBM_F16U ? set_shapes<19, __half, F_SPLITU>(b, sms)
+                                     : set_shapes<19, __half>(b, sms);
+    else
+        st = storage == MRLBM_F32    ? set_shapes<27, float>(b, sms)
+             : storage == MRLBM_F16U ? set_shapes<27, __half, F_SPLITU>(b, sms)
+                                     : set_shapes<27, __half>(b, sms);
+    if (st) { delete b; return st; }
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
         cudaMalloc(&b->d_ctl, sizeof(BatchCtl)) != cudaSuccess ||
@@ -413,6 +433,23 @@ extern "C" mrlbm_status mrlbm_batch_chunk_for(mrlbm_batch* b, int nx, int ny, in
 // aside and afterwards copies it back and restores the step counters: the
 // timed steps (an even number, so the buffer parities come back) leave no
 // trace in any solve.
+extern "C" mrlbm_status mrlbm_batch_set_rows(mrlbm_batch* b, int rows)
+{
+    if (!b) return fail(MRLBM_EINVAL, "null batch");
+    if (rows != TYI_BULK && rows != TYI_WALL)
+        return fail(MRLBM_EINVAL, "batch tile height %d: %d or %d rows", rows, TYI_BULK, TYI_WALL);
+    CK(cudaStreamSynchronize(b->stream));
+    set_rows(b, rows);
+    return refresh(b);
+}
+
+extern "C" mrlbm_status mrlbm_batch_get_rows(mrlbm_batch* b, int* rows)
+{
+    if (!b || !rows) return fail(MRLBM_EINVAL, "null argument");
+    *rows = b->rows;
+    return MRLBM_OK;
+}
+
 extern "C" mrlbm_status mrlbm_batch_autotune(mrlbm_batch* b)
 {
     if (!b) return fail(MRLBM_EINVAL, "null batch");
@@ -456,22 +493,43 @@ extern "C" mrlbm_status mrlbm_batch_autotune(mrlbm_batch* b)
         CK(cudaEventElapsedTime(ms, b->ev0, b->ev1));
         return MRLBM_OK;
     };
+    // for each tile height: the z chunk per size class by coordinate
+    // search, then the whole batch timed with those chunks; the faster
+    // height and its chunks are kept
     mrlbm_status st = MRLBM_OK;
-    for (int c : classes) {
-        float best = 1e30f;
-        int best_lz = 32;
-        for (int lz : cand) {
-            b->lz_by_class[c] = lz;
-            float ms = 0.f;
-            if ((st = timed(&ms))) break;
-            if (ms < best * 0.98f) {
-                best = ms;
-                best_lz = lz;
+    const int rows0 = b->rows;
+    int best_rows = rows0;
+    float best_total = 1e30f;
+    std::map<int, int> best_map = b->lz_by_class;
+    for (int rows : {rows0, rows0 == TYI_BULK ? TYI_WALL : TYI_BULK}) {
+        set_rows(b, rows);
+        for (int c : classes) {
+            float best = 1e30f;
+            int best_lz = 32;
+            for (int lz : cand) {
+                b->lz_by_class[c] = lz;
+                float ms = 0.f;
+                if ((st = timed(&ms))) break;
+                if (ms < best * 0.98f) {
+                    best = ms;
+                    best_lz = lz;
+                }
             }
+            b->lz_by_class[c] = best_lz;
+            if (st) break;
         }
-        b->lz_by_class[c] = best_lz;
         if (st) break;
+        float total = 0.f;
+        if ((st = timed(&total))) break;
+        // the starting height unless the other is 2 % faster
+        if (rows == rows0 || total < best_total * 0.98f) {
+            best_total = total;
+            best_rows = rows;
+            best_map = b->lz_by_class;
+        }
     }
+    set_rows(b, best_rows);
+    b->lz_by_class = best_map;
     // restore the members and the step counters (the device counter too)
     cudaStreamSynchronize(b->stream);
     for (const Saved& s : saved) {

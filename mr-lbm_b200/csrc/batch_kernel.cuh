@@ -10,9 +10,11 @@
 
 namespace mrlbm {
 
-// rows per CTA (members share the single-domain kernel's tensor maps of that
-// height): 8, two CTAs per SM, except D3Q27 split-velocity fp16 batches (S =
-// F_SPLITU), whose 15 stored words of a power-law member spill at 8 rows
+// rows per CTA: either tile height of the single-domain kernels (members
+// share their tensor maps), 8 with two CTAs per SM or 14 with one; the batch
+// starts at this one (8, except D3Q27 split-velocity fp16 batches, whose 15
+// stored words of a power-law member spill at 8 rows) and its autotuner
+// measures both
 __host__ __device__ constexpr int batch_tyi(int q, int s) { return (q == 27 && s != 0) ? TYI_WALL : TYI_BULK; }
 // static shared memory of the batch kernel (the work item and its step
 // arguments), kept out of the ring's share
@@ -48,21 +50,19 @@ struct BatchCtl {
     int nitems;  // active work items
 };
 
-template <int Q, typename T, int FLAGS>
+template <int Q, typename T, int FLAGS, int TYI>
 __device__ __forceinline__ bool batch_column(
     const StepArgs& a, const CUtensorMap* map, const BatchItem& it,
-    const ZSmem<Q, T, batch_tyi(Q, FLAGS & F_SPLITU), batch_npm<T, FLAGS & F_SPLITU>(), false, BATCH_STATIC_SMEM>& sm,
-    unsigned& g0)
+    const ZSmem<Q, T, TYI, batch_npm<T, FLAGS & F_SPLITU>(), false, BATCH_STATIC_SMEM>& sm, unsigned& g0)
 {
-    return zmarch_column<Q, T, FLAGS, batch_tyi(Q, FLAGS & F_SPLITU)>(a, map, it.X0, it.Y0, it.z0,
-                                                                      min(it.z0 + a.lz, a.nz), sm, g0);
+    return zmarch_column<Q, T, FLAGS, TYI>(a, map, it.X0, it.Y0, it.z0, min(it.z0 + a.lz, a.nz), sm, g0);
 }
 
 // S = F_SPLITU for split-storage fp16 batches (their members' flag sets carry
 // it), else 0: one kernel per storage kind keeps each kernel's code and
 // register demand to the flag sets it can meet.
-template <int Q, typename T, int S = 0>
-__global__ void __launch_bounds__(32 * (batch_tyi(Q, S) + 2), ctas_per_sm(batch_tyi(Q, S)))
+template <int Q, typename T, int S, int TYI>
+__global__ void __launch_bounds__(32 * (TYI + 2), ctas_per_sm(TYI))
     batch_step(const BatchDomain* __restrict__ doms, const BatchItem* __restrict__ items, BatchCtl* ctl)
 {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(32 * (batch_tyi(Q, S) + 2), ctas_per_sm(batch_
     __shared__ __align__(16) StepArgs s_args;
     static_assert(sizeof(StepArgs) + 16 <= BATCH_STATIC_SMEM, "batch static shared memory");
     // ring slots for the largest flag set
-    const ZSmem<Q, T, batch_tyi(Q, S), batch_npm<T, S>(), false, BATCH_STATIC_SMEM> sm(smem);
+    const ZSmem<Q, T, TYI, batch_npm<T, S>(), false, BATCH_STATIC_SMEM> sm(smem);
     zmarch_init_barriers(sm);
     const int step = *((volatile int*)&ctl->step);
     const int nitems = *((volatile int*)&ctl->nitems);
@@ -89,11 +89,11 @@ __global__ void __launch_bounds__(32 * (batch_tyi(Q, S) + 2), ctas_per_sm(batch_
         __syncthreads();
         bool ok = true;
         switch (D.flags) {
-            case S: ok = batch_column<Q, T, S>(s_args, &D.map[par], item, sm, g0); break;
-            case S | F_BC: ok = batch_column<Q, T, S | F_BC>(s_args, &D.map[par], item, sm, g0); break;
-            case S | F_BC | F_FORCE: ok = batch_column<Q, T, S | F_BC | F_FORCE>(s_args, &D.map[par], item, sm, g0); break;
+            case S: ok = batch_column<Q, T, S, TYI>(s_args, &D.map[par], item, sm, g0); break;
+            case S | F_BC: ok = batch_column<Q, T, S | F_BC, TYI>(s_args, &D.map[par], item, sm, g0); break;
+            case S | F_BC | F_FORCE: ok = batch_column<Q, T, S | F_BC | F_FORCE, TYI>(s_args, &D.map[par], item, sm, g0); break;
             case S | F_BC | F_FORCE | F_POWERLAW:
-                ok = batch_column<Q, T, S | F_BC | F_FORCE | F_POWERLAW>(s_args, &D.map[par], item, sm, g0);
+                ok = batch_column<Q, T, S | F_BC | F_FORCE | F_POWERLAW, TYI>(s_args, &D.map[par], item, sm, g0);
                 break;
             default: break;  // rejected on the host when the domain joins
         }

@@ -180,6 +180,8 @@ def lib():
             "mrlbm_batch_time_steps": [VP, C.c_int, FP],
             "mrlbm_batch_info": [VP, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_longlong)],
             "mrlbm_batch_autotune": [VP],
+            "mrlbm_batch_set_rows": [VP, C.c_int],
+            "mrlbm_batch_get_rows": [VP, C.POINTER(C.c_int)],
             "mrlbm_batch_chunk_for": [VP, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int)],
             "mrlbm_server_create": [C.c_int, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int, C.POINTER(VP)],
             "mrlbm_server_destroy": [VP],
@@ -534,6 +536,15 @@ class Batch:
 
     def autotune(self):
         check(self.L.mrlbm_batch_autotune(self.h))
+
+    def set_rows(self, rows):
+        """Tile height of the batch kernel: 8 or 14 interior rows per CTA."""
+        check(self.L.mrlbm_batch_set_rows(self.h, int(rows)))
+
+    def rows(self):
+        v = C.c_int()
+        check(self.L.mrlbm_batch_get_rows(self.h, C.byref(v)))
+        return v.value
 
     def chunk_for(self, nx, ny, nz):
         lz = C.c_int()

@@ -38,12 +38,15 @@ def run_alone(desc, nt, steps):
     return m
 
 
-@pytest.mark.parametrize("storage", [mrlbm.F32, mrlbm.F16])
-def test_batch_members_equal_alone(storage):
+@pytest.mark.parametrize("storage,rows", [(mrlbm.F32, 8), (mrlbm.F16, 8), (mrlbm.F32, 14), (mrlbm.F16U, 14)])
+def test_batch_members_equal_alone(storage, rows):
+    """Both tile heights of the batch kernel (8 rows, two CTAs an SM; 14, one)."""
     cases = [cavity(24, 100, storage), cavity(37, 400, storage, ny=29, nz=41), cavity(50, 1000, storage),
              cavity(33, 60, storage, ny=47, nz=26), duct(28, 1, storage), duct(35, 2, storage)]
     steps = 40
     b = mrlbm.Batch(mrlbm.D3Q19, storage)
+    b.set_rows(rows)
+    assert b.rows() == rows
     mem = []
     for d, nt in cases:
         m = b.add(d)
@@ -106,7 +109,10 @@ def test_batch_autotune_keeps_results():
         mem.append(m)
     b.step(6)
     before = [(m.step_count, m.moments()) for m in mem]
-    b.autotune()                   # times candidate chunks on the members, then restores them
+    b.autotune()                   # times candidate chunks and tile heights on the members, then restores them
+    assert b.rows() in (8, 14)
+    with pytest.raises(mrlbm.MrlbmError):
+        b.set_rows(10)
     for (steps, mom), m in zip(before, mem):
         assert m.step_count == steps == 6
         np.testing.assert_array_equal(m.moments(), mom)
