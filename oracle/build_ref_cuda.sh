@@ -20,10 +20,12 @@
 #   _ref/refsim_rb64         rayleighBenard_Periodic (thermal), 64 x 64 x 8, 1000 steps
 #   _ref/cases/*             the same cases compiled in this library's case mode
 #   _ref/refsim_voxel64      voxel (sphere.csv obstacle), D3Q19, 64^3, 500 steps
+#   _ref/refsim_bingham32    Bingham channel, D3Q19, 32 x 32 x 64, Re 10, 1000 steps
 #   _ref/refsim_lid64_ckpt   C1 (edges as walls), 1000 steps, checkpoint after step 500
 #   _ref/refsim_lid64_load   C1 (edges as walls) to step 1000 from a checkpoint
 # CASES_ONLY=1 rebuilds only the case-mode programs; THERMAL_ONLY=1 only refsim_rb64;
-# VOXEL_ONLY=1 only refsim_voxel64; CKPT_ONLY=1 only the two checkpoint programs.
+# VOXEL_ONLY=1 only refsim_voxel64; BINGHAM_ONLY=1 only refsim_bingham32; CKPT_ONLY=1 only the
+# two checkpoint programs.
 set -euo pipefail
 REF=${REF:?set REF to the reference checkout (its src/ folder is read)}
 HERE=$(cd "$(dirname "$0")" && pwd)
@@ -54,7 +56,10 @@ build_case() {
     echo "built $OUT/$name"
 }
 
-if [ -z "${CASES_ONLY:-}" ] && [ -z "${THERMAL_ONLY:-}" ] && [ -z "${VOXEL_ONLY:-}" ] && [ -z "${CKPT_ONLY:-}" ]; then
+# which blocks run: all of them, or the one an *_ONLY variable names
+ONLY="${CASES_ONLY:-}${THERMAL_ONLY:-}${VOXEL_ONLY:-}${CKPT_ONLY:-}${BINGHAM_ONLY:-}"
+
+if [ -z "$ONLY" ]; then
 # C1: lid-driven cavity 64^3, Re 100, lid velocity 0.05 (tau from Re, constants.inc:35-36)
 build_case refsim_lid64 lidDrivenCavity_3D D3Q19 2000 64 \
   'sed -i "s/^constexpr dfloat RE = .*/constexpr dfloat RE = 100;/; s/^constexpr dfloat U_MAX = .*/constexpr dfloat U_MAX = 0.05;/" "$c/constants.inc"; sed -i "s/^#define REPORT_SAVE .*/#define REPORT_SAVE (false)/" "$c/output.inc"'
@@ -85,7 +90,7 @@ build_case refsim_tgv256_q27 taylorGreen D3Q27 1000 256 \
 build_case refsim_bench256 benchmark D3Q19 1000 256 'true'
 fi
 
-if { [ -z "${CASES_ONLY:-}" ] && [ -z "${THERMAL_ONLY:-}" ] && [ -z "${CKPT_ONLY:-}" ]; } || [ -n "${VOXEL_ONLY:-}" ]; then
+if [ -z "$ONLY" ] || [ -n "${VOXEL_ONLY:-}" ]; then
 # voxel obstacle case (VOXEL_FILENAME "sphere.csv", read from the working
 # directory), 64^3 periodic, 500 steps.  As shipped its U_MAX = 0 gives
 # TAU = 0.5 (no viscosity) and its fluid starts at rest with the body force
@@ -98,7 +103,25 @@ build_case refsim_voxel64 voxel D3Q19 500 64 \
 fi
 [ -n "${VOXEL_ONLY:-}" ] && exit 0
 
-if { [ -z "${CASES_ONLY:-}" ] && [ -z "${THERMAL_ONLY:-}" ] && [ -z "${VOXEL_ONLY:-}" ]; } || [ -n "${CKPT_ONLY:-}" ]; then
+if [ -z "$ONLY" ] || [ -n "${BINGHAM_ONLY:-}" ]; then
+# Bingham channel (parallelPlates_D3Q19_turbulent_Bingham: walls in y,
+# periodic x and z, body force along z, a Bingham fluid with yield stress
+# S_Y = Bn U_MAX^2, a log-law start with cuRAND perturbations), shrunk from
+# 192 x 192 x 1536 to 32 x 32 x 64 (del = 16, NZ = 4 del) and run at Re 10
+# instead of 180 (tau 0.528 instead of 0.5015, which such a coarse grid does
+# not survive), 1000 steps.  Its FZ = U_TAU^2 / del is set to 0 (the
+# reference's kernel drops the force, src/mlbm.cu:76-78; this library applies
+# it): the log-law start decays under the walls and the yield stress.
+# The case's treat_data.inc (turbulence statistics: mean flow and velocity
+# fluctuations per distance from the walls) runs at a report at step 500
+# (REPORT_SAVE, MACR_SAVE 500 for its mean counter, SAVEDATA on to write its
+# files).
+build_case refsim_bingham32 parallelPlates_D3Q19_turbulent_Bingham D3Q19 1000 32 \
+  'sed -i "s/^constexpr int del = .*/constexpr int del = 16;/; s/^constexpr unsigned int NZ = .*/constexpr unsigned int NZ = 4*del;/; s/^constexpr dfloat RE = .*/constexpr dfloat RE = 10.0;/; s/^constexpr dfloat FZ = .*/constexpr dfloat FZ = 0.0;/" "$c/constants.inc"; sed -i "s/^#define REPORT_SAVE .*/#define REPORT_SAVE (500)/; s/^#define MACR_SAVE .*/#define MACR_SAVE (500)/; s/^#define SAVEDATA .*/#define SAVEDATA (true)/" "$c/output.inc"'
+fi
+[ -n "${BINGHAM_ONLY:-}" ] && exit 0
+
+if [ -z "$ONLY" ] || [ -n "${CKPT_ONLY:-}" ]; then
 # checkpoint interchange, on C1 with the lid's edges as walls, 1000 steps:
 # refsim_lid64_ckpt writes its checkpoint file set and its macroscopic fields
 # (.bin and legacy VTK) after step 500 (CHECKPOINT_SAVE, MACR_SAVE 500);
@@ -114,7 +137,7 @@ build_case refsim_lid64_load lidDrivenCavity_3D D3Q19 1000 64 \
 fi
 [ -n "${CKPT_ONLY:-}" ] && exit 0
 
-if { [ -z "${CASES_ONLY:-}" ] && [ -z "${VOXEL_ONLY:-}" ] && [ -z "${CKPT_ONLY:-}" ]; } || [ -n "${THERMAL_ONLY:-}" ]; then
+if [ -z "$ONLY" ] || [ -n "${THERMAL_ONLY:-}" ]; then
 # thermal: rayleighBenard_Periodic (D3Q19 flow + D3G19 scalar, THERMAL_MODEL),
 # 64 x 64 x 8, Pr 10, Ra 1e5, hot WEST / cold EAST walls, gravity along x,
 # 1000 steps; final rho, u and C as .bin.  The case ships NZ = 4, which is
@@ -150,6 +173,10 @@ $PY "$CB" "$REF/src/cases/benchmark" -o "$OUT/cases/bench256" --set N_STEPS=1000
 # voxel obstacle case as refsim_voxel64 runs it
 $PY "$CB" "$REF/src/cases/voxel" -o "$OUT/cases/voxel64" --set N=64 --set N_STEPS=500 --set U_MAX=0.05 \
     --set U_0_Z=0.02 --set FZ=0.0 --set "REPORT_SAVE=(false)" $common_out
+# Bingham channel as refsim_bingham32 runs it
+$PY "$CB" "$REF/src/cases/parallelPlates_D3Q19_turbulent_Bingham" -o "$OUT/cases/bingham32" --set del=16 \
+    --set NZ=4*del --set RE=10.0 --set FZ=0.0 --set N_STEPS=1000 $common_out --set "REPORT_SAVE=(500)" --set "MACR_SAVE=(500)" \
+    --set "SAVEDATA=(true)"
 # thermal: rayleighBenard_Periodic as refsim_rb64 runs it (NZ = 8, 1000 steps)
 $PY "$CB" "$REF/src/cases/rayleighBenard_Periodic" -o "$OUT/cases/rb64" --set NZ=8 --set N_STEPS=1000 \
     --set "REPORT_SAVE=(false)" $common_out

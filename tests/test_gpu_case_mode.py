@@ -10,6 +10,9 @@ same inputs.
   kinetic-energy reports (every 100 steps) must agree.
 * lidDrivenCavity_3D 64^3: the case's own bc_definition.inc running inside the
   z-march kernel must agree with the library's generic moment-BC solver.
+* parallelPlates_D3Q19_turbulent_Bingham at 32 x 32 x 64, Re 10, 1000 steps:
+  the Bingham fields, and the turbulence statistics its treat_data.inc
+  writes through the reference's host context, must agree.
 * voxel (an obstacle case whose VOXEL_FILENAME names a CSV of solid nodes),
   64^3, 500 steps, with a sphere and a blob that wraps across the periodic
   faces: the case's voxel file, its 254-mask bc_definition.inc and the
@@ -158,3 +161,41 @@ def test_thermal_case_matches_reference_program(tmp_path):
     rho_err = float(np.max(np.abs(a["rho"] - b["rho"])))
     print("RB case mode vs reference program: C rel L2 %.3e, max|du| / U %.3e, max|drho| %.3e" % (c_err, u_err, rho_err))
     assert c_err < 1e-4 and u_err < 2e-4 and rho_err < 1e-5
+
+
+def test_bingham_case_matches_reference_program(tmp_path):
+    """parallelPlates_D3Q19_turbulent_Bingham (walls in y, periodic x and z,
+    Bingham fluid with yield stress Bn U_MAX^2, cuRAND-perturbed log-law
+    start; its body force set to 0 in both builds, since the reference's
+    kernel drops it) at 32 x 32 x 64 and Re 10, 1000 steps,
+    compiled unchanged in case mode against the reference's own program: the
+    final fields, and the turbulence statistics its treat_data.inc writes
+    at the step-500 report (mean velocity and velocity fluctuations per
+    distance from the walls, through the reference's host idxMom layout and
+    saveTreatData)."""
+    ml_ref = run(os.path.join(REF, "refsim_bingham32"), tmp_path / "ref")
+    ml_ours = run(os.path.join(REF, "cases", "bingham32"), tmp_path / "ours")
+    shape = (64, 32, 32)
+    out = {}
+    for who in ("ref", "ours"):
+        base = os.path.join(tmp_path / who, "TEST", "001", "001_")
+        out[who] = {v: np.fromfile(base + "%s001000.bin" % v, dtype=np.float32).reshape(shape)
+                    for v in ("rho", "ux", "uy", "uz")}
+    e = u_err(out["ours"], out["ref"])
+    drho = float(np.max(np.abs(out["ours"]["rho"] - out["ref"]["rho"])))
+    stats = {}
+    for name in ("ux_mean", "uy_mean", "uz_mean", "ux_fluct", "uy_fluct", "uz_fluct", "uxuy_fluct", "uxuz_fluct",
+                 "uyuz_fluct"):
+        rows = []
+        for who in ("ref", "ours"):
+            with open(os.path.join(tmp_path / who, "TEST", "001", "001_turbulent_%s.txt" % name)) as f:
+                lines = [ln.strip() for ln in f if ln.strip()]
+            assert len(lines) == 1 and lines[0].startswith("step,500,"), (who, name, lines[:2])
+            rows.append(np.array([float(v) for v in lines[0].split(",")[2:]]))
+        assert rows[0].shape == rows[1].shape == (16,)
+        stats[name] = float(np.max(np.abs(rows[1] - rows[0])) / max(np.max(np.abs(rows[0])), 1e-30))
+    print("bingham 32x32x64: reference %.0f MLUPS, case mode %.0f MLUPS; u rel L2 %.2e, max |drho| %.2e; "
+          "statistics max rel diff %s" % (ml_ref or 0, ml_ours or 0, e, drho,
+                                          ", ".join("%s %.1e" % kv for kv in stats.items())))
+    assert e < 1e-4 and drho < 1e-5
+    assert max(stats.values()) < 1e-3
