@@ -196,6 +196,7 @@ struct StepArgs {
     float t_src;       // thermal: source added to C at bulk nodes
     float scale[NM_MAX];   // storage scale per moment (1 for fp32)
     float iscale[NM_MAX];
+    int nbc;           // classes in the table bc
 };
 
 __host__ __device__ __forceinline__ long long pidx(int x, int y, int z, int pitch, long long plane)
@@ -411,17 +412,32 @@ __device__ __forceinline__ void bc_known_sums(uint32_t known, const float* p, fl
 // bc_definition.inc:637-663, solved generically).  The class words are read
 // one at a time: read as 16-byte vectors they all issue up front and spill at
 // the 102 registers a thread of the two-CTA wall kernels may use.
-template <int Q>
+template <bool SH>
+__device__ __forceinline__ float class_word(const float* w)
+{
+    if constexpr (SH) return *w;
+    else return __ldg(w);
+}
+template <bool SH>
+__device__ __forceinline__ uint32_t class_word(const uint32_t* w)
+{
+    if constexpr (SH) return *w;
+    else return __ldg(w);
+}
+
+// SH: plain loads (c may point at the CTA's shared-memory copy of the class),
+// else read-only cache loads from the table in global memory
+template <int Q, bool SH = false>
 __device__ __forceinline__ void bc_moments(const BcClass* __restrict__ c, const float* p, float omega,
                                            float omega0, float* mac)
 {
     float b[7], X[7];
-    bc_known_sums<Q>(__ldg(&c->known), p, b);
+    bc_known_sums<Q>(class_word<SH>(&c->known), p, b);
 #pragma unroll
     for (int r = 0; r < 7; r++) {
         float acc = 0.f;
 #pragma unroll
-        for (int k = 0; k < 7; k++) acc = fmaf(__ldg(&c->ainv[r * 7 + k]), b[k], acc);
+        for (int k = 0; k < 7; k++) acc = fmaf(class_word<SH>(&c->ainv[r * 7 + k]), b[k], acc);
         X[r] = acc;
     }
     // per-node omega (non-Newtonian): Sherman-Morrison update of A(omega0)^-1;
@@ -430,16 +446,16 @@ __device__ __forceinline__ void bc_moments(const BcClass* __restrict__ c, const 
     if (dw != 0.f) {
         float dot = 0.f;
 #pragma unroll
-        for (int r = 0; r < 7; r++) dot = fmaf(__ldg(&c->qa[r]), b[r], dot);
-        const float corr = dw * dot / (1.0f + dw * __ldg(&c->s));
+        for (int r = 0; r < 7; r++) dot = fmaf(class_word<SH>(&c->qa[r]), b[r], dot);
+        const float corr = dw * dot / (1.0f + dw * class_word<SH>(&c->s));
 #pragma unroll
-        for (int r = 0; r < 7; r++) X[r] = fmaf(-corr, __ldg(&c->v[r]), X[r]);
+        for (int r = 0; r < 7; r++) X[r] = fmaf(-corr, class_word<SH>(&c->v[r]), X[r]);
     }
     const float rho = X[0], ir = 1.0f / rho;
     mac[0] = rho;
-    mac[1] = __ldg(&c->u[0]);
-    mac[2] = __ldg(&c->u[1]);
-    mac[3] = __ldg(&c->u[2]);
+    mac[1] = class_word<SH>(&c->u[0]);
+    mac[2] = class_word<SH>(&c->u[1]);
+    mac[3] = class_word<SH>(&c->u[2]);
 #pragma unroll
     for (int k = 0; k < 6; k++) mac[4 + k] = X[1 + k] * ir;
 }
@@ -488,6 +504,28 @@ constexpr uint32_t BC_KIND_OUTFLOW = 2;  // nodeTypeMap bits 8-10
 __device__ __forceinline__ void thermal_wall(const StepArgs& a, const BcClass* __restrict__ c, const float* pg,
                                              unsigned oidx, float& C, float* q);
 
+// D3Q19 flow-only wall kernels stage the first classes of the table in shared
+// memory (ZSmem::CT of them, in the space the ring leaves; the count staged
+// is a word of the 128-byte header), so the wall solve's 50-odd class words
+// come from shared memory instead of the read-only cache.  Classes past the
+// staged count are read from global memory.
+constexpr int HDR_STAGED_CLASSES = 40;  // byte offset of the count in the header
+__device__ __forceinline__ unsigned char* dyn_smem()
+{
+    extern __shared__ __align__(128) unsigned char dyn_smem_base[];
+    return dyn_smem_base;
+}
+__device__ __forceinline__ int staged_classes()
+{
+    return *reinterpret_cast<const int*>(dyn_smem() + HDR_STAGED_CLASSES);
+}
+__device__ __forceinline__ const BcClass* staged_class(int cls)
+{
+    return reinterpret_cast<const BcClass*>(dyn_smem() + 128) + cls;
+}
+// The run-time class table, read from global memory (D3Q27, thermal and
+// batch kernels: a second inlined copy of the solve, or the shared copy's
+// generic loads, measured slower or spilled there).
 struct TableBC {
     template <int Q, typename T>
     static __device__ __forceinline__ void apply(const StepArgs& a, uint8_t cls, const float* p, float omega,
@@ -521,6 +559,48 @@ struct OutflowBC {
         thermal_wall(a, a.bc + cls, pg, oidx, C, q);
     }
 };
+
+// The class table staged in shared memory, for the Newtonian D3Q19 wall
+// kernels: a staged class is solved with shared-memory loads, any other from
+// global memory (two inlined copies of the solve, which fit their registers:
+// +11 % on a 128^3 cavity against TableBC).
+struct TableBCShared : TableBC {
+    template <int Q, typename T>
+    static __device__ __forceinline__ void apply(const StepArgs& a, uint8_t cls, const float* p, float omega,
+                                                 int x, int y, int z, float* mac)
+    {
+        if ((int)cls < staged_classes()) bc_moments<Q, true>(staged_class(cls), p, omega, a.omega0, mac);
+        else bc_moments<Q>(a.bc + cls, p, omega, a.omega0, mac);
+    }
+};
+
+// The class table staged in shared memory, for the non-Newtonian D3Q19 wall
+// kernels: one solve through a generic pointer to the shared or the global
+// copy (two copies spill there; +7 % on a power-law duct against TableBC).
+struct TableBCGeneric : TableBC {
+    template <int Q, typename T>
+    static __device__ __forceinline__ void apply(const StepArgs& a, uint8_t cls, const float* p, float omega,
+                                                 int x, int y, int z, float* mac)
+    {
+        const BcClass* c = (int)cls < staged_classes() ? staged_class(cls) : a.bc + cls;
+        bc_moments<Q, true>(c, p, omega, a.omega0, mac);
+    }
+};
+
+// policies whose kernels stage the class table
+template <typename BCP>
+struct stages_classes : std::false_type {};
+template <>
+struct stages_classes<TableBCShared> : std::true_type {};
+template <>
+struct stages_classes<TableBCGeneric> : std::true_type {};
+
+// the class-table policy of a single-domain wall kernel
+template <int Q, int FLAGS>
+using table_policy_t =
+    std::conditional_t<Q == 19 && (FLAGS & F_THERMAL) == 0,
+                       std::conditional_t<(FLAGS & (F_POWERLAW | F_BINGHAM)) != 0, TableBCGeneric, TableBCShared>,
+                       TableBC>;
 
 // Power-law omega by Newton iteration (src/nnf.h:61-89 with its compile
 // defects fixed) and Bingham (src/nnf.h:92-98).
@@ -1229,7 +1309,7 @@ __device__ __forceinline__ void prod_b(const StepArgs& a, int k, int zp, const f
 // (kernels that switch between flag sets at run time size them for the
 // largest set), and the ring has NSTAGE_MAX stages when they fit next to the
 // exchange buffers, else fewer.
-template <int Q, typename T, int TYI, int NPM, bool TH = false, int RESERVE = 0>
+template <int Q, typename T, int TYI, int NPM, bool TH = false, int RESERVE = 0, bool WC = false>
 struct ZSmem {
     static constexpr int NR = TYI + 2;  // stage rows = exchange rows
     static constexpr size_t stage_max = ((size_t)NR * NPM * 2 * box_x<T>() * sizeof(T) + 127) / 128 * 128;
@@ -1246,7 +1326,20 @@ struct ZSmem {
     static constexpr int NS = fixed + NSTAGE_MAX * stage_max <= budget         ? NSTAGE_MAX
                               : fixed + (NSTAGE_MAX - 1) * stage_max <= budget ? NSTAGE_MAX - 1
                                                                                : NSTAGE_MAX - 2;
-    static constexpr size_t bytes = fixed + NS * stage_max;
+    static constexpr size_t ring_bytes = fixed + NS * stage_max;
+    // WC: the wall kernel's class table, as many classes as the space the
+    // ring leaves holds (at most 255), right after the header
+    static constexpr size_t ct_bytes_of(int n) { return ((size_t)n * sizeof(BcClass) + 127) / 128 * 128; }
+    static constexpr int ct_fit()
+    {
+        int n = WC ? (int)((budget - ring_bytes) / sizeof(BcClass)) : 0;
+        if (n > 255) n = 255;
+        while (n > 0 && ring_bytes + ct_bytes_of(n) > budget) n--;
+        return n;
+    }
+    static constexpr int CT = ct_fit();
+    static constexpr size_t ct_bytes = ct_bytes_of(CT);
+    static constexpr size_t bytes = ring_bytes + ct_bytes;
     static_assert(bytes <= budget, "shared memory over the sm_100 limit");
     uint64_t* bars;   // the ring's mbarriers, then the CTA's timeout flag (bars + NSTAGE_MAX)
     unsigned char* stages;
@@ -1259,7 +1352,7 @@ struct ZSmem {
     __device__ __forceinline__ explicit ZSmem(unsigned char* smem)
     {
         bars = reinterpret_cast<uint64_t*>(smem);
-        stages = smem + 128;
+        stages = smem + 128 + ct_bytes;
         ex4 = reinterpret_cast<float4*>(stages + NS * stage_max);
         ex1 = reinterpret_cast<float*>(ex4 + 2 * Exchange<Q, TYI>::buf4);
         exg4 = reinterpret_cast<float4*>(ex1 + 2 * Exchange<Q, TYI>::buf1);
@@ -1276,7 +1369,7 @@ struct ZSmem {
 // chain columns without re-initialising its mbarriers.  Warps 0 .. TYI-1 run
 // the interior pipeline (interior_loop), warps TYI and TYI+1 the helper one
 // (helper_loop); both take the same barriers in the same order.
-template <int Q, typename T, int FLAGS, int TYI, typename BCP, int NPM, int RES = 0>
+template <int Q, typename T, int FLAGS, int TYI, typename BCP, int NPM, int RES = 0, bool WC = false>
 struct ZMarch {
     static constexpr int NR = TYI + 2;
     static constexpr int BX = box_x<T>();
@@ -1291,7 +1384,7 @@ struct ZMarch {
     static constexpr size_t stage_bytes = (size_t)NR * ROW * sizeof(T);
     using EX = Exchange<Q, TYI>;
     using EXG = Exchange<19, TYI>;
-    using SM = ZSmem<Q, T, TYI, NPM, TH, RES>;
+    using SM = ZSmem<Q, T, TYI, NPM, TH, RES, WC>;
     static constexpr int NS = SM::NS;
     static constexpr int TMA_THREAD = 32 * TYI;  // lane 0 of the bottom helper
     static_assert(NP <= NPM, "ring slots sized for fewer moment pairs");
@@ -1524,12 +1617,13 @@ struct ZMarch {
 // One column (X0, Y0) x planes [z0, zend) of one domain.  g0 is the CTA's
 // running production count (advanced by the column's productions).  Returns
 // false when a bounded wait timed out (the CTA must stop).
-template <int Q, typename T, int FLAGS, int TYI, typename BCP = TableBC, int NPM, int RES>
+template <int Q, typename T, int FLAGS, int TYI, typename BCP = TableBC, int NPM, int RES, bool WC>
 __device__ __forceinline__ bool zmarch_column(const StepArgs& a, const CUtensorMap* map, int X0, int Y0, int z0,
-                                              int zend, const ZSmem<Q, T, TYI, NPM, (FLAGS & F_THERMAL) != 0, RES>& sm,
+                                              int zend,
+                                              const ZSmem<Q, T, TYI, NPM, (FLAGS & F_THERMAL) != 0, RES, WC>& sm,
                                               unsigned& g0)
 {
-    using ZM = ZMarch<Q, T, FLAGS, TYI, BCP, NPM, RES>;
+    using ZM = ZMarch<Q, T, FLAGS, TYI, BCP, NPM, RES, WC>;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     // aligned box start (padded column): the TMA x coordinate, 2 elements a
     // node, must be a multiple of 16 bytes
@@ -1540,7 +1634,7 @@ __device__ __forceinline__ bool zmarch_column(const StepArgs& a, const CUtensorM
     zm.cph = zm.phase(0);
 #ifdef MRLBM_BOUNDS_CHECK
     if (threadIdx.x == 0) {
-        using SMT = ZSmem<Q, T, TYI, NPM, (FLAGS & F_THERMAL) != 0, RES>;
+        using SMT = ZSmem<Q, T, TYI, NPM, (FLAGS & F_THERMAL) != 0, RES, WC>;
         g_bounds.stage_lo = smem_u32(sm.stages);
         g_bounds.stage_hi = smem_u32(sm.stages) + (unsigned)(SMT::NS * SMT::stage_max);
         g_bounds.ex_lo = smem_u32(sm.ex4);
@@ -1581,12 +1675,25 @@ __device__ __forceinline__ bool zmarch_column(const StepArgs& a, const CUtensorM
     return true;
 }
 
-template <int Q, typename T, int TYI, int NPM, bool TH, int RES>
-__device__ __forceinline__ void zmarch_init_barriers(const ZSmem<Q, T, TYI, NPM, TH, RES>& sm)
+// Barriers, the timeout flag and, in wall kernels, the staged copy of the
+// first ZSmem::CT classes of the table bc (nbc classes)
+template <int Q, typename T, int TYI, int NPM, bool TH, int RES, bool WC>
+__device__ __forceinline__ void zmarch_init_barriers(const ZSmem<Q, T, TYI, NPM, TH, RES, WC>& sm,
+                                                     const BcClass* bc = nullptr, int nbc = 0)
 {
+    using SMT = ZSmem<Q, T, TYI, NPM, TH, RES, WC>;
+    int staged = 0;
+    if constexpr (SMT::CT > 0) {
+        staged = nbc < SMT::CT ? nbc : SMT::CT;
+        const float4* src = reinterpret_cast<const float4*>(bc);
+        float4* dst = reinterpret_cast<float4*>(dyn_smem() + 128);
+        const int n = staged * (int)(sizeof(BcClass) / 16);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = __ldg(src + i);
+    }
     if (threadIdx.x == 0) {
         *reinterpret_cast<int*>(sm.bars + NSTAGE_MAX) = 0;  // the timeout flag
-        for (int s = 0; s < ZSmem<Q, T, TYI, NPM, TH, RES>::NS; s++) mbar_init(&sm.bars[s], 1);
+        *reinterpret_cast<int*>(dyn_smem() + HDR_STAGED_CLASSES) = staged;
+        for (int s = 0; s < SMT::NS; s++) mbar_init(&sm.bars[s], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -1600,8 +1707,9 @@ __global__ void __launch_bounds__(32 * (TYI + 2), ctas_per_sm(TYI))
     zmarch_step(const __grid_constant__ CUtensorMap map_in, const StepArgs a)
 {
     extern __shared__ __align__(128) unsigned char smem[];
-    const ZSmem<Q, T, TYI, npairs_of(FLAGS), (FLAGS & F_THERMAL) != 0> sm(smem);
-    zmarch_init_barriers(sm);
+    constexpr bool WC = (FLAGS & F_BC) != 0 && stages_classes<BCP>::value;
+    const ZSmem<Q, T, TYI, npairs_of(FLAGS), (FLAGS & F_THERMAL) != 0, 0, WC> sm(smem);
+    zmarch_init_barriers(sm, a.bc, a.nbc);
     unsigned g0 = 0;
     const int z0 = blockIdx.z * a.lz;
     (void)zmarch_column<Q, T, FLAGS, TYI, BCP>(a, &map_in, blockIdx.x * TILE_X, blockIdx.y * TYI, z0,
@@ -1614,10 +1722,11 @@ __host__ __device__ inline dim3 zmarch_grid(int nx, int ny, int nz, int tyi, int
     return dim3((nx + TILE_X - 1) / TILE_X, (ny + tyi - 1) / tyi, (nz + lz - 1) / lz);
 }
 
-template <int Q, typename T, int FLAGS, int TYI>
+template <int Q, typename T, int FLAGS, int TYI, typename BCP = TableBC>
 constexpr size_t step_smem_bytes()
 {
-    return ZSmem<Q, T, TYI, npairs_of(FLAGS), (FLAGS & F_THERMAL) != 0>::bytes;
+    return ZSmem<Q, T, TYI, npairs_of(FLAGS), (FLAGS & F_THERMAL) != 0, 0,
+                 (FLAGS & F_BC) != 0 && stages_classes<BCP>::value>::bytes;
 }
 
 }  // namespace mrlbm

@@ -642,6 +642,7 @@ void mrlbm::fill_step_args(const mrlbm_domain* dom, StepArgs& a, int parity, int
     a.err = dom->err;
     a.cls = dom->cls;
     a.bc = dom->bc;
+    a.nbc = dom->nclasses;
     a.nx = d.nx; a.ny = d.ny; a.nz = d.nz; a.pitch = dom->pitch;
     a.plane = dom->plane; a.field = dom->field;
     a.periodic = (d.periodic[0] ? 1 : 0) | (d.periodic[1] ? 2 : 0) | (d.periodic[2] ? 4 : 0);

@@ -9,13 +9,13 @@
 
 namespace mrlbm {
 
-template <int Q, typename T, int FLAGS, typename BCP = TableBC>
+template <int Q, typename T, int FLAGS, typename BCP = table_policy_t<Q, FLAGS>>
 static mrlbm_status launch_step_t(const CUtensorMap* maps, const StepArgs& a, cudaStream_t s)
 {
     constexpr int TYI = tile_rows(FLAGS);
     constexpr int NW = TYI + 2;
     const CUtensorMap& map = maps[tile_kind(TYI)];
-    constexpr size_t smem = step_smem_bytes<Q, T, FLAGS, TYI>();
+    constexpr size_t smem = step_smem_bytes<Q, T, FLAGS, TYI, BCP>();
     static_assert(smem <= smem_budget(TYI), "shared memory over the sm_100 limit");
     auto kern = zmarch_step<Q, T, FLAGS, TYI, BCP>;
     int dev = 0;
