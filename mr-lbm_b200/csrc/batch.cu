@@ -51,7 +51,7 @@ template <int Q, typename T, int S, int TYI>
 mrlbm_status set_shape(mrlbm_batch* b, int sms)
 {
     const int k = tile_kind(TYI);
-    b->smem[k] = ZSmem<Q, T, TYI, batch_npm<T, S>(), false, BATCH_STATIC_SMEM>::bytes;
+    b->smem[k] = ZSmem<Q, T, TYI, batch_npm<T, S>(), false, BATCH_STATIC_SMEM, batch_stages(Q)>::bytes;
     cudaError_t e =
         cudaFuncSetAttribute(batch_step<Q, T, S, TYI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem[k]);
     if (e != cudaSuccess) return fail(MRLBM_ECUDA, "batch attribute: %s", cudaGetErrorString(e));

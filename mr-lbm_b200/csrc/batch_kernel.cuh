@@ -50,12 +50,20 @@ struct BatchCtl {
     int nitems;  // active work items
 };
 
+// D3Q19 batches stage the class table of the member a work item belongs to
+// (each member has its own), as the single-domain wall kernels do
+__host__ __device__ constexpr bool batch_stages(int q) { return q == 19; }
+
 template <int Q, typename T, int FLAGS, int TYI>
 __device__ __forceinline__ bool batch_column(
     const StepArgs& a, const CUtensorMap* map, const BatchItem& it,
-    const ZSmem<Q, T, TYI, batch_npm<T, FLAGS & F_SPLITU>(), false, BATCH_STATIC_SMEM>& sm, unsigned& g0)
+    const ZSmem<Q, T, TYI, batch_npm<T, FLAGS & F_SPLITU>(), false, BATCH_STATIC_SMEM, batch_stages(Q)>& sm,
+    unsigned& g0)
 {
-    return zmarch_column<Q, T, FLAGS, TYI>(a, map, it.X0, it.Y0, it.z0, min(it.z0 + a.lz, a.nz), sm, g0);
+    // one generic-pointer solve for every flag set: the batch kernel holds
+    // them all, and two inlined solves per set spill
+    using BCP = std::conditional_t<batch_stages(Q), TableBCGeneric, TableBC>;
+    return zmarch_column<Q, T, FLAGS, TYI, BCP>(a, map, it.X0, it.Y0, it.z0, min(it.z0 + a.lz, a.nz), sm, g0);
 }
 
 // S = F_SPLITU for split-storage fp16 batches (their members' flag sets carry
@@ -70,8 +78,10 @@ __global__ void __launch_bounds__(32 * (TYI + 2), ctas_per_sm(TYI))
     __shared__ __align__(16) StepArgs s_args;
     static_assert(sizeof(StepArgs) + 16 <= BATCH_STATIC_SMEM, "batch static shared memory");
     // ring slots for the largest flag set
-    const ZSmem<Q, T, TYI, batch_npm<T, S>(), false, BATCH_STATIC_SMEM> sm(smem);
-    zmarch_init_barriers(sm);
+    using SMT = ZSmem<Q, T, TYI, batch_npm<T, S>(), false, BATCH_STATIC_SMEM, batch_stages(Q)>;
+    const SMT sm(smem);
+    zmarch_init_barriers(sm);  // nothing staged yet
+    int staged_dom = -1;
     const int step = *((volatile int*)&ctl->step);
     const int nitems = *((volatile int*)&ctl->nitems);
     unsigned g0 = 0;
@@ -86,6 +96,19 @@ __global__ void __launch_bounds__(32 * (TYI + 2), ctas_per_sm(TYI))
         constexpr int NW = (int)(sizeof(StepArgs) / 4);
         if (threadIdx.x < NW)
             reinterpret_cast<int*>(&s_args)[threadIdx.x] = reinterpret_cast<const int*>(&D.args[par])[threadIdx.x];
+        if constexpr (SMT::CT > 0) {
+            // another member: its classes (the previous column's reads of the
+            // staged table ended at that column's last barrier)
+            if (item.dom != staged_dom) {
+                const int nbc = D.args[par].nbc;
+                const int n = nbc < SMT::CT ? nbc : SMT::CT;
+                const float4* src = reinterpret_cast<const float4*>(D.args[par].bc);
+                float4* dst = reinterpret_cast<float4*>(dyn_smem() + 128);
+                for (int i = threadIdx.x; i < n * (int)(sizeof(BcClass) / 16); i += blockDim.x) dst[i] = __ldg(src + i);
+                if (threadIdx.x == 0) *reinterpret_cast<int*>(dyn_smem() + HDR_STAGED_CLASSES) = n;
+                staged_dom = item.dom;
+            }
+        }
         __syncthreads();
         bool ok = true;
         switch (D.flags) {
