@@ -257,6 +257,7 @@ def run_gpu_arm(args):
     nodes = N ** 3
     d = mrlbm.make_desc(N, N, N, lattice=LATTICE, storage=mrlbm.F32, periodic=(1, 1, 1), tau=TAU)
     dom = mrlbm.Domain(d)
+    dom.set_tile_order(bool(args.tile_order))
     dom.init_taylor_green(U0, L_TG)
     # warm-up
     dom.step(max(args.warmup, 3))
@@ -642,6 +643,7 @@ def run_cavity_workload(args):
     n, q = args.cavity_n, args.cavity_lattice
     d = mrlbm.lid_cavity_desc(n, re=100.0, lid_u=0.05, lattice=q)
     dom = mrlbm.Domain(d)
+    dom.set_tile_order(bool(args.tile_order))
     dom.set_node_types(mrlbm.lid_cavity_node_types(n, n, n, 1))
     dom.init_uniform()
     dom.step(max(args.warmup, 3))
@@ -816,6 +818,8 @@ def main():
     ap.add_argument("--precision-re", type=float, default=RE)
     ap.add_argument("--reference", default=None, help="precision workload: FP64 planes from oracle/tgv_reference.py")
     ap.add_argument("--cavity-n", type=int, default=128, help="cavity workload: grid edge")
+    ap.add_argument("--tile-order", type=int, default=1, choices=[0, 1],
+                    help="vortex and cavity workloads: overlapped tile-ordered steps (1) or whole-launch order (0)")
     ap.add_argument("--cavity-lattice", type=int, default=19, choices=[19, 27])
     ap.add_argument("--domains", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=5000)

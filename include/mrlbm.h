@@ -204,6 +204,16 @@ mrlbm_status mrlbm_get_step(mrlbm_domain* dom, int* step);
 mrlbm_status mrlbm_set_z_chunk(mrlbm_domain* dom, int lz);
 mrlbm_status mrlbm_get_z_chunk(mrlbm_domain* dom, int* lz);
 
+/* Tile-ordered steps (on = 1, the default): within one mrlbm_step call each
+ * step launch may start while the one before it finishes, and a tile waits
+ * only for the previous step's tiles around it (a per-tile word on the
+ * device, with a bounded wait that raises MRLBM_ETIMEDOUT), so the SMs that
+ * the last CTAs of a step leave idle already run the next step.  on = 0
+ * orders whole launches.  Results are bit-identical either way.  Domains
+ * with outflow walls or a thermal scalar always order whole launches.  No
+ * reference counterpart (one kernel launch per step, src/main.cu:183-200). */
+mrlbm_status mrlbm_set_tile_order(mrlbm_domain* dom, int on);
+
 /* Launch on a caller's stream (a cudaStream_t of the domain's device; NULL
  * returns to the domain's own stream, so the legacy default stream cannot be
  * chosen).  The stream must outlive the domain or be reset first.  Work already queued on the previous

@@ -57,6 +57,11 @@ struct mrlbm_domain {
     float* stage = nullptr;         // float staging buffer for layout conversions
     bool have_snap = false;
     cudaGraphExec_t graph_exec = nullptr;
+    // tile-ordered steps (zmarch_step): ticket counter + a word per tile
+    bool tile_order = true;
+    unsigned* sched = nullptr;
+    size_t sched_words = 0;
+    long long sched_key = -1;  // grid the state belongs to (x, y, z tiles)
 };
 
 namespace mrlbm {
@@ -73,10 +78,12 @@ inline bool is_half_storage(int storage) { return storage == MRLBM_F16 || storag
 mrlbm_status domain_alloc(mrlbm_domain* dom);
 int choose_lz(const mrlbm_domain* dom, int tyi);
 void fill_step_args(const mrlbm_domain* dom, StepArgs& a, int parity, int& flags);
-mrlbm_status enqueue_step(mrlbm_domain* dom, int parity, cudaStream_t s);
+// chained: the launch before this one on s is this domain's step
+mrlbm_status enqueue_step(mrlbm_domain* dom, int parity, cudaStream_t s, bool chained);
+mrlbm_status prepare_tile_order(mrlbm_domain* dom, cudaStream_t s);
 // maps: the read buffer's two tensor maps (tile kinds TYI_BULK, TYI_WALL)
 template <int Q, typename T>
-mrlbm_status dispatch_step(const CUtensorMap* maps, const StepArgs& a, int flags, cudaStream_t s);
+mrlbm_status dispatch_step(const CUtensorMap* maps, const StepArgs& a, int flags, cudaStream_t s, bool pdl);
 mrlbm_status make_tensor_maps(mrlbm_domain* dom);
 mrlbm_status fill_ghosts(mrlbm_domain* dom);
 mrlbm_status check_device_error(mrlbm_domain* dom);

@@ -113,6 +113,7 @@ __host__ __device__ constexpr int tile_rows_of_kind(int kind) { return kind == 0
 constexpr uint8_t CLS_BULK = 0;
 constexpr uint8_t CLS_SOLID = 255;
 constexpr unsigned WAIT_LIMIT = 1u << 26;  // mbarrier polls before giving up (~seconds)
+constexpr unsigned DEP_LIMIT = 1u << 21;   // tile-order polls (an L2 round trip + 64 ns each, ~seconds)
 
 // Bounds-check build (-DMRLBM_BOUNDS_CHECK, libmrlbm_check.so): every
 // shared-memory access of the step kernels is checked against the CTA's
@@ -181,7 +182,8 @@ struct StepArgs {
     int storage;                      // its element type (mrlbm_storage)
     const uint8_t* __restrict__ cls;  // padded [nz+2][ny+2][pitch]
     const BcClass* __restrict__ bc;
-    int* err;                         // bit 0: a bounded wait timed out
+    int* err;                         // bit 0: a bounded wait timed out; bit 2: a tile-order wait did
+    unsigned* sched;                  // null, or the tile-order state of the single-domain step (zmarch_step)
     int nx, ny, nz, pitch;
     long long plane, field;  // elements
     int periodic;            // bit a set: axis a periodic
@@ -510,6 +512,7 @@ __device__ __forceinline__ void thermal_wall(const StepArgs& a, const BcClass* _
 // come from shared memory instead of the read-only cache.  Classes past the
 // staged count are read from global memory.
 constexpr int HDR_STAGED_CLASSES = 40;  // byte offset of the count in the header
+constexpr int HDR_TICKET = 48;          // tile-ordered step: the CTA's work index and step index
 __device__ __forceinline__ unsigned char* dyn_smem()
 {
     extern __shared__ __align__(128) unsigned char dyn_smem_base[];
@@ -1701,9 +1704,90 @@ __device__ __forceinline__ void zmarch_init_barriers(const ZSmem<Q, T, TYI, NPM,
     __syncthreads();
 }
 
+// Tile-ordered steps.  Each launch of the single-domain step may begin while
+// the launch before it is still finishing (programmatic dependent launch):
+// instead of waiting for the whole previous grid, a tile waits only for the
+// previous step's tiles it reads from or writes over, so the SMs that the
+// previous step's last CTAs leave idle already run the next step.  State
+// (sched): a 64-bit ticket counter, then one word per tile (x tile, y tile,
+// z chunk) holding 1 + the last step that finished it.  A CTA takes ticket
+// t: step s = t / tiles, work index w = t % tiles; tickets follow the CTAs'
+// start order, and every CTA of a launch holds its ticket before the next
+// launch starts.  Work index w is column w % columns (x tiles fastest, as the
+// plain grid runs) of chunk (w / columns + s) % chunks: each step starts one
+// chunk further on, so its first tiles need the previous step's first
+// finished chunks (a periodic z axis makes chunk 0 read the last chunk's
+// ghost plane).  A tile of step s reads planes z0 - 1 .. z1 and rows and
+// columns one node beyond its own, and writes its nodes plus their ghost
+// copies, so it waits for the 27 tiles around it (periodic wrap included,
+// which also covers every ghost copy) to hold s; waiting for them to finish
+// step s - 1 covers both their writes of the buffer it reads and their reads
+// of the buffer it writes.
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Takes the CTA's ticket and waits for the tiles around its tile; returns the
+// step index and sets the tile.  Ends with no CTA barrier: the caller's next
+// one orders the waits before the tile's first load.
+__device__ __forceinline__ unsigned tile_order_begin(const StepArgs& a, int& tx, int& ty, int& kc)
+{
+    unsigned* hdr = reinterpret_cast<unsigned*>(dyn_smem() + HDR_TICKET);
+    const unsigned ncol = gridDim.x * gridDim.y, ntile = ncol * gridDim.z;
+    if (threadIdx.x == 0) {
+        const unsigned long long t = atomicAdd(reinterpret_cast<unsigned long long*>(a.sched), 1ull);
+        hdr[0] = (unsigned)(t % ntile);
+        hdr[1] = (unsigned)(t / ntile);
+    }
+    __syncthreads();
+    const unsigned w = hdr[0], s = hdr[1];
+    // every CTA of this launch holds its ticket: the next launch may start
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    const unsigned col = w % ncol;
+    tx = (int)(col % gridDim.x);
+    ty = (int)(col / gridDim.x);
+    kc = (int)((w / ncol + s) % gridDim.z);
+    if (threadIdx.x < 27) {
+        const int dx = (int)threadIdx.x % 3 - 1, dy = (int)threadIdx.x / 3 % 3 - 1, dz = (int)threadIdx.x / 9 - 1;
+        const int nx = (tx + dx + (int)gridDim.x) % (int)gridDim.x;
+        const int ny = (ty + dy + (int)gridDim.y) % (int)gridDim.y;
+        const int nz = (kc + dz + (int)gridDim.z) % (int)gridDim.z;
+        const unsigned* f = a.sched + 2 + ((size_t)nz * gridDim.y + ny) * gridDim.x + nx;
+        bool ok = false;
+        for (unsigned it = 0; it < DEP_LIMIT; it++) {
+            if ((int)(ld_acquire_u32(f) - s) >= 0) {
+                ok = true;
+                break;
+            }
+            // another tile gave up already: so does this one, at once
+            if ((it & 1023u) == 1023u && (*reinterpret_cast<volatile int*>(a.err) & 4)) break;
+            __nanosleep(64);
+        }
+        // on a timeout the step runs on (its result is flagged), so the
+        // tiles waiting on this one do not time out in turn
+        if (!ok) atomicOr(a.err, 4);
+    }
+    return s;
+}
+
+// Marks the CTA's tile done with step s; called after a CTA barrier that
+// follows the tile's last global store.
+__device__ __forceinline__ void tile_order_end(const StepArgs& a, int tx, int ty, int kc, unsigned s)
+{
+    if (threadIdx.x == 0) {
+        __threadfence();
+        unsigned* f = a.sched + 2 + ((size_t)kc * gridDim.y + ty) * gridDim.x + tx;
+        asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(f), "r"(s + 1u) : "memory");
+    }
+}
+
 // Single-domain step: one CTA per (x tile, y tile, z chunk of lz planes).
 // Launch order runs x tiles fastest, so the CTAs resident at one time march
 // neighbouring columns through the same planes and their halo reads hit L2.
+// With a.sched set, a CTA's tile comes from its ticket instead (tile_order_begin).
 template <int Q, typename T, int FLAGS, int TYI, typename BCP = TableBC>
 __global__ void __launch_bounds__(32 * (TYI + 2), ctas_per_sm(TYI))
     zmarch_step(const __grid_constant__ CUtensorMap map_in, const StepArgs a)
@@ -1711,11 +1795,18 @@ __global__ void __launch_bounds__(32 * (TYI + 2), ctas_per_sm(TYI))
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr bool WC = (FLAGS & F_BC) != 0 && stages_classes<BCP>::value;
     const ZSmem<Q, T, TYI, npairs_of(FLAGS), (FLAGS & F_THERMAL) != 0, 0, WC> sm(smem);
-    zmarch_init_barriers(sm, a.bc, a.nbc);
+    int tx = blockIdx.x, ty = blockIdx.y, kc = blockIdx.z;
+    unsigned s = 0;
+    if (a.sched) s = tile_order_begin(a, tx, ty, kc);
+    zmarch_init_barriers(sm, a.bc, a.nbc);  // ends with a CTA barrier
+    // the tiles' stores of the previous step were made visible to this
+    // thread through the generic proxy; the ring's loads use the async one
+    if (a.sched) asm volatile("fence.proxy.async.global;" ::: "memory");
     unsigned g0 = 0;
-    const int z0 = blockIdx.z * a.lz;
-    (void)zmarch_column<Q, T, FLAGS, TYI, BCP>(a, &map_in, blockIdx.x * TILE_X, blockIdx.y * TYI, z0,
-                                          min(z0 + a.lz, a.nz), sm, g0);
+    const int z0 = kc * a.lz;
+    (void)zmarch_column<Q, T, FLAGS, TYI, BCP>(a, &map_in, tx * TILE_X, ty * TYI, z0, min(z0 + a.lz, a.nz), sm, g0);
+    // zmarch_column ends with a CTA barrier on every path
+    if (a.sched) tile_order_end(a, tx, ty, kc, s);
 }
 
 // Grid of the single-domain step.

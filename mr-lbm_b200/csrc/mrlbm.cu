@@ -412,6 +412,7 @@ extern "C" mrlbm_status mrlbm_domain_destroy(mrlbm_domain* dom)
     cudaFree(dom->m[1]);
     cudaFree(dom->cls);
     cudaFree(dom->err);
+    cudaFree(dom->sched);
     cudaFree(dom->bc);
     cudaFree(dom->red_scratch);
     cudaFree(dom->usnap);
@@ -640,6 +641,7 @@ void mrlbm::fill_step_args(const mrlbm_domain* dom, StepArgs& a, int parity, int
         a.out_p[p] = 2 * p < dom->nms ? static_cast<char*>(dom->m[parity ^ 1]) + (size_t)p * 2 * dom->field * dom->esize
                                      : nullptr;
     a.err = dom->err;
+    a.sched = nullptr;
     a.cls = dom->cls;
     a.bc = dom->bc;
     a.nbc = dom->nclasses;
@@ -670,23 +672,84 @@ void mrlbm::fill_step_args(const mrlbm_domain* dom, StepArgs& a, int parity, int
     a.lz = dom->lz > 0 ? dom->lz : dom->lz_t[tile_kind(tile_rows(flags))];
 }
 
-mrlbm_status mrlbm::enqueue_step(mrlbm_domain* dom, int parity, cudaStream_t s)
+// Tile-ordered steps (zmarch_step, tile_order_begin): the state is sized and
+// zeroed for the step's grid, on stream s, whenever the grid changes.  Flag
+// sets whose wall rules read the previous moments through the read-only
+// cache (outflow, thermal) keep whole-grid ordering: that cache is only
+// coherent across launches that do not overlap.  Returns whether the step
+// is tile-ordered and sets the state's grid.
+static bool tile_order_state(mrlbm_domain* dom, const StepArgs& a, int flags, cudaStream_t s, bool& reset,
+                             mrlbm_status& st)
+{
+    st = MRLBM_OK;
+    reset = false;
+    if (!dom->tile_order || (flags & (F_OUTFLOW | F_THERMAL))) return false;
+    const dim3 g = zmarch_grid(a.nx, a.ny, a.nz, tile_rows(flags), a.lz);
+    const long long key = ((long long)g.z << 42) | ((long long)g.y << 21) | (long long)g.x;
+    if (key == dom->sched_key) return true;
+    if (dom->graph_exec) {  // its launches carry the old state
+        cudaStreamSynchronize(s);
+        cudaGraphExecDestroy(dom->graph_exec);
+        dom->graph_exec = nullptr;
+    }
+    const size_t words = 2 + (size_t)g.x * g.y * g.z;
+    if (words > dom->sched_words) {
+        if (dom->sched) {
+            cudaStreamSynchronize(s);
+            cudaFree(dom->sched);
+            dom->sched = nullptr;
+            dom->sched_words = 0;
+        }
+        cudaError_t e = cudaMalloc(&dom->sched, words * sizeof(unsigned));
+        if (e != cudaSuccess) {
+            st = fail(MRLBM_ECUDA, "tile-order state: %s", cudaGetErrorString(e));
+            return false;
+        }
+        dom->sched_words = words;
+    }
+    cudaError_t e = cudaMemsetAsync(dom->sched, 0, words * sizeof(unsigned), s);
+    if (e != cudaSuccess) {
+        st = fail(MRLBM_ECUDA, "tile-order state: %s", cudaGetErrorString(e));
+        return false;
+    }
+    dom->sched_key = key;
+    reset = true;
+    return true;
+}
+
+mrlbm_status mrlbm::prepare_tile_order(mrlbm_domain* dom, cudaStream_t s)
+{
+    StepArgs a;
+    int flags;
+    fill_step_args(dom, a, dom->cur, flags);
+    bool reset;
+    mrlbm_status st;
+    (void)tile_order_state(dom, a, flags, s, reset, st);
+    return st;
+}
+
+mrlbm_status mrlbm::enqueue_step(mrlbm_domain* dom, int parity, cudaStream_t s, bool chained)
 {
     StepArgs a;
     int flags;
     fill_step_args(dom, a, parity, flags);
+    bool reset;
+    mrlbm_status st;
+    if (tile_order_state(dom, a, flags, s, reset, st)) a.sched = dom->sched;
+    if (st) return st;
+    // a zeroed state follows a memset on the stream: no overlap with it
+    const bool pdl = a.sched && chained && !reset;
     const int q = dom->q;
     const int stg = dom->d.storage;
-    mrlbm_status st;
     const CUtensorMap* maps = dom->tmap[parity];
     if (q == 19) {
-        if (stg == MRLBM_F32) st = dispatch_step<19, float>(maps, a, flags, s);
-        else if (is_half_storage(stg)) st = dispatch_step<19, __half>(maps, a, flags, s);
-        else st = dispatch_step<19, __nv_bfloat16>(maps, a, flags, s);
+        if (stg == MRLBM_F32) st = dispatch_step<19, float>(maps, a, flags, s, pdl);
+        else if (is_half_storage(stg)) st = dispatch_step<19, __half>(maps, a, flags, s, pdl);
+        else st = dispatch_step<19, __nv_bfloat16>(maps, a, flags, s, pdl);
     } else {
-        if (stg == MRLBM_F32) st = dispatch_step<27, float>(maps, a, flags, s);
-        else if (is_half_storage(stg)) st = dispatch_step<27, __half>(maps, a, flags, s);
-        else st = dispatch_step<27, __nv_bfloat16>(maps, a, flags, s);
+        if (stg == MRLBM_F32) st = dispatch_step<27, float>(maps, a, flags, s, pdl);
+        else if (is_half_storage(stg)) st = dispatch_step<27, __half>(maps, a, flags, s, pdl);
+        else st = dispatch_step<27, __nv_bfloat16>(maps, a, flags, s, pdl);
     }
     return st;
 }
@@ -695,7 +758,8 @@ extern "C" mrlbm_status mrlbm_step(mrlbm_domain* dom, int nsteps)
 {
     if (!dom || nsteps < 0) return fail(MRLBM_EINVAL, "bad argument");
     for (int s = 0; s < nsteps; s++) {
-        mrlbm_status st = enqueue_step(dom, dom->cur, dom->stream);
+        // launches after the first follow this call's own step on the stream
+        mrlbm_status st = enqueue_step(dom, dom->cur, dom->stream, s > 0);
         if (st) return st;
         dom->cur ^= 1;
         dom->step++;
@@ -711,10 +775,14 @@ extern "C" mrlbm_status mrlbm_step_graph(mrlbm_domain* dom, int nsteps)
     // One graph of GRAPH_STEPS launches starting from parity 0 (an even count,
     // so replays chain); an odd leading step or a short remainder runs eagerly.
     if (!dom->graph_exec) {
+        // the tile-order state is set up outside the capture (a replay must
+        // not zero it); the captured launches order whole grids
+        mrlbm_status pst = prepare_tile_order(dom, dom->stream);
+        if (pst) return pst;
         cudaGraph_t g;
         CK(cudaStreamBeginCapture(dom->stream, cudaStreamCaptureModeThreadLocal));
         for (int s = 0; s < GRAPH_STEPS; s++) {
-            mrlbm_status st = enqueue_step(dom, s & 1, dom->stream);
+            mrlbm_status st = enqueue_step(dom, s & 1, dom->stream, false);
             if (st) {
                 cudaStreamEndCapture(dom->stream, &g);
                 if (g) cudaGraphDestroy(g);
@@ -762,7 +830,9 @@ mrlbm_status mrlbm::check_device_error(mrlbm_domain* dom)
         if (h & 2)
             return fail(MRLBM_EBOUNDS, "a step kernel skipped an out-of-range access (flag 0x%x: kinds 0x%x)", h,
                         (h >> 8) & 0xff);
-        return fail(MRLBM_ETIMEDOUT, "a step kernel gave up waiting for its tile loads (flag 0x%x)", h);
+        return fail(MRLBM_ETIMEDOUT,
+                    "a step kernel gave up waiting for its tile loads or for the previous step's tiles (flag 0x%x)",
+                    h);
     }
     return MRLBM_OK;
 }
@@ -835,6 +905,19 @@ extern "C" mrlbm_status mrlbm_set_z_chunk(mrlbm_domain* dom, int lz)
         dom->graph_exec = nullptr;
     }
     dom->lz = lz;
+    return MRLBM_OK;
+}
+
+extern "C" mrlbm_status mrlbm_set_tile_order(mrlbm_domain* dom, int on)
+{
+    if (!dom) return fail(MRLBM_EINVAL, "null argument");
+    if (on != 0 && on != 1) return fail(MRLBM_EINVAL, "tile order %d is not 0 or 1", on);
+    dom->tile_order = on != 0;
+    if (dom->graph_exec) {  // the captured launches carry the old setting
+        cudaStreamSynchronize(dom->stream);
+        cudaGraphExecDestroy(dom->graph_exec);
+        dom->graph_exec = nullptr;
+    }
     return MRLBM_OK;
 }
 

@@ -1,3 +1,3 @@
 // Step-kernel variants for D3Q27 with __half moment storage.
 #include "step_dispatch.cuh"
-template mrlbm_status mrlbm::dispatch_step<27, __half>(const CUtensorMap*, const mrlbm::StepArgs&, int, cudaStream_t);
+template mrlbm_status mrlbm::dispatch_step<27, __half>(const CUtensorMap*, const mrlbm::StepArgs&, int, cudaStream_t, bool);

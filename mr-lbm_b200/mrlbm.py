@@ -203,6 +203,7 @@ def lib():
             "mrlbm_selftest_bounded_wait": [C.c_uint, C.POINTER(C.c_double)],
             "mrlbm_set_stream": [VP, VP],
             "mrlbm_set_z_chunk": [VP, C.c_int],
+            "mrlbm_set_tile_order": [VP, C.c_int],
             "mrlbm_nccl_unique_id": [VP],
             "mrlbm_nccl_comm_init": [C.c_int, VP, C.c_int, C.POINTER(VP)],
             "mrlbm_nccl_comm_destroy": [VP],
@@ -363,6 +364,12 @@ class Domain:
     def set_z_chunk(self, lz):
         """z planes per CTA of the step (0: automatic); results do not depend on it."""
         check(self.L.mrlbm_set_z_chunk(self.h, int(lz)))
+
+    def set_tile_order(self, on):
+        """Tile-ordered steps (True, the default): a step may start while the
+        one before it finishes, each tile waiting for its neighbours only;
+        False orders whole launches.  Results do not depend on it."""
+        check(self.L.mrlbm_set_tile_order(self.h, 1 if on else 0))
 
     def z_chunk(self):
         v = C.c_int()
