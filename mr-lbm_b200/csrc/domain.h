@@ -44,6 +44,7 @@ struct mrlbm_domain {
     float scale[mrlbm::NM_MAX] = {}, iscale[mrlbm::NM_MAX] = {};
     int lz = 0;                      // z planes per work item when a batch has set it (0: single-domain choice)
     int lz_t[2] = {16, 16};          // single-domain z planes per CTA, per tile kind
+    int lz_o[2] = {16, 16};          // the same for tile-ordered (overlapping) steps
     int nsm = 148;                   // SMs of the device the domain lives on
     cudaStream_t stream = nullptr;      // where the domain's work is queued
     cudaStream_t own_stream = nullptr;  // the stream the domain created (stream unless mrlbm_set_stream)
@@ -77,6 +78,9 @@ void storage_scales(int storage, int nm, float* scale, float* iscale);
 inline bool is_half_storage(int storage) { return storage == MRLBM_F16 || storage == MRLBM_F16U; }
 mrlbm_status domain_alloc(mrlbm_domain* dom);
 int choose_lz(const mrlbm_domain* dom, int tyi);
+int choose_lz_overlap(const mrlbm_domain* dom, int tyi);
+// whether a step with these flags is tile-ordered (overlapping launches)
+bool tile_ordered(const mrlbm_domain* dom, int flags);
 void fill_step_args(const mrlbm_domain* dom, StepArgs& a, int parity, int& flags);
 // chained: the launch before this one on s is this domain's step
 mrlbm_status enqueue_step(mrlbm_domain* dom, int parity, cudaStream_t s, bool chained);

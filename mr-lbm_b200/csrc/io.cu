@@ -382,7 +382,8 @@ extern "C" mrlbm_status mrlbm_save_info(mrlbm_domain* dom, const char* path_file
 }
 
 // The same text for a description alone, on the host (no device work): the
-// step's geometry is that of a domain without wall classes on a 148-SM B200.
+// step's geometry is that of a domain without wall classes on a 148-SM B200,
+// stepped tile-ordered (the default).
 extern "C" mrlbm_status mrlbm_info_text(const mrlbm_desc* d, const char* id_sim, const char* case_name, int nsteps,
                                         double mlups, char* buf, size_t cap, size_t* len)
 {
@@ -392,7 +393,8 @@ extern "C" mrlbm_status mrlbm_info_text(const mrlbm_desc* d, const char* id_sim,
     tmp.nsm = 148;
     const int flags = (d->rheology != MRLBM_NEWTONIAN ? F_POWERLAW | F_BC : 0) | (d->thermal ? F_THERMAL : 0);
     const int by = tile_rows(flags);
-    const std::string t = info_text(*d, id_sim, case_name, nsteps, mlups, by, choose_lz(&tmp, by));
+    const int lz = tile_ordered(&tmp, flags) ? choose_lz_overlap(&tmp, by) : choose_lz(&tmp, by);
+    const std::string t = info_text(*d, id_sim, case_name, nsteps, mlups, by, lz);
     *len = t.size();
     if (buf) {
         if (cap < t.size() + 1) return fail(MRLBM_EINVAL, "buffer of %zu bytes, the text needs %zu", cap, t.size() + 1);
